@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""PFC site-steps/s on B200: the fused ETD1 stepper on the 2048^2 stdPFC polycrystal.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (stdPFC polycrystal, 2048^2): dx = dy = pi/4, dt = 0.5, r = epsilon = -0.3,
+Gamma = beta = q0 = 1, g = 0; mean psi = -0.3 plus 0.01 U[-1,1] noise (seed 0) and
+64 seeds of radius 12 dx with the rotated one-mode profile (seed 1). Synthetic,
+seeded; no dataset is involved.
+
+One bench step = one ETD1 time step (row kernel + column kernel). `value` is the
+FP32-mixed form with the state resident in HBM, each step timed with CUDA events
+on the launching stream and L2 flushed (a 256 MiB write) between steps, so every
+step starts from HBM. The FP64 plain form is timed the same way (`fp64_plain`).
+`e2e` is the same metric through the public Python API (`State.n[...] = host`,
+`TimeStep()` x 100, `CalculateFreeEnergy()`, `State.n.get()`), host buffers pinned,
+both copies inside the timed region. Under torchrun with N > 1 every rank runs an
+independent replica (a single simulation does not shard profitably over NVLink);
+timings are the max over ranks.
+
+`--impl reference` times the reference's CPU algorithm (the oracle port of
+stdpfc_cpu, threaded pocketfft through scipy.fft with every host core) on the
+same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "PFC site-steps/s (stdPFC 2048^2 polycrystal, FP32-mixed ETD1 step)"
+UNIT = "site-steps/s"
+NX = NY = 2048
+DX = math.pi / 4
+PARAMS = dict(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.3, g=0.0, dt=0.5)
+E2E_STEPS = 100
+FLUSH_BYTES = 256 << 20
+
+
+def workload_config(extra=None):
+    c = {"workload": "stdPFC polycrystal 2048x2048, dx=pi/4, dt=0.5, r=-0.3, 64 seeds r=12dx, FP32-mixed",
+         "nx": NX, "ny": NY, "model": "stdPFC", "precision": "fp32_mixed",
+         "l2": "flushed between steps (256 MiB write)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def initial_field():
+    from pfc_models_b200 import fields, spectral
+    g = spectral.Build2DGeometry(NX, NY, NX * DX, NY * DX)
+    return g, fields.GeneratePolycrystalInitialConditions(g, -0.3, 0.01, nSeeds=64, radius=12 * DX,
+                                                          A=0.5, q=math.sqrt(3) / 2, noise_seed=0, seed=1)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle port)
+def cpu_baseline(max_seconds=20.0, max_steps=20):
+    """Reference CPU algorithm (oracle port of stdpfc_cpu) on this host, all cores."""
+    from oracle import pfc_oracle as orc
+    geom_h, f0 = initial_field()
+    geom = orc.build_geometry(NX, NY, NX * DX, NY * DX)
+    cores = os.cpu_count() or 1
+    sim = orc.OracleSim("std", orc.Params(**PARAMS), geom, fft="scipy", workers=cores)
+    sim.set_field(f0)
+    sim.step()  # warm-up (plan caches)
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < max_steps and (time.perf_counter() - t_start) < max_seconds:
+        t0 = time.perf_counter()
+        sim.step()
+        times.append(time.perf_counter() - t0)
+    med = statistics.median(times)
+    return {"value": NX * NY / med, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{len(times)} ETD1 steps of the same 2048^2 workload, median step "
+                      f"{med * 1e3:.1f} ms (numpy/scipy pocketfft, {cores} threads)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import pfc_oracle as orc
+    _, f0 = initial_field()
+    geom = orc.build_geometry(NX, NY, NX * DX, NY * DX)
+    cores = os.cpu_count() or 1
+    sim = orc.OracleSim("std", orc.Params(**PARAMS), geom, fft="scipy", workers=cores)
+    sim.set_field(f0)
+    for _ in range(max(args.warmup, 1)):
+        sim.step()
+    budget_s = 150.0
+    times = []
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        sim.step()
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_all > budget_s:
+            break
+    total = sum(times)
+    value = NX * NY * len(times) / total
+    sample = (f"{len(times)} of {args.steps} requested ETD1 steps at 2048^2 "
+              f"(stopped at the {budget_s:.0f} s budget)" if len(times) < args.steps else
+              f"{len(times)} ETD1 steps at 2048^2")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded polycrystal)",
+            "config": workload_config({"precision": "fp64 (reference CPU algorithm)", "l2": "n/a (CPU)"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample + f", numpy/scipy pocketfft, {cores} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    distributed = world > 1
+    if distributed:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+
+    def barrier():
+        if distributed:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not distributed:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from pfc_models_b200 import stdpfc
+
+    geom, f0 = initial_field()
+    flush_buf = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def flush():
+        flush_buf.zero_()
+
+    def build(precision):
+        sim = stdpfc.BuildB200_Simulation(stdpfc.BuildStdPFCModelParameters(**PARAMS), geom, precision=precision)
+        sim.State.n[...] = f0
+        return sim
+
+    def time_steps(sim, k, sampler=None):
+        ms_r, ms_c = [], []
+        launches0 = sim.plan.launches()
+        barrier()
+        if sampler:
+            sampler.start()
+        for _ in range(k):
+            r, c = sim.plan.step_timed(1)
+            ms_r.append(r)
+            ms_c.append(c)
+            flush()
+        barrier()
+        clocks = sampler.stop() if sampler else None
+        return ms_r, ms_c, sim.plan.launches() - launches0, clocks
+
+    sites = NX * NY
+    results = {}
+    for precision in ("fp32", "fp64"):
+        sim = build(precision)
+        for _ in range(max(args.warmup, 3)):
+            sim.plan.step_timed(1)
+            flush()
+        sampler = ClockSampler(local) if precision == "fp32" else None
+        ms_r, ms_c, launches, clocks = time_steps(sim, args.steps, sampler)
+        total_ms = max_over_ranks(sum(ms_r) + sum(ms_c))
+        results[precision] = dict(sim=sim, ms_r=ms_r, ms_c=ms_c, total_ms=total_ms, launches=launches,
+                                  clocks=clocks, value=world * sites * args.steps / (total_ms / 1e3))
+    # F agreement of the two forms after the same number of steps from the same field
+    F32 = results["fp32"]["sim"].Reduce()
+    F64 = results["fp64"]["sim"].Reduce()
+    dF = abs(F32[0] / F64[0] - 1)
+    mass_drift = abs(F32[2] - float(np.mean(f0)))
+
+    # ---- end to end through the public API, host buffers pinned
+    sim = results["fp32"]["sim"]
+    host_in = torch.from_numpy(f0).pin_memory()
+    e2e_frames = max(2, min(args.steps // 20, 10))
+    sim.State.n[...] = host_in
+    sim.TimeSteps(E2E_STEPS)
+    sim.CalculateFreeEnergy()
+    barrier()
+    s = torch.cuda.current_stream(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(s)
+    for _ in range(e2e_frames):
+        sim.State.n[...] = host_in
+        for _ in range(E2E_STEPS):
+            sim.TimeStep()
+        sim.CalculateFreeEnergy()
+        sim.State.n.get()
+    ev1.record(s)
+    barrier()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    e2e_value = world * sites * E2E_STEPS * e2e_frames / (e2e_ms / 1e3)
+
+    # ---- roofline of the dominant kernel (column pass: reads V and n_hat, writes n_hat' and W)
+    hbm, peak_kind = peaks()
+    r32 = results["fp32"]
+    col_ms = statistics.mean(r32["ms_c"])
+    row_ms = statistics.mean(r32["ms_r"])
+    elt = 8  # complex64
+    spec = (NX // 2) * NY * elt
+    col_bytes, row_bytes = 4 * spec, 2 * spec
+    dominant = "column" if col_ms >= row_ms else "row"
+    dom_bytes, dom_ms = (col_bytes, col_ms) if dominant == "column" else (row_bytes, row_ms)
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    step_achieved = (col_bytes + row_bytes) / ((col_ms + row_ms) / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get(f"fp32_{dominant}")
+        except Exception:
+            traffic = None
+
+    if rank == 0:
+        ms_per_step = r32["total_ms"] / args.steps
+        line = {
+            "metric": METRIC, "value": r32["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 mean, ETD coefficients and reductions)",
+            "data": "synthetic (seeded polycrystal)",
+            "config": workload_config({"parallelism": "replicas" if world > 1 else "single GPU"}),
+            "gpu_launches": r32["launches"],
+            "fp64_plain": {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["total_ms"] / args.steps,
+                           "fp32_over_fp64": r32["value"] / results["fp64"]["value"]},
+            "accuracy": {"dF_over_F_fp32_vs_fp64": dF, "mass_drift_fp32": mass_drift,
+                         "after_steps": max(args.warmup, 3) + args.steps},
+            "roofline": {"bound": "hbm", "kernel": f"{dominant} pass (FP32)", "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": dom_bytes,
+                         "step": {"achieved": step_achieved, "frac": step_achieved / hbm,
+                                  "bytes_per_site": (col_bytes + row_bytes) / sites,
+                                  "row_ms": row_ms, "col_ms": col_ms}},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": sites * 8,
+                    "d2h_bytes_per_step": sites * 8 + 24,
+                    "note": f"one e2e step = H2D of the field, {E2E_STEPS} TimeStep() calls, "
+                            "CalculateFreeEnergy(), State.n.get()"},
+            "clocks": r32["clocks"],
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line))
+    for r in results.values():
+        r["sim"].plan.close()
+    if distributed:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

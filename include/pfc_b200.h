@@ -1,0 +1,148 @@
+/*
+ * pfc_b200.h — C ABI of the B200 (sm_100a) pseudo-spectral ETD1 stepper for
+ * standard and log phase-field-crystal models in 2D.
+ *
+ * Plain C types only: ints, doubles, raw device pointers, and a CUDA stream
+ * passed as `void*` (a cudaStream_t; NULL is the legacy default stream).
+ * Every function returns PFC_OK (0) or a PFC_E_* code; pfc_last_error()
+ * returns the message of the last failure on the calling thread. No C++
+ * exception crosses this boundary. A plan is not thread-safe: use one plan per
+ * host thread / stream at a time.
+ *
+ * Reference interfaces (paths relative to the reference's src/pfc_models/):
+ * each entry point below names the Python call of the reference it replaces.
+ */
+#ifndef PFC_B200_H
+#define PFC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PFC_ABI_VERSION 1
+
+/* return codes */
+#define PFC_OK 0
+#define PFC_E_ARG 1         /* invalid argument or unsupported size */
+#define PFC_E_CUDA 2        /* a CUDA runtime call failed */
+#define PFC_E_NAN 3         /* a non-finite value was detected in the state */
+#define PFC_E_TIMEOUT 4     /* a bounded device-side wait gave up */
+#define PFC_E_STATE 5       /* call out of order (e.g. step before set_state) */
+#define PFC_E_NOMEM 6       /* device allocation failed */
+
+/* models */
+#define PFC_MODEL_STD 0     /* nonlinearity g n^2 + n^3        (models/stdpfc) */
+#define PFC_MODEL_LOG 1     /* nonlinearity ln(phi) + g phi^2 + phi^3 (models/logpfc) */
+
+/* precision forms */
+#define PFC_FP64_PLAIN 0    /* FP64 end to end */
+#define PFC_FP32_MIXED 1    /* FP32 FFTs and pointwise math on the deviation psi - mean;
+                               FP64 mean, ETD coefficients, near-singular log, reductions */
+
+/* fields for pfc_get_field */
+#define PFC_FIELD_N 0           /* current density field n (or phi) */
+#define PFC_FIELD_MU 1          /* mu of the state at the start of the last step */
+#define PFC_FIELD_LOCAL_MU 2    /* Gaussian-filtered mu, same state */
+#define PFC_FIELD_LOCAL_N 3     /* Gaussian-filtered n of the state at the start of the last step */
+#define PFC_FIELD_NONLIN_MU 4   /* nonlinear part of mu, same state */
+#define PFC_FIELD_OF_CURRENT 0x100  /* OR-ed in: use the current state instead */
+
+/* spectra for pfc_get_spectrum (complex128, shape (ny, nx/2+1), row-major, unnormalised rfft2) */
+#define PFC_SPEC_N_HAT 0        /* rfft2 of n at the start of the last step (State.n_hat) */
+#define PFC_SPEC_N_HAT_NOW 1    /* rfft2 of the current n */
+
+/* status bits (pfc_status) */
+#define PFC_STATUS_NONFINITE 1  /* a reduction met a NaN/Inf */
+
+/*
+ * Problem description. Field meanings follow
+ * BuildStdPFCModelParameters / BuildLogPFCModelParameters
+ * (models/stdpfc/simulation.py:60-80, models/logpfc/simulation.py:51-75) and
+ * Build2DGeometry (discretization/spectral/geometry_2d.py:70-88).
+ * nx must be even; nx and ny may contain only the prime factors 2, 3, 5, 7, 11, 13.
+ */
+typedef struct pfc_problem {
+  int32_t nx, ny;          /* grid points along x (fast axis) and y */
+  int32_t model;           /* PFC_MODEL_* */
+  int32_t precision;       /* PFC_FP64_PLAIN or PFC_FP32_MIXED */
+  double lx, ly;           /* box lengths */
+  double gamma, beta, q0, epsilon, g, dt;
+  double small_z_tol;      /* ETD1 series threshold, kernels.py:55 (default 2e-5) */
+  double min_phi;          /* log model: clamp floor when clamp_log != 0 */
+  int32_t clamp_log;       /* 0: unclamped log, as the reference (logpfc/simulation.py:296) */
+  int32_t flags;           /* reserved, 0 */
+} pfc_problem;
+
+typedef struct pfc_plan pfc_plan;
+
+/* Replaces BuildCupyGPU_Simulation (models/stdpfc/simulation.py:270-286,
+ * models/logpfc/simulation.py:265-281) with _SimulationState.__init__
+ * (models/stdpfc/simulation.py:99-164): builds the k-space operator, the ETD1
+ * coefficients (kernel_etd, discretization/spectral/kernels.py:55-71) in FP64,
+ * twiddle tables and the device buffers, on the current CUDA device. */
+int pfc_plan_create(const pfc_problem* problem, pfc_plan** out);
+
+/* Frees every device buffer the plan owns. */
+int pfc_plan_destroy(pfc_plan* plan);
+
+/* Replaces `sim.State.n[...] = cp.asarray(n0)` (tests/test_smoke_models.py:226-239,
+ * phase_diagram adapter set_state, models/stdpfc_cpu/phase_diagram.py:262-263):
+ * loads a real FP64 field of shape (ny, nx), row-major, from device memory. */
+int pfc_set_state(pfc_plan* plan, const double* dev_field, void* stream);
+
+/* Replaces reads of `sim.State.n` / `sim.n.get()` (models/stdpfc/simulation.py:283):
+ * writes the current field as FP64 (ny, nx) to device memory. */
+int pfc_get_state(pfc_plan* plan, double* dev_field, void* stream);
+
+/* Replaces `for _ in range(nsteps): sim.TimeStep()` (models/stdpfc/simulation.py:225-235,
+ * models/logpfc/simulation.py:220-230). Stream-ordered, no host synchronisation. */
+int pfc_step(pfc_plan* plan, int64_t nsteps, void* stream);
+
+/* pfc_step with instrumentation: also returns the summed device time (ms) of
+ * the row-pass and column-pass kernels, measured with CUDA events recorded on
+ * `stream` around each launch. Synchronises the stream before returning. */
+int pfc_step_timed(pfc_plan* plan, int64_t nsteps, double* ms_row, double* ms_col, void* stream);
+
+/* Replaces CalculateFreeEnergy (models/stdpfc/simulation.py:249-268,
+ * models/logpfc/simulation.py:244-263) without the full-field device-to-host copy:
+ * writes three doubles to dev_out3 = {F per site, mean mu per site, mean density},
+ * accumulated in compensated FP64 on the device. */
+int pfc_reduce(pfc_plan* plan, double* dev_out3, void* stream);
+
+/* Replaces State.mu / State.local_mu (models/stdpfc/simulation.py:143-155, 217-219),
+ * Get_local_n (:237-247) and State.nonlin_mu, computed on demand. `w` is the
+ * Gaussian width of kernel_local (kernels.py:49-52; the models use 2*pi). */
+int pfc_get_field(pfc_plan* plan, int which, double w, double* dev_field, void* stream);
+
+/* Replaces State.n_hat (models/stdpfc/simulation.py:133-137): complex128 (ny, nx/2+1). */
+int pfc_get_spectrum(pfc_plan* plan, int which, double* dev_c128, void* stream);
+
+/* Host copies of the FP64 ETD1 coefficients the plan built: A = exp(L dt) and
+ * Bg = B * Gamma * lap (kernels.py:55-71 times the factor of calc_n_next_impl,
+ * models/stdpfc/simulation.py:326-331), each (ny, nx/2+1) row-major. */
+int pfc_get_coefficients(pfc_plan* plan, double* host_a, double* host_bg);
+
+/* Device status bits (PFC_STATUS_*), read synchronously on the plan's last stream. */
+int pfc_status(pfc_plan* plan, int32_t* out_status);
+
+/* Launch configuration chosen for this plan, for reporting: out[0..7] =
+ * {row rows/CTA, row threads/FFT, row CTAs, col columns/CTA, col threads/FFT,
+ *  col CTAs, row smem bytes, col smem bytes}. */
+int pfc_plan_info(pfc_plan* plan, int64_t* out8);
+
+/* Kernel launches issued by this plan since creation (for accounting). */
+int64_t pfc_launch_count(pfc_plan* plan);
+
+/* Copies the last error message of this thread into buf (NUL-terminated). */
+int pfc_last_error(char* buf, size_t len);
+
+int pfc_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PFC_B200_H */

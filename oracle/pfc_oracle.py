@@ -1,0 +1,200 @@
+"""ORACLE — test infrastructure, not product code.
+
+A CPU restatement (NumPy / SciPy FFT) of the reference's pseudo-spectral ETD1
+stepper for standard and log PFC in 2D, used to check the CUDA path. Only
+``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+(and its ``--impl reference`` arm) may import it, and only as the checker or
+as the timed CPU baseline; the product never routes through it.
+
+Parity is pinned: ``tests/test_oracle_golden.py`` checks this module against
+fixtures generated by running the unmodified reference
+(``tests/golden/make_golden.py``), including the reference's own recorded
+free energies (stdpfc_cpu/test_regression.py:64, logpfc_cpu/test_regression.py:28-32).
+
+Each function cites the reference lines it restates (paths relative to the
+reference project root, ``src/pfc_models/...``).
+"""
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+try:  # threaded pocketfft (same algorithm as numpy.fft); optional
+    import scipy.fft as _sfft
+except Exception:  # pragma: no cover
+    _sfft = None
+
+
+# ---------------------------------------------------------------- substrate
+@dataclass
+class Geometry:
+    """discretization/spectral/geometry_2d.py:70-88 (Build2DGeometry)."""
+    Nx: int
+    Ny: int
+    Lx: float
+    Ly: float
+    dx: float
+    dy: float
+    X: np.ndarray
+    Y: np.ndarray
+    KX: np.ndarray
+    KY: np.ndarray
+    K2: np.ndarray
+
+
+def build_geometry(Nx, Ny, Lx, Ly) -> Geometry:
+    """geometry_2d.py:70-88: x, y by linspace(endpoint=False); kx = 2 pi rfftfreq(Nx, dx),
+    ky = 2 pi fftfreq(Ny, dy); meshgrids of shape (Ny, Nx) and (Ny, Nx//2+1)."""
+    dx, dy = Lx / Nx, Ly / Ny
+    x = np.linspace(0, Lx, Nx, endpoint=False)
+    y = np.linspace(0, Ly, Ny, endpoint=False)
+    X, Y = np.meshgrid(x, y)
+    kx = 2 * np.pi * np.fft.rfftfreq(Nx, d=dx)
+    ky = 2 * np.pi * np.fft.fftfreq(Ny, d=dy)
+    KX, KY = np.meshgrid(kx, ky)
+    return Geometry(Nx, Ny, Lx, Ly, dx, dy, X, Y, KX, KY, KX**2 + KY**2)
+
+
+def laplacian(geom: Geometry) -> np.ndarray:
+    """kernels.py:45 (d2_dlap = -(KX^2 + KY^2)); the models take its real part
+    (stdpfc/simulation.py:112)."""
+    return -(geom.KX**2 + geom.KY**2)
+
+
+def gaussian(geom: Geometry, w: float) -> np.ndarray:
+    """kernels.py:49-52 (kernel_local): exp(-|k|^2 w^2 / 2)."""
+    return np.exp(-((geom.KX) ** 2 + (geom.KY) ** 2) * w**2 / 2)
+
+
+def linear_mu(beta, q0, epsilon, lap):
+    """stdpfc/simulation.py:83-90 and logpfc/simulation.py:78-85: beta (q0^2 + lap)^2 + epsilon."""
+    return beta * (q0**2 + lap) ** 2 + epsilon
+
+
+def linear_n(Gamma, beta, q0, epsilon, lap):
+    """stdpfc/simulation.py:92-96: Gamma lap (beta (q0^2 + lap)^2 + epsilon)."""
+    return Gamma * lap * linear_mu(beta, q0, epsilon, lap)
+
+
+def etd1(kLinear, dt, small_z_tol=2e-5):
+    """kernels.py:55-71 (kernel_etd): A = exp(L dt); B = (A - 1)/L where |L dt| > tol,
+    else dt (1 + z/2 + z^2/6)."""
+    z = kLinear * dt
+    A = np.exp(z)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        B = np.where(np.abs(z) > small_z_tol, (A - 1) / kLinear, dt * (1 + z / 2 + z**2 / 6))
+    return A, B
+
+
+# ---------------------------------------------------------------- model
+@dataclass
+class Params:
+    """stdpfc/simulation.py:60-80 (BuildStdPFCModelParameters) and
+    logpfc/simulation.py:51-75 (BuildLogPFCModelParameters)."""
+    Gamma: float = 1.0
+    beta: float = 1.0
+    q0: float = 1.0
+    epsilon: float = 1.0
+    g: float = 1.0
+    dt: float = 0.01
+    smallZTol: float = 2e-5
+
+
+def nonlin_mu(model: str, n: np.ndarray, g: float) -> np.ndarray:
+    """std: g n^2 + n^3 (stdpfc_cpu/simulation.py:323-333, stdpfc/simulation.py:297).
+    log: ln(phi) + g phi^2 + phi^3, unclamped (logpfc_cpu/simulation.py:321-331,
+    logpfc/simulation.py:296)."""
+    if model == "std":
+        return g * (n**2) + (n**3)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.log(n) + g * (n**2) + (n**3)
+
+
+class OracleSim:
+    """The reference CPU stepper (stdpfc_cpu/simulation.py:238-248, logpfc_cpu/simulation.py:233-243),
+    restated without the unused diagnostics batch.
+
+    ``fft`` selects numpy.fft (default; the algorithm the fixtures were generated with)
+    or scipy.fft with ``workers`` threads (same pocketfft algorithm, used for timing).
+    """
+
+    def __init__(self, model, params: Params, geom: Geometry, fft="numpy", workers=1):
+        assert model in ("std", "log")
+        self.model, self.p, self.geom = model, params, geom
+        self.t = 0.0
+        lap = laplacian(geom)
+        self.lap = lap
+        self.lin_mu = linear_mu(params.beta, params.q0, params.epsilon, lap)
+        kl = linear_n(params.Gamma, params.beta, params.q0, params.epsilon, lap)
+        self.A, self.B = etd1(kl, params.dt, params.smallZTol)
+        # the reference's update multiplies B by (Gamma * lap) per step
+        # (stdpfc_cpu/simulation.py:365-372); both products are kept in the same order
+        self.gauss = gaussian(geom, 2 * np.pi)
+        self.n = np.zeros((geom.Ny, geom.Nx))
+        self.n_hat = np.zeros((geom.Ny, geom.Nx // 2 + 1), dtype=complex)
+        self.nonlin_mu_hat = np.zeros_like(self.n_hat)
+        if fft == "scipy" and _sfft is not None:
+            w = workers if workers and workers > 0 else os.cpu_count()
+            self._rfft2 = lambda a: _sfft.rfft2(a, workers=w)
+            self._irfft2 = lambda a, s: _sfft.irfft2(a, s=s, workers=w)
+        else:
+            self._rfft2 = lambda a: np.fft.rfft2(a)
+            self._irfft2 = lambda a, s: np.fft.irfft2(a, s=s)
+
+    def set_field(self, n):
+        self.n = np.array(n, dtype=np.float64, copy=True)
+
+    def step(self):
+        """One ETD1 step: batch1 (nonlinearity + rfft2), batch3 (update + irfft2), n <- n_next."""
+        p = self.p
+        N = nonlin_mu(self.model, self.n, p.g)                     # _Batch1_CalcNonlinMu
+        self.n_hat = self._rfft2(self.n)
+        self.nonlin_mu_hat = self._rfft2(N)
+        n_next_hat = self.A * self.n_hat + self.B * (p.Gamma * self.lap * self.nonlin_mu_hat)
+        self.n = self._irfft2(n_next_hat, self.n.shape)            # _Batch3_CalcNNext
+        self.t += p.dt
+
+    def mu(self):
+        """mu = irfft2(L_mu n_hat + N_hat) of the current field (stdpfc/simulation.py:299-308, batch2)."""
+        N = nonlin_mu(self.model, self.n, self.p.g)
+        mu_hat = self.lin_mu * self._rfft2(self.n) + self._rfft2(N)
+        return self._irfft2(mu_hat, self.n.shape)
+
+    def free_energy(self):
+        """stdpfc_cpu/simulation.py:263-285 (std) and logpfc_cpu/simulation.py:259-283 (log):
+        mean of n irfft2(beta/2 (q0^2 + lap)^2 n_hat) + eps/2 n^2 + g/3 n^3 + n^4/4 (+ n ln n)."""
+        p, n = self.p, self.n
+        n_hat = self._rfft2(n)
+        lin_f = self._irfft2((p.beta / 2.0) * (p.q0**2 + self.lap) ** 2 * n_hat, n.shape)
+        nonlin_f = (p.epsilon / 2.0) * n**2 + (p.g / 3.0) * n**3 + (1 / 4.0) * n**4
+        if self.model == "log":
+            with np.errstate(divide="ignore", invalid="ignore"):
+                nonlin_f = n * np.log(n) + nonlin_f
+        return float((n * lin_f + nonlin_f).mean())
+
+    def mu_per_site(self):
+        """Mean chemical potential: mu_hat(0)/(Nx Ny) = L_mu(0) mean(n) + mean(N(n));
+        the quantity the adapters' liquid_chemical_potential gives in closed form for a
+        uniform field (stdpfc_cpu/phase_diagram.py:312-320, logpfc_cpu/phase_diagram.py:336-347)."""
+        p = self.p
+        return float(linear_mu(p.beta, p.q0, p.epsilon, 0.0) * self.n.mean()
+                     + nonlin_mu(self.model, self.n, p.g).mean())
+
+    def local_field(self, w=2 * np.pi):
+        """Get_local_n (stdpfc/simulation.py:237-247) on the current field: irfft2(G rfft2(n))."""
+        return self._irfft2(gaussian(self.geom, w) * self._rfft2(self.n), self.n.shape)
+
+
+def run(model, params: Params, geom: Geometry, field0, steps, record_every=None):
+    """Step ``field0`` for ``steps`` steps; return (final field, [(step, F, mean), ...])."""
+    sim = OracleSim(model, params, geom)
+    sim.set_field(field0)
+    rec = []
+    for s in range(steps + 1):
+        if record_every and s % record_every == 0:
+            rec.append((s, sim.free_energy(), float(sim.n.mean())))
+        if s < steps:
+            sim.step()
+    return sim.n, rec

@@ -1,0 +1,92 @@
+"""ctypes binding of ``libpfc_b200.so`` (the C ABI of ``include/pfc_b200.h``).
+
+The shared library is built in-tree by :mod:`pfc_models_b200.build` and must
+sit next to this file. There is no fallback: if the library is missing or a
+CUDA device is absent, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpfc_b200.so")
+
+PFC_OK, PFC_E_ARG, PFC_E_CUDA, PFC_E_NAN, PFC_E_TIMEOUT, PFC_E_STATE, PFC_E_NOMEM = range(7)
+MODEL_STD, MODEL_LOG = 0, 1
+FP64_PLAIN, FP32_MIXED = 0, 1
+FIELD_N, FIELD_MU, FIELD_LOCAL_MU, FIELD_LOCAL_N, FIELD_NONLIN_MU = range(5)
+FIELD_OF_CURRENT = 0x100
+SPEC_N_HAT, SPEC_N_HAT_NOW = 0, 1
+
+# every symbol include/pfc_b200.h declares, with (restype, argtypes)
+_vp, _i32, _i64, _dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+SIGNATURES = {
+    "pfc_abi_version": (ctypes.c_int, []),
+    "pfc_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
+    "pfc_plan_create": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "pfc_plan_destroy": (ctypes.c_int, [_vp]),
+    "pfc_set_state": (ctypes.c_int, [_vp, _vp, _vp]),
+    "pfc_get_state": (ctypes.c_int, [_vp, _vp, _vp]),
+    "pfc_step": (ctypes.c_int, [_vp, _i64, _vp]),
+    "pfc_step_timed": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(_dbl), ctypes.POINTER(_dbl), _vp]),
+    "pfc_reduce": (ctypes.c_int, [_vp, _vp, _vp]),
+    "pfc_get_field": (ctypes.c_int, [_vp, ctypes.c_int, _dbl, _vp, _vp]),
+    "pfc_get_spectrum": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
+    "pfc_get_coefficients": (ctypes.c_int, [_vp, _vp, _vp]),
+    "pfc_status": (ctypes.c_int, [_vp, ctypes.POINTER(_i32)]),
+    "pfc_plan_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64)]),
+    "pfc_launch_count": (_i64, [_vp]),
+}
+
+
+class PfcProblem(ctypes.Structure):
+    """Mirror of ``pfc_problem`` in include/pfc_b200.h."""
+    _fields_ = [
+        ("nx", _i32), ("ny", _i32), ("model", _i32), ("precision", _i32),
+        ("lx", _dbl), ("ly", _dbl),
+        ("gamma", _dbl), ("beta", _dbl), ("q0", _dbl), ("epsilon", _dbl), ("g", _dbl), ("dt", _dbl),
+        ("small_z_tol", _dbl), ("min_phi", _dbl),
+        ("clamp_log", _i32), ("flags", _i32),
+    ]
+
+
+class PfcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[pfc error {code}] {msg}")
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path: str | None = None):
+    """Load the library once; raise if it is not built."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = path or LIB_PATH
+        if not os.path.exists(p):
+            raise ImportError(f"{p} is not built: run `python -m pfc_models_b200.build` "
+                              "(there is no CPU fallback)")
+        lib = ctypes.CDLL(p)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(1024)
+    load().pfc_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int):
+    if rc != PFC_OK:
+        raise PfcError(rc, last_error())

@@ -1,0 +1,572 @@
+// Row and column kernels of the fused ETD1 step, plus the state, field and
+// reduction kernels that share their transforms.
+//
+// Data layout in HBM. Every spectral array holds nx/2 "packed" columns of ny
+// complex values, stored column-major ([kx][y], y fastest) so that a column
+// transform reads one contiguous run. Column 0 packs the two real-valued
+// columns of a real-input row transform: entry = X[0] + i X[nx/2] (DC and
+// Nyquist). The 2-D spectrum of that packed column is P = H0 + i HM with H0, HM
+// the Hermitian kx = 0 and kx = nx/2 columns of the true rfft2; every kernel
+// unpacks them from the pair (ky, -ky) before applying a kx-dependent factor.
+//
+// Per step, with M = nx/2 (state: n_hat = packed rfft2 of n, W = its column
+// inverse scaled by 1/(nx ny), so that the unnormalised row C2R of W is n):
+//   row kernel    W  -> C2R -> N(n) -> R2C -> V        (read 1, write 1)
+//   column kernel V  -> FFT_y -> n_hat' = A n_hat + Bg N_hat -> n_hat'
+//                 n_hat' -> IFFT_y -> W'                 (read 2, write 2)
+// FP32_MIXED runs the same kernels on delta = n - mean in float; the mean is an
+// FP64 device scalar and the packed DC of delta_hat is held at exactly zero.
+#pragma once
+#include "pfc_fft.cuh"
+
+#ifndef PFC_LB
+#define PFC_LB __launch_bounds__(256)
+#endif
+
+namespace pfc {
+
+enum : int { kModelStd = 0, kModelLog = 1 };
+enum : int { kRowStep = 0, kRowForward = 1, kRowMaterialize = 2, kRowReduce = 3 };
+enum : int { kColStep = 0, kColInit = 1, kColCombine = 2, kColParseval = 3, kColExport = 4 };
+enum : int { kCombineMu = 0, kCombineLocalMu = 1, kCombineLocalN = 2, kCombineNonlin = 3, kCombineN = 4 };
+
+// Slots of the device scalar block.
+enum : int {
+  kScalMean = 0,     // mean density (FP64); 0 for the plain form
+  kScalC1 = 1,       // deviation form: N(mean + d) - N(mean) = d (c1 + d (c2 + d)) [+ log term]
+  kScalC2 = 2,
+  kScalInvMean = 3,  // 1 / mean (log model)
+  kScalN0 = 4,       // N(mean): constant dropped from the deviation nonlinearity
+  kScalLogMin = 5,   // log(min_phi) - log(mean) (clamped log, deviation form)
+  kScalZero = 6,     // always 0
+  kScalCorr = 7,     // mean correction of a materialised deviation field
+  kScalMuConst = 8,  // L_mu(0) mean + N(mean): constant part of mu in the deviation form
+  kScalCount = 12
+};
+
+// ---------------------------------------------------------------- compensated sums
+struct KSum {
+  double s, c;
+};
+__device__ __forceinline__ void ksum_add(KSum& a, double x) {
+  const double t = a.s + x;
+  if (fabs(a.s) >= fabs(x)) a.c += (a.s - t) + x; else a.c += (x - t) + a.s;
+  a.s = t;
+}
+__device__ __forceinline__ KSum ksum_merge(KSum a, KSum b) {
+  KSum r;
+  const double t = a.s + b.s;
+  const double bp = t - a.s;
+  const double e = (a.s - (t - bp)) + (b.s - bp);  // TwoSum error
+  r.s = t;
+  r.c = a.c + b.c + e;
+  return r;
+}
+
+// Deterministic block reduction of NQ compensated sums; thread 0 writes
+// (s, c) pairs to out[0 .. 2*NQ).
+template <int NQ>
+__device__ void block_reduce_store(KSum* v, double* out) {
+  __shared__ KSum red[32][NQ];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      KSum o;
+      o.s = __shfl_down_sync(0xffffffffu, v[q].s, off);
+      o.c = __shfl_down_sync(0xffffffffu, v[q].c, off);
+      v[q] = ksum_merge(v[q], o);
+    }
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) red[warp][q] = v[q];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      KSum acc = red[0][q];
+      for (int w = 1; w < nw; ++w) acc = ksum_merge(acc, red[w][q]);
+      out[2 * q] = acc.s;
+      out[2 * q + 1] = acc.c;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- nonlinearity
+// Plain FP64 form: the reference's expressions
+// (models/stdpfc/simulation.py:297, models/logpfc/simulation.py:296).
+template <int MODEL>
+__device__ __forceinline__ double nonlin_plain(double n, double g, int clamp, double min_phi, double min_log) {
+  const double n2 = n * n;
+  double r = g * n2 + n2 * n;
+  if (MODEL == kModelLog) r += (clamp && !(n > min_phi)) ? min_log : log(n);
+  return r;
+}
+
+// FP32 deviation form: N(mean + d) - N(mean). The log term is
+// log1p(d / mean); where 1 + d/mean < 1/8 it is evaluated in FP64.
+template <int MODEL>
+__device__ __forceinline__ float nonlin_dev(float d, float c1, float c2, float inv, double inv_d, int clamp,
+                                            double min_phi_rel, float log_min) {
+  float r = d * (c1 + d * (c2 + d));
+  if (MODEL == kModelLog) {
+    const float x = d * inv;
+    float l;
+    if (x > -0.875f) {
+      l = log1pf(x);
+    } else {
+      const double xd = (double)d * inv_d;   // near-singular branch in FP64
+      l = (clamp && !(1.0 + xd > min_phi_rel)) ? log_min : (float)log1p(xd);
+    }
+    r += l;
+  }
+  return r;
+}
+
+// ---------------------------------------------------------------- arguments
+template <class T>
+struct RowArgs {
+  int nx, ny, m, rows, tpf, ld;
+  FftDesc fft;
+  const cplx<T>* tw;
+  const cplx<T>* rtw;       // exp(-2 pi i k / nx), k < m
+  const cplx<T>* in;        // packed spectra [kx][y]
+  cplx<T>* out;             // packed spectra [kx][y]
+  const double* in_real;    // (ny, nx) FP64 (forward mode)
+  double* out_real;         // (ny, nx) FP64 (materialise mode)
+  const double* scal;       // device scalar block
+  const double* add;        // materialise: constant added (device pointer), may be null
+  double* partials;         // per-CTA compensated sums
+  int clamp;
+  double g, min_phi, min_log, epsilon;
+};
+
+template <class T>
+struct ColArgs {
+  int nx, ny, m, cols, tpf, ld, nyh;
+  FftDesc fft;
+  const cplx<T>* tw;
+  const cplx<T>* in;        // V (step/init/combine), n_hat (parseval/export)
+  const cplx<T>* nin;       // n_hat (step/combine)
+  cplx<T>* nout;            // n_hat' (step/init)
+  cplx<T>* wout;            // W' (step/init/combine)
+  const cplx<T>* coef;      // (A, Bg) pairs [kx][ky], kx <= m, ky <= ny/2
+  double* partials;
+  double* out_c128;         // export: (ny, m+1) complex128
+  int dev_form;             // deviation form: keep the DC of column 0 at zero
+  int combine;              // kCombine*
+  double scale;             // 1 / (nx ny)
+  double fx, fy;            // 1/(nx dx), 1/(ny dy): k = 2 pi idx f
+  double beta, q0, epsilon, w;  // L_mu, L_f, Gaussian width
+  const double* scal;       // device scalar block (export adds the deviation-form DC)
+};
+
+// wavenumber^2 of packed-column entry (kx, ky), numpy rfftfreq/fftfreq convention
+__device__ __forceinline__ double ksq(int kx, int ky, int ny, double fx, double fy) {
+  const double twopi = 6.283185307179586;
+  const int kys = (ky <= (ny - 1) / 2) ? ky : ky - ny;
+  const double kxp = twopi * ((double)kx * fx);
+  const double kyp = twopi * ((double)kys * fy);
+  return kxp * kxp + kyp * kyp;
+}
+
+// ---------------------------------------------------------------- row kernel
+// rows transforms of length m per CTA, tpf threads each; smem = rows * ld complex.
+template <class T, int MODE, int MODEL, int RSET>
+__global__ void PFC_LB row_kernel(RowArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int m = a.m, ny = a.ny, rows = a.rows, tpf = a.tpf, ld = a.ld;
+  const int y0 = blockIdx.x * rows;
+  const int f = threadIdx.x / tpf, lt = threadIdx.x - f * tpf;
+  const int y = y0 + f;
+  const bool valid = (y < ny);
+  cplx<T>* buf = sm + f * ld;
+  const bool dev = (sizeof(T) == 4);
+
+  if (MODE != kRowForward) {
+    // packed spectra, column-major [kx][y]: `rows` consecutive y per kx
+    for (int i = threadIdx.x; i < rows * m; i += blockDim.x) {
+      const int r = i % rows, kx = i / rows;
+      cplx<T> v = mk(T(0), T(0));
+      if (y0 + r < ny) v = a.in[(size_t)kx * ny + (y0 + r)];
+      sm[r * ld + kx] = v;
+    }
+    __syncthreads();
+    // pre-process pairs (k, m-k) of the inverse real transform
+    for (int k = lt; k <= m / 2; k += tpf) {
+      if (k == 0) {
+        const cplx<T> p = buf[0];
+        buf[0] = mk(p.x + p.y, p.x - p.y);
+      } else {
+        const int kk = m - k;
+        const cplx<T> xk = buf[k], xm = buf[kk];
+        const cplx<T> s = xk + conj(xm), d = xk - conj(xm);
+        const cplx<T> u = mul_i(cmul(conj(a.rtw[k]), d));
+        buf[k] = s + u;
+        if (kk != k) buf[kk] = conj(s - u);
+      }
+    }
+    __syncthreads();
+    fft_run<true, RSET>(buf, a.fft, a.tw, lt, tpf);
+    // buf[j] = x[2j] + i x[2j+1]
+  } else {
+    // real FP64 field (ny, nx), row-major; deviation form subtracts the mean
+    const double mean = dev ? a.scal[kScalMean] : 0.0;
+    const double2* src = reinterpret_cast<const double2*>(a.in_real + (size_t)y * a.nx);
+    for (int j = lt; j < m; j += tpf) {
+      cplx<T> v = mk(T(0), T(0));
+      if (valid) {
+        const double2 p = src[j];
+        v = mk((T)(p.x - mean), (T)(p.y - mean));
+      }
+      buf[j] = v;
+    }
+    __syncthreads();
+  }
+
+  if (MODE == kRowStep) {
+    if (dev) {
+      const float c1 = (float)a.scal[kScalC1], c2 = (float)a.scal[kScalC2];
+      const float inv = (float)a.scal[kScalInvMean];
+      const double inv_d = a.scal[kScalInvMean];
+      const double mphi_rel = a.min_phi * inv_d;
+      const float lmin = (float)a.scal[kScalLogMin];
+      for (int j = lt; j < m; j += tpf) {
+        const cplx<T> z = buf[j];
+        buf[j] = mk((T)nonlin_dev<MODEL>((float)z.x, c1, c2, inv, inv_d, a.clamp, mphi_rel, lmin),
+                    (T)nonlin_dev<MODEL>((float)z.y, c1, c2, inv, inv_d, a.clamp, mphi_rel, lmin));
+      }
+    } else {
+      for (int j = lt; j < m; j += tpf) {
+        const cplx<T> z = buf[j];
+        buf[j] = mk((T)nonlin_plain<MODEL>((double)z.x, a.g, a.clamp, a.min_phi, a.min_log),
+                    (T)nonlin_plain<MODEL>((double)z.y, a.g, a.clamp, a.min_phi, a.min_log));
+      }
+    }
+    __syncthreads();
+  }
+
+  if (MODE == kRowStep || MODE == kRowForward) {
+    fft_run<false, RSET>(buf, a.fft, a.tw, lt, tpf);
+    // post-process pairs (k, m-k) of the forward real transform
+    for (int k = lt; k <= m / 2; k += tpf) {
+      if (k == 0) {
+        const cplx<T> z = buf[0];
+        buf[0] = mk(z.x + z.y, z.x - z.y);
+      } else {
+        const int kk = m - k;
+        const cplx<T> zk = buf[k], zm = buf[kk];
+        const cplx<T> e = T(0.5) * (zk + conj(zm));
+        const cplx<T> o = T(0.5) * rot4<false>(zk - conj(zm));
+        const cplx<T> t = cmul(a.rtw[k], o);
+        buf[k] = e + t;
+        if (kk != k) buf[kk] = conj(e - t);
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < rows * m; i += blockDim.x) {
+      const int r = i % rows, kx = i / rows;
+      if (y0 + r < ny) a.out[(size_t)kx * ny + (y0 + r)] = sm[r * ld + kx];
+    }
+    return;
+  }
+
+  if (MODE == kRowMaterialize) {
+    const double add = a.add ? *a.add : 0.0;
+    KSum acc[1] = {{0.0, 0.0}};
+    if (valid) {
+      double2* dst = reinterpret_cast<double2*>(a.out_real + (size_t)y * a.nx);
+      for (int j = lt; j < m; j += tpf) {
+        const cplx<T> z = buf[j];
+        dst[j] = make_double2(add + (double)z.x, add + (double)z.y);
+        ksum_add(acc[0], (double)z.x);
+        ksum_add(acc[0], (double)z.y);
+      }
+    }
+    if (a.partials) block_reduce_store<1>(acc, a.partials + 2 * blockIdx.x);
+    return;
+  }
+
+  if (MODE == kRowReduce) {
+    // sums of: raw value (mean), free-energy polynomial, nonlinear mu
+    const double mean = dev ? a.scal[kScalMean] : 0.0;
+    const double eps = a.epsilon, g = a.g;
+    KSum acc[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    if (valid) {
+      for (int j = lt; j < m; j += tpf) {
+        const cplx<T> z = buf[j];
+        const double vv[2] = {(double)z.x, (double)z.y};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const double n = mean + vv[h];
+          const double n2 = n * n;
+          double fpoly = (eps / 2.0) * n2 + (g / 3.0) * (n2 * n) + (1 / 4.0) * (n2 * n2);
+          double nl = g * n2 + n2 * n;
+          if (MODEL == kModelLog) {
+            const double ln = (a.clamp && !(n > a.min_phi)) ? a.min_log : log(n);
+            fpoly = n * log(n) + fpoly;
+            nl += ln;
+          }
+          ksum_add(acc[0], vv[h]);
+          ksum_add(acc[1], fpoly);
+          ksum_add(acc[2], nl);
+        }
+      }
+    }
+    block_reduce_store<3>(acc, a.partials + 6 * blockIdx.x);
+  }
+}
+
+// ---------------------------------------------------------------- column kernel
+template <class T>
+__device__ __forceinline__ void unpack_pair(cplx<T> pk, cplx<T> pkp, cplx<T>& h0, cplx<T>& hm) {
+  h0 = T(0.5) * (pk + conj(pkp));
+  hm = T(0.5) * rot4<false>(pk - conj(pkp));
+}
+
+// cols transforms of length ny per CTA, tpf threads each; smem = cols * ld complex.
+template <class T, int MODE, int RSET>
+__global__ void PFC_LB col_kernel(ColArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int ny = a.ny, m = a.m, cols = a.cols, tpf = a.tpf, ld = a.ld, nyh = a.nyh;
+  const int c0 = blockIdx.x * cols;
+  const int f = threadIdx.x / tpf, lt = threadIdx.x - f * tpf;
+  const int kx = c0 + f;
+  const bool valid = kx < m;
+  cplx<T>* buf = sm + f * ld;
+
+  if (MODE == kColParseval || MODE == kColExport) {
+    // no transform: direct pass over n_hat
+    KSum acc[1] = {{0.0, 0.0}};
+    if (valid) {
+      const cplx<T>* col = a.in + (size_t)kx * ny;
+      for (int ky = lt; ky < ny; ky += tpf) {
+        const int kyp = ky == 0 ? 0 : ny - ky;
+        if (kx == 0) {
+          cplx<T> h0, hm;
+          unpack_pair(col[ky], col[kyp], h0, hm);
+          if (MODE == kColParseval) {
+            const double k0 = ksq(0, ky, ny, a.fx, a.fy), kM = ksq(m, ky, ny, a.fx, a.fy);
+            const double l0 = (a.beta / 2.0) * (a.q0 * a.q0 - k0) * (a.q0 * a.q0 - k0);
+            const double lM = (a.beta / 2.0) * (a.q0 * a.q0 - kM) * (a.q0 * a.q0 - kM);
+            ksum_add(acc[0], l0 * ((double)h0.x * h0.x + (double)h0.y * h0.y));
+            ksum_add(acc[0], lM * ((double)hm.x * hm.x + (double)hm.y * hm.y));
+          } else {
+            double* o = a.out_c128 + 2 * ((size_t)ky * (m + 1));
+            double dc = 0.0;
+            if (a.dev_form && ky == 0) dc = a.scal[kScalMean] * ((double)a.nx * (double)a.ny);
+            o[0] = (double)h0.x + dc; o[1] = h0.y;
+            o[2 * m] = hm.x; o[2 * m + 1] = hm.y;
+          }
+        } else {
+          const cplx<T> v = col[ky];
+          if (MODE == kColParseval) {
+            const double k2 = ksq(kx, ky, ny, a.fx, a.fy);
+            const double l = (a.beta / 2.0) * (a.q0 * a.q0 - k2) * (a.q0 * a.q0 - k2);
+            ksum_add(acc[0], 2.0 * l * ((double)v.x * v.x + (double)v.y * v.y));
+          } else {
+            double* o = a.out_c128 + 2 * ((size_t)ky * (m + 1) + kx);
+            o[0] = v.x; o[1] = v.y;
+          }
+        }
+      }
+    }
+    if (MODE == kColParseval) block_reduce_store<1>(acc, a.partials + 2 * blockIdx.x);
+    return;
+  }
+
+  const bool need_v = !(MODE == kColCombine && a.combine == kCombineLocalN);
+  if (need_v) {
+    // contiguous columns c0 .. c0+cols-1
+    for (int i = threadIdx.x; i < cols * ny; i += blockDim.x) {
+      const int c = i / ny, ky = i - c * ny;
+      cplx<T> v = mk(T(0), T(0));
+      if (c0 + c < m) v = a.in[(size_t)c0 * ny + i];
+      sm[c * ld + ky] = v;
+    }
+    __syncthreads();
+    fft_run<false, RSET>(buf, a.fft, a.tw, lt, tpf);
+  }
+
+  if (MODE == kColInit) {
+    if (valid) {
+      cplx<T>* out = a.nout + (size_t)kx * ny;
+      for (int ky = lt; ky < ny; ky += tpf) {
+        cplx<T> v = buf[ky];
+        if (a.dev_form && kx == 0 && ky == 0) { v.x = T(0); buf[0] = v; }
+        out[ky] = v;
+      }
+    }
+    __syncthreads();
+  } else if (MODE == kColStep) {
+    if (valid) {
+      const cplx<T>* nin = a.nin + (size_t)kx * ny;
+      cplx<T>* nout = a.nout + (size_t)kx * ny;
+      for (int ky = lt; ky <= ny / 2; ky += tpf) {
+        const int kyp = ky == 0 ? 0 : ny - ky;
+        const cplx<T> qk = buf[ky], qkp = buf[kyp];
+        const cplx<T> pk = nin[ky], pkp = nin[kyp];
+        cplx<T> ok, okp;
+        if (kx == 0) {
+          const cplx<T> c0v = a.coef[ky], cMv = a.coef[(size_t)m * nyh + ky];
+          cplx<T> h0, hm, g0, gm;
+          unpack_pair(pk, pkp, h0, hm);
+          unpack_pair(qk, qkp, g0, gm);
+          const cplx<T> h0n = c0v.x * h0 + c0v.y * g0;
+          const cplx<T> hmn = cMv.x * hm + cMv.y * gm;
+          ok = h0n + mul_i(hmn);
+          okp = conj(h0n) + mul_i(conj(hmn));
+        } else {
+          const cplx<T> c = a.coef[(size_t)kx * nyh + ky];
+          ok = c.x * pk + c.y * qk;
+          okp = c.x * pkp + c.y * qkp;
+        }
+        nout[ky] = ok;
+        buf[ky] = ok;
+        if (kyp != ky) { nout[kyp] = okp; buf[kyp] = okp; }
+      }
+    }
+    __syncthreads();
+  } else if (MODE == kColCombine) {
+    // mu_hat = L_mu n_hat + N_hat (optionally Gaussian-filtered), or G n_hat, or N_hat
+    if (valid) {
+      const cplx<T>* nin = a.nin + (size_t)kx * ny;
+      const double q2 = a.q0 * a.q0;
+      for (int ky = lt; ky <= ny / 2; ky += tpf) {
+        const int kyp = ky == 0 ? 0 : ny - ky;
+        // multipliers for n_hat and N_hat at (kx, ky) and, for the packed column, (m, ky)
+        double mn[2], mq[2];
+        for (int h = 0; h < (kx == 0 ? 2 : 1); ++h) {
+          const int kxx = (h == 0) ? kx : m;
+          const double k2 = ksq(kxx, ky, ny, a.fx, a.fy);
+          const double lmu = a.beta * (q2 - k2) * (q2 - k2) + a.epsilon;
+          const double gs = exp(-k2 * a.w * a.w / 2);
+          switch (a.combine) {
+            case kCombineMu: mn[h] = lmu; mq[h] = 1.0; break;
+            case kCombineLocalMu: mn[h] = gs * lmu; mq[h] = gs; break;
+            case kCombineLocalN: mn[h] = gs; mq[h] = 0.0; break;
+            case kCombineNonlin: mn[h] = 0.0; mq[h] = 1.0; break;
+            default: mn[h] = 1.0; mq[h] = 0.0; break;
+          }
+        }
+        const cplx<T> pk = nin[ky], pkp = nin[kyp];
+        cplx<T> qk = mk(T(0), T(0)), qkp = qk;
+        if (need_v) { qk = buf[ky]; qkp = buf[kyp]; }
+        cplx<T> ok, okp;
+        if (kx == 0) {
+          cplx<T> h0, hm, g0, gm;
+          unpack_pair(pk, pkp, h0, hm);
+          unpack_pair(qk, qkp, g0, gm);
+          const cplx<T> h0n = (T)mn[0] * h0 + (T)mq[0] * g0;
+          const cplx<T> hmn = (T)mn[1] * hm + (T)mq[1] * gm;
+          ok = h0n + mul_i(hmn);
+          okp = conj(h0n) + mul_i(conj(hmn));
+        } else {
+          ok = (T)mn[0] * pk + (T)mq[0] * qk;
+          okp = (T)mn[0] * pkp + (T)mq[0] * qkp;
+        }
+        buf[ky] = ok;
+        if (kyp != ky) buf[kyp] = okp;
+      }
+    }
+    __syncthreads();
+  }
+
+  fft_run<true, RSET>(buf, a.fft, a.tw, lt, tpf);
+  const T s = (T)a.scale;
+  for (int i = threadIdx.x; i < cols * ny; i += blockDim.x) {
+    const int c = i / ny, ky = i - c * ny;
+    if (c0 + c < m) {
+      const cplx<T> v = sm[c * ld + ky];
+      a.wout[(size_t)c0 * ny + i] = mk(s * v.x, s * v.y);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- small kernels
+// Final reduction of per-CTA compensated partials, in a fixed order.
+// row partials: 3 sums (raw, fpoly, nonlin) x nrow; col partials: 1 sum x ncol.
+// out3 = {F per site, mu per site, mean}.
+__global__ void finalize_reduce_kernel(const double* rowp, int nrow, const double* colp, int ncol,
+                                       const double* scal, double inv_sites, double lmu0, double lf0,
+                                       int dev_form, double* out3, int* status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  KSum q[3] = {{0, 0}, {0, 0}, {0, 0}};
+  for (int b = 0; b < nrow; ++b)
+    for (int k = 0; k < 3; ++k) {
+      KSum o = {rowp[6 * b + 2 * k], rowp[6 * b + 2 * k + 1]};
+      q[k] = ksum_merge(q[k], o);
+    }
+  KSum p = {0, 0};
+  for (int b = 0; b < ncol; ++b) {
+    KSum o = {colp[2 * b], colp[2 * b + 1]};
+    p = ksum_merge(p, o);
+  }
+  const double mean_dev = dev_form ? scal[kScalMean] : 0.0;
+  const double raw_mean = (q[0].s + q[0].c) * inv_sites;
+  double grad = (p.s + p.c) * inv_sites * inv_sites;
+  if (dev_form) grad += lf0 * mean_dev * mean_dev;   // k = 0 term carried in FP64
+  const double F = grad + (q[1].s + q[1].c) * inv_sites;
+  const double mean = dev_form ? mean_dev : raw_mean;
+  const double mu = lmu0 * mean + (q[2].s + q[2].c) * inv_sites;
+  out3[0] = F;
+  out3[1] = mu;
+  out3[2] = mean;
+  if (!isfinite(F) || !isfinite(mu) || !isfinite(raw_mean)) atomicOr(status, 1);
+}
+
+// Sum of materialise partials -> scal[kScalCorr] = sum / sites (deviation mean correction).
+__global__ void finalize_mean_kernel(const double* p, int nb, double inv_sites, double* scal) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  KSum acc = {0, 0};
+  for (int b = 0; b < nb; ++b) {
+    KSum o = {p[2 * b], p[2 * b + 1]};
+    acc = ksum_merge(acc, o);
+  }
+  scal[kScalCorr] = (acc.s + acc.c) * inv_sites;
+}
+
+__global__ void shift_kernel(double* x, size_t n, const double* by) {
+  const double s = *by;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    x[i] -= s;
+}
+
+// Compensated sum of a real field (grid-stride), per-CTA partials.
+__global__ void field_sum_kernel(const double* x, size_t n, double* partials) {
+  KSum acc[1] = {{0.0, 0.0}};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    ksum_add(acc[0], x[i]);
+  block_reduce_store<1>(acc, partials + 2 * blockIdx.x);
+}
+
+// Deviation-form scalars from the mean (std and log nonlinearities).
+__global__ void set_scalars_kernel(const double* p, int nb, double inv_sites, int model, double g,
+                                   double min_phi, double lmu0, double* scal) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  KSum acc = {0, 0};
+  for (int b = 0; b < nb; ++b) {
+    KSum o = {p[2 * b], p[2 * b + 1]};
+    acc = ksum_merge(acc, o);
+  }
+  const double mu = (acc.s + acc.c) * inv_sites;
+  scal[kScalMean] = mu;
+  scal[kScalC1] = 2.0 * g * mu + 3.0 * mu * mu;
+  scal[kScalC2] = g + 3.0 * mu;
+  scal[kScalInvMean] = (mu != 0.0) ? 1.0 / mu : 0.0;
+  double n0 = g * mu * mu + mu * mu * mu;
+  if (model == kModelLog) n0 += log(mu);
+  scal[kScalN0] = n0;
+  scal[kScalLogMin] = (model == kModelLog && min_phi > 0.0 && mu > 0.0) ? log(min_phi) - log(mu) : 0.0;
+  scal[kScalZero] = 0.0;
+  scal[kScalCorr] = 0.0;
+  scal[kScalMuConst] = lmu0 * mu + n0;
+}
+
+}  // namespace pfc

@@ -1,0 +1,719 @@
+// Host side of the C ABI declared in include/pfc_b200.h: plan construction
+// (factorisation, twiddles, FP64 ETD1 coefficients, launch shapes), buffer
+// ownership and the launch sequences of each entry point.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "pfc_b200.h"
+#include "pfc_kernels.cuh"
+
+using namespace pfc;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define PFC_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(PFC_E_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
+                  __FILE__, __LINE__);                                                  \
+  } while (0)
+
+#define PFC_LAUNCHED()                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = cudaGetLastError();                                                \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(PFC_E_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), \
+                  __FILE__, __LINE__);                                                  \
+  } while (0)
+
+// Largest radix first for the power-of-two part (16 in FP32, 8 in FP64, which
+// bounds the registers one butterfly needs), then the odd primes.
+bool factorize(int n, bool fp32, std::vector<int>& radices) {
+  radices.clear();
+  int p2 = 0;
+  while (n % 2 == 0) { n /= 2; ++p2; }
+  if (fp32)
+    while (p2 >= 4) { radices.push_back(16); p2 -= 4; }
+  while (p2 >= 3) { radices.push_back(8); p2 -= 3; }
+  if (p2 == 2) radices.push_back(4);
+  if (p2 == 1) radices.push_back(2);
+  for (int r : {3, 5, 7, 11, 13})
+    while (n % r == 0) { radices.push_back(r); n /= r; }
+  return n == 1 && (int)radices.size() <= kMaxPass;
+}
+
+constexpr int kBlockMax = 256;  // PFC_LB in pfc_kernels.cuh
+constexpr int kMaxElemsF = PFC_MAXE_F, kMaxElemsD = PFC_MAXE_D;  // as MaxElems in pfc_fft.cuh
+
+// must match MaxBfly in pfc_fft.cuh
+int max_bfly(int radix, bool fp32) {
+  if (radix % 2 == 1 && radix > 3) return 1;
+  const int e = fp32 ? kMaxElemsF : kMaxElemsD;
+  return e / radix > 0 ? e / radix : 1;
+}
+
+bool all_pow2(const std::vector<int>& radices) {
+  for (int r : radices)
+    if (r & (r - 1)) return false;
+  return true;
+}
+
+// Appends the pass tables of an n-point transform to `tw` (complex, long double
+// accuracy rounded once) and fills `d`.
+void build_fft(int n, const std::vector<int>& radices, std::vector<long double>& tw, FftDesc& d) {
+  const long double twopi = 6.283185307179586476925286766559L;
+  d.n = n;
+  d.npass = (int)radices.size();
+  int ns = 1;
+  for (int p = 0; p < d.npass; ++p) {
+    const int R = radices[p];
+    d.radix[p] = R;
+    d.ns[p] = ns;
+    d.twoff[p] = (int)(tw.size() / 2);
+    for (int k = 0; k < ns; ++k)
+      for (int q = 1; q < R; ++q) {
+        const long long num = (long long)q * k % ((long long)ns * R);
+        const long double ang = -twopi * (long double)num / (long double)(ns * R);
+        tw.push_back(cosl(ang));
+        tw.push_back(sinl(ang));
+      }
+    if (R >= 5) {
+      d.rootoff[p] = (int)(tw.size() / 2);
+      for (int mm = 0; mm < R; ++mm) {
+        const long double ang = -twopi * (long double)mm / (long double)R;
+        tw.push_back(cosl(ang));
+        tw.push_back(sinl(ang));
+      }
+    } else {
+      d.rootoff[p] = -1;
+    }
+    ns *= R;
+  }
+  for (int p = d.npass; p < kMaxPass; ++p) { d.radix[p] = 0; d.ns[p] = 0; d.twoff[p] = 0; d.rootoff[p] = -1; }
+}
+
+int threads_per_fft(const std::vector<int>& radices, int n, bool fp32) {
+  int need = 1;
+  for (int R : radices) {
+    const int nr = n / R;
+    const int mb = max_bfly(R, fp32);
+    need = std::max(need, (nr + mb - 1) / mb);
+  }
+  int t = 1;
+  while (t < need) t <<= 1;
+  return t;
+}
+
+}  // namespace
+
+struct pfc_plan {
+  pfc_problem prob;
+  int device = 0;
+  bool fp32 = false;
+  int nx = 0, ny = 0, m = 0, nyh = 0;
+  size_t nspec = 0;     // m * ny complex elements per spectral array
+  size_t elt = 0;       // bytes per complex element
+  // device buffers
+  void* nhat[2] = {nullptr, nullptr};
+  void* W = nullptr;
+  void* V = nullptr;
+  void* W2 = nullptr;
+  void* coef = nullptr;
+  void* tw = nullptr;
+  double* partials = nullptr;
+  size_t npartials = 0;
+  double* scal = nullptr;
+  int* status = nullptr;
+  // transforms and launch shapes
+  FftDesc rowfft{}, colfft{};
+  int rt_off = 0;       // offset of the real-packing twiddles in tw
+  int row_tpf = 0, rows = 0, row_ld = 0, row_grid = 0, row_rset = kRadixPow2;
+  int col_tpf = 0, cols = 0, col_ld = 0, col_grid = 0, col_rset = kRadixPow2;
+  size_t row_smem = 0, col_smem = 0;
+  int cur = 0;
+  bool state_set = false;
+  long long steps_since_set = 0;
+  long long launches = 0;
+  std::vector<double> hostA, hostBg;  // FP64 coefficients, (ny, m+1)
+  double lmu0 = 0, lf0 = 0;
+};
+
+namespace {
+
+template <class T>
+RowArgs<T> row_args(const pfc_plan* h) {
+  RowArgs<T> a{};
+  a.nx = h->nx; a.ny = h->ny; a.m = h->m; a.rows = h->rows; a.tpf = h->row_tpf; a.ld = h->row_ld;
+  a.fft = h->rowfft;
+  a.tw = reinterpret_cast<const cplx<T>*>(h->tw);
+  a.rtw = reinterpret_cast<const cplx<T>*>(h->tw) + h->rt_off;
+  a.scal = h->scal;
+  a.clamp = h->prob.clamp_log;
+  a.g = h->prob.g;
+  a.min_phi = h->prob.min_phi;
+  a.min_log = (h->prob.min_phi > 0) ? std::log(h->prob.min_phi) : -INFINITY;
+  a.epsilon = h->prob.epsilon;
+  return a;
+}
+
+template <class T>
+ColArgs<T> col_args(const pfc_plan* h) {
+  ColArgs<T> a{};
+  a.nx = h->nx; a.ny = h->ny; a.m = h->m; a.cols = h->cols; a.tpf = h->col_tpf; a.ld = h->col_ld;
+  a.nyh = h->nyh;
+  a.fft = h->colfft;
+  a.tw = reinterpret_cast<const cplx<T>*>(h->tw);
+  a.coef = reinterpret_cast<const cplx<T>*>(h->coef);
+  a.dev_form = h->fp32 ? 1 : 0;
+  a.scale = 1.0 / ((double)h->nx * (double)h->ny);
+  const double dx = h->prob.lx / h->nx, dy = h->prob.ly / h->ny;
+  a.fx = 1.0 / (h->nx * dx);
+  a.fy = 1.0 / (h->ny * dy);
+  a.beta = h->prob.beta; a.q0 = h->prob.q0; a.epsilon = h->prob.epsilon;
+  a.scal = h->scal;
+  return a;
+}
+
+// The nonlinearity only matters in the step and reduce modes; other modes use the std instance.
+template <int MODE> constexpr bool row_uses_model() { return MODE == kRowStep || MODE == kRowReduce; }
+
+template <class T, int MODE, int MODEL, int RSET>
+void* row_fn() { return (void*)row_kernel<T, MODE, MODEL, RSET>; }
+
+template <class T, int MODE>
+void* pick_row(int model, int rset) {
+  const bool log = row_uses_model<MODE>() && model == kModelLog;
+  if (rset == kRadixPow2) return log ? row_fn<T, MODE, kModelLog, kRadixPow2>() : row_fn<T, MODE, kModelStd, kRadixPow2>();
+  return log ? row_fn<T, MODE, kModelLog, kRadixAll>() : row_fn<T, MODE, kModelStd, kRadixAll>();
+}
+
+template <class T, int MODE>
+void* pick_col(int rset) {
+  if (MODE == kColParseval || MODE == kColExport || rset == kRadixPow2) return (void*)col_kernel<T, MODE, kRadixPow2>;
+  return (void*)col_kernel<T, MODE, kRadixAll>;
+}
+
+template <class T, int MODE>
+int launch_row(pfc_plan* h, const RowArgs<T>& a, cudaStream_t s) {
+  void* fn = pick_row<T, MODE>(h->prob.model, h->row_rset);
+  void* args[] = {(void*)&a};
+  cudaError_t e = cudaLaunchKernel(fn, dim3(h->row_grid), dim3(h->rows * h->row_tpf), args, h->row_smem, s);
+  ++h->launches;
+  if (e != cudaSuccess) return fail(PFC_E_CUDA, "row kernel launch failed: %s", cudaGetErrorString(e));
+  return PFC_OK;
+}
+
+template <class T, int MODE>
+int launch_col(pfc_plan* h, const ColArgs<T>& a, cudaStream_t s) {
+  void* fn = pick_col<T, MODE>(h->col_rset);
+  void* args[] = {(void*)&a};
+  cudaError_t e = cudaLaunchKernel(fn, dim3(h->col_grid), dim3(h->cols * h->col_tpf), args, h->col_smem, s);
+  ++h->launches;
+  if (e != cudaSuccess) return fail(PFC_E_CUDA, "column kernel launch failed: %s", cudaGetErrorString(e));
+  return PFC_OK;
+}
+
+template <class T>
+int set_smem_attrs(pfc_plan* h) {
+#define PFC_ATTR(fn, bytes) PFC_CUDA(cudaFuncSetAttribute((const void*)(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(bytes)))
+  const int md = h->prob.model, rr = h->row_rset, cr = h->col_rset;
+  PFC_ATTR((pick_row<T, kRowStep>(md, rr)), h->row_smem);
+  PFC_ATTR((pick_row<T, kRowForward>(md, rr)), h->row_smem);
+  PFC_ATTR((pick_row<T, kRowMaterialize>(md, rr)), h->row_smem);
+  PFC_ATTR((pick_row<T, kRowReduce>(md, rr)), h->row_smem);
+  PFC_ATTR((pick_col<T, kColStep>(cr)), h->col_smem);
+  PFC_ATTR((pick_col<T, kColInit>(cr)), h->col_smem);
+  PFC_ATTR((pick_col<T, kColCombine>(cr)), h->col_smem);
+  PFC_ATTR((pick_col<T, kColParseval>(cr)), h->col_smem);
+  PFC_ATTR((pick_col<T, kColExport>(cr)), h->col_smem);
+#undef PFC_ATTR
+  return PFC_OK;
+}
+
+// ---- entry point bodies, templated on the working precision
+template <class T>
+int do_set_state(pfc_plan* h, const double* field, cudaStream_t s) {
+  const size_t sites = (size_t)h->nx * h->ny;
+  if (h->fp32) {
+    field_sum_kernel<<<256, 256, 0, s>>>(field, sites, h->partials);
+    ++h->launches;
+    PFC_LAUNCHED();
+    set_scalars_kernel<<<1, 32, 0, s>>>(h->partials, 256, 1.0 / (double)sites, h->prob.model, h->prob.g,
+                                        h->prob.min_phi, h->lmu0, h->scal);
+    ++h->launches;
+    PFC_LAUNCHED();
+  }
+  RowArgs<T> ra = row_args<T>(h);
+  ra.in_real = field;
+  ra.out = reinterpret_cast<cplx<T>*>(h->V);
+  int rc = launch_row<T, kRowForward>(h, ra, s);
+  if (rc) return rc;
+  ColArgs<T> ca = col_args<T>(h);
+  ca.in = reinterpret_cast<const cplx<T>*>(h->V);
+  ca.nout = reinterpret_cast<cplx<T>*>(h->nhat[h->cur]);
+  ca.wout = reinterpret_cast<cplx<T>*>(h->W);
+  rc = launch_col<T, kColInit>(h, ca, s);
+  if (rc) return rc;
+  h->state_set = true;
+  h->steps_since_set = 0;
+  return PFC_OK;
+}
+
+template <class T>
+int do_step(pfc_plan* h, long long nsteps, cudaStream_t s) {
+  RowArgs<T> ra = row_args<T>(h);
+  ra.in = reinterpret_cast<const cplx<T>*>(h->W);
+  ra.out = reinterpret_cast<cplx<T>*>(h->V);
+  ColArgs<T> ca = col_args<T>(h);
+  ca.in = reinterpret_cast<const cplx<T>*>(h->V);
+  ca.wout = reinterpret_cast<cplx<T>*>(h->W);
+  for (long long i = 0; i < nsteps; ++i) {
+    int rc = launch_row<T, kRowStep>(h, ra, s);
+    if (rc) return rc;
+    ca.nin = reinterpret_cast<const cplx<T>*>(h->nhat[h->cur]);
+    ca.nout = reinterpret_cast<cplx<T>*>(h->nhat[h->cur ^ 1]);
+    rc = launch_col<T, kColStep>(h, ca, s);
+    if (rc) return rc;
+    h->cur ^= 1;
+    ++h->steps_since_set;
+  }
+  return PFC_OK;
+}
+
+template <class T>
+int do_step_timed(pfc_plan* h, long long nsteps, double* ms_row, double* ms_col, cudaStream_t s) {
+  std::vector<cudaEvent_t> ev(3 * (size_t)nsteps, nullptr);
+  int rc = PFC_OK;
+  for (auto& e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) { rc = fail(PFC_E_CUDA, "cudaEventCreate failed"); break; }
+  RowArgs<T> ra = row_args<T>(h);
+  ra.in = reinterpret_cast<const cplx<T>*>(h->W);
+  ra.out = reinterpret_cast<cplx<T>*>(h->V);
+  ColArgs<T> ca = col_args<T>(h);
+  ca.in = reinterpret_cast<const cplx<T>*>(h->V);
+  ca.wout = reinterpret_cast<cplx<T>*>(h->W);
+  for (long long i = 0; i < nsteps && rc == PFC_OK; ++i) {
+    cudaEventRecord(ev[3 * i], s);
+    rc = launch_row<T, kRowStep>(h, ra, s);
+    if (rc) break;
+    cudaEventRecord(ev[3 * i + 1], s);
+    ca.nin = reinterpret_cast<const cplx<T>*>(h->nhat[h->cur]);
+    ca.nout = reinterpret_cast<cplx<T>*>(h->nhat[h->cur ^ 1]);
+    rc = launch_col<T, kColStep>(h, ca, s);
+    if (rc) break;
+    cudaEventRecord(ev[3 * i + 2], s);
+    h->cur ^= 1;
+    ++h->steps_since_set;
+  }
+  double tr = 0, tc = 0;
+  if (rc == PFC_OK) {
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = fail(PFC_E_CUDA, "pfc_step_timed: %s", cudaGetErrorString(e));
+    for (long long i = 0; i < nsteps && rc == PFC_OK; ++i) {
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]);
+      cudaEventElapsedTime(&b, ev[3 * i + 1], ev[3 * i + 2]);
+      tr += a; tc += b;
+    }
+  }
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  if (ms_row) *ms_row = tr;
+  if (ms_col) *ms_col = tc;
+  return rc;
+}
+
+template <class T>
+int do_materialize(pfc_plan* h, const void* spec, const double* add, double* out, bool correct_mean,
+                   cudaStream_t s) {
+  RowArgs<T> ra = row_args<T>(h);
+  ra.in = reinterpret_cast<const cplx<T>*>(spec);
+  ra.out_real = out;
+  ra.add = add;
+  ra.partials = correct_mean ? h->partials : nullptr;
+  int rc = launch_row<T, kRowMaterialize>(h, ra, s);
+  if (rc) return rc;
+  if (correct_mean) {
+    const size_t sites = (size_t)h->nx * h->ny;
+    finalize_mean_kernel<<<1, 32, 0, s>>>(h->partials, h->row_grid, 1.0 / (double)sites, h->scal);
+    ++h->launches;
+    PFC_LAUNCHED();
+    shift_kernel<<<1024, 256, 0, s>>>(out, sites, h->scal + kScalCorr);
+    ++h->launches;
+    PFC_LAUNCHED();
+  }
+  return PFC_OK;
+}
+
+template <class T>
+int do_get_state(pfc_plan* h, double* out, cudaStream_t s) {
+  return do_materialize<T>(h, h->W, h->scal + (h->fp32 ? kScalMean : kScalZero), out, h->fp32, s);
+}
+
+template <class T>
+int do_reduce(pfc_plan* h, double* out3, cudaStream_t s) {
+  double* rowp = h->partials;
+  double* colp = h->partials + 6 * (size_t)h->row_grid;
+  RowArgs<T> ra = row_args<T>(h);
+  ra.in = reinterpret_cast<const cplx<T>*>(h->W);
+  ra.partials = rowp;
+  int rc = launch_row<T, kRowReduce>(h, ra, s);
+  if (rc) return rc;
+  ColArgs<T> ca = col_args<T>(h);
+  ca.in = reinterpret_cast<const cplx<T>*>(h->nhat[h->cur]);
+  ca.partials = colp;
+  rc = launch_col<T, kColParseval>(h, ca, s);
+  if (rc) return rc;
+  const double sites = (double)h->nx * (double)h->ny;
+  finalize_reduce_kernel<<<1, 32, 0, s>>>(rowp, h->row_grid, colp, h->col_grid, h->scal, 1.0 / sites, h->lmu0,
+                                          h->lf0, h->fp32 ? 1 : 0, out3, h->status);
+  ++h->launches;
+  PFC_LAUNCHED();
+  return PFC_OK;
+}
+
+// Nonlinear row spectra V of the "previous" state, and that state's n_hat.
+template <class T>
+int prepare_previous(pfc_plan* h, bool current, const void** nhat_old, cudaStream_t s) {
+  if (h->steps_since_set > 0 && !current) {
+    *nhat_old = h->nhat[h->cur ^ 1];
+    return PFC_OK;
+  }
+  RowArgs<T> ra = row_args<T>(h);
+  ra.in = reinterpret_cast<const cplx<T>*>(h->W);
+  ra.out = reinterpret_cast<cplx<T>*>(h->V);
+  int rc = launch_row<T, kRowStep>(h, ra, s);
+  if (rc) return rc;
+  *nhat_old = h->nhat[h->cur];
+  return PFC_OK;
+}
+
+template <class T>
+int do_get_field(pfc_plan* h, int which, double w, double* out, cudaStream_t s) {
+  const bool current = (which & PFC_FIELD_OF_CURRENT) != 0;
+  which &= ~PFC_FIELD_OF_CURRENT;
+  if (which == PFC_FIELD_N) return do_get_state<T>(h, out, s);
+  if (!h->W2) {
+    PFC_CUDA(cudaMalloc(&h->W2, h->nspec * h->elt));
+  }
+  const void* nold = nullptr;
+  int rc = prepare_previous<T>(h, current, &nold, s);
+  if (rc) return rc;
+  ColArgs<T> ca = col_args<T>(h);
+  ca.in = reinterpret_cast<const cplx<T>*>(h->V);
+  ca.nin = reinterpret_cast<const cplx<T>*>(nold);
+  ca.wout = reinterpret_cast<cplx<T>*>(h->W2);
+  ca.w = w;
+  int addslot = kScalZero;
+  switch (which) {
+    case PFC_FIELD_MU: ca.combine = kCombineMu; addslot = h->fp32 ? kScalMuConst : kScalZero; break;
+    case PFC_FIELD_LOCAL_MU: ca.combine = kCombineLocalMu; addslot = h->fp32 ? kScalMuConst : kScalZero; break;
+    case PFC_FIELD_LOCAL_N: ca.combine = kCombineLocalN; addslot = h->fp32 ? kScalMean : kScalZero; break;
+    case PFC_FIELD_NONLIN_MU: ca.combine = kCombineNonlin; addslot = h->fp32 ? kScalN0 : kScalZero; break;
+    default: return fail(PFC_E_ARG, "pfc_get_field: unknown field %d", which);
+  }
+  rc = launch_col<T, kColCombine>(h, ca, s);
+  if (rc) return rc;
+  return do_materialize<T>(h, h->W2, h->scal + addslot, out, false, s);
+}
+
+template <class T>
+int do_get_spectrum(pfc_plan* h, int which, double* out, cudaStream_t s) {
+  const void* src = h->nhat[h->cur];
+  if (which == PFC_SPEC_N_HAT && h->steps_since_set > 0) src = h->nhat[h->cur ^ 1];
+  ColArgs<T> ca = col_args<T>(h);
+  ca.in = reinterpret_cast<const cplx<T>*>(src);
+  ca.out_c128 = out;
+  int rc = launch_col<T, kColExport>(h, ca, s);
+  if (rc) return rc;
+  return PFC_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- C ABI
+extern "C" {
+
+int pfc_abi_version(void) { return PFC_ABI_VERSION; }
+
+int pfc_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return PFC_E_ARG;
+  snprintf(buf, len, "%s", g_last_error.c_str());
+  return PFC_OK;
+}
+
+int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
+  if (!p || !out) return fail(PFC_E_ARG, "pfc_plan_create: null argument");
+  *out = nullptr;
+  if (p->nx < 4 || p->ny < 2 || (p->nx & 1))
+    return fail(PFC_E_ARG, "pfc_plan_create: nx must be even and >= 4, ny >= 2 (got %d x %d)", p->nx, p->ny);
+  if (p->model != PFC_MODEL_STD && p->model != PFC_MODEL_LOG)
+    return fail(PFC_E_ARG, "pfc_plan_create: unknown model %d", p->model);
+  if (p->precision != PFC_FP64_PLAIN && p->precision != PFC_FP32_MIXED)
+    return fail(PFC_E_ARG, "pfc_plan_create: unknown precision %d", p->precision);
+  if (!(p->lx > 0) || !(p->ly > 0) || !(p->dt > 0))
+    return fail(PFC_E_ARG, "pfc_plan_create: lx, ly, dt must be positive");
+  std::vector<int> rrow, rcol;
+  const int m = p->nx / 2;
+  const bool fp32 = (p->precision == PFC_FP32_MIXED);
+  if (!factorize(m, fp32, rrow))
+    return fail(PFC_E_ARG, "pfc_plan_create: nx/2 = %d has a prime factor other than 2,3,5,7,11,13", m);
+  if (!factorize(p->ny, fp32, rcol))
+    return fail(PFC_E_ARG, "pfc_plan_create: ny = %d has a prime factor other than 2,3,5,7,11,13", p->ny);
+
+  pfc_plan* h = new pfc_plan();
+  h->prob = *p;
+  h->fp32 = (p->precision == PFC_FP32_MIXED);
+  h->nx = p->nx; h->ny = p->ny; h->m = m; h->nyh = p->ny / 2 + 1;
+  h->nspec = (size_t)m * p->ny;
+  h->row_rset = all_pow2(rrow) ? kRadixPow2 : kRadixAll;
+  h->col_rset = all_pow2(rcol) ? kRadixPow2 : kRadixAll;
+  h->elt = h->fp32 ? sizeof(float2) : sizeof(double2);
+  cudaGetDevice(&h->device);
+
+  auto cleanup_fail = [&](int rc) { pfc_plan_destroy(h); return rc; };
+
+  // ---- twiddles: row passes, column passes, real-packing table
+  std::vector<long double> tw;
+  build_fft(m, rrow, tw, h->rowfft);
+  build_fft(p->ny, rcol, tw, h->colfft);
+  h->rt_off = (int)(tw.size() / 2);
+  {
+    const long double twopi = 6.283185307179586476925286766559L;
+    for (int k = 0; k < m; ++k) {
+      const long double ang = -twopi * (long double)k / (long double)p->nx;
+      tw.push_back(cosl(ang));
+      tw.push_back(sinl(ang));
+    }
+  }
+
+  // ---- launch shapes
+  const int cbytes = (int)h->elt;
+  int smem_opt = 0;
+  cudaDeviceGetAttribute(&smem_opt, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  if (smem_opt <= 0) smem_opt = 227 * 1024;
+  const int budget = std::min(smem_opt - 8 * 1024, 200 * 1024);
+  {
+    h->row_tpf = threads_per_fft(rrow, m, h->fp32);
+    h->row_ld = m + 1;
+    int rows = std::max(1, 32 / h->row_tpf);                 // whole warps
+    const int coalesce = std::max(1, 64 / cbytes);           // >= 64 B per kx run
+    while (rows < coalesce) rows *= 2;
+    while (2 * rows * h->row_tpf <= kBlockMax && (size_t)(2 * rows) * h->row_ld * cbytes <= (size_t)budget / 2 && rows < p->ny)
+      rows *= 2;
+    while ((size_t)rows * h->row_ld * cbytes > (size_t)budget && rows > std::max(1, 32 / h->row_tpf)) rows /= 2;
+    if ((size_t)rows * h->row_ld * cbytes > (size_t)budget || rows * h->row_tpf > kBlockMax)
+      return cleanup_fail(fail(PFC_E_ARG, "pfc_plan_create: row transform of %d points does not fit", m));
+    h->rows = rows;
+    h->row_grid = (p->ny + rows - 1) / rows;
+    h->row_smem = (size_t)rows * h->row_ld * cbytes;
+  }
+  {
+    h->col_tpf = threads_per_fft(rcol, p->ny, h->fp32);
+    h->col_ld = p->ny;
+    int cols = std::max(1, 32 / h->col_tpf);
+    while (2 * cols * h->col_tpf <= kBlockMax && (size_t)(2 * cols) * h->col_ld * cbytes <= (size_t)budget / 2 && cols < m)
+      cols *= 2;
+    if ((size_t)cols * h->col_ld * cbytes > (size_t)budget || cols * h->col_tpf > kBlockMax)
+      return cleanup_fail(fail(PFC_E_ARG, "pfc_plan_create: column transform of %d points does not fit", p->ny));
+    h->cols = cols;
+    h->col_grid = (m + cols - 1) / cols;
+    h->col_smem = (size_t)cols * h->col_ld * cbytes;
+  }
+
+  // ---- FP64 ETD1 coefficients (kernels.py:55-71) and the update factor Gamma*lap
+  const double dx = p->lx / p->nx, dy = p->ly / p->ny;
+  const double fx = 1.0 / (p->nx * dx), fy = 1.0 / (p->ny * dy);
+  const double twopi = 6.283185307179586;
+  h->hostA.assign((size_t)p->ny * (m + 1), 0.0);
+  h->hostBg.assign((size_t)p->ny * (m + 1), 0.0);
+  std::vector<double> coefA((size_t)(m + 1) * h->nyh), coefB((size_t)(m + 1) * h->nyh);
+  for (int ky = 0; ky < p->ny; ++ky) {
+    const int kys = (ky <= (p->ny - 1) / 2) ? ky : ky - p->ny;
+    const double kyp = twopi * ((double)kys * fy);
+    for (int kx = 0; kx <= m; ++kx) {
+      const double kxp = twopi * ((double)kx * fx);
+      const double lap = -(kxp * kxp + kyp * kyp);
+      const double t = p->q0 * p->q0 + lap;
+      const double lmu = p->beta * (t * t) + p->epsilon;
+      const double gl = p->gamma * lap;
+      const double ln = gl * lmu;
+      const double z = ln * p->dt;
+      const double A = std::exp(z);
+      const double B = (std::fabs(z) > p->small_z_tol) ? (A - 1) / ln : p->dt * (1 + z / 2 + z * z / 6);
+      const double Bg = B * gl;
+      h->hostA[(size_t)ky * (m + 1) + kx] = A;
+      h->hostBg[(size_t)ky * (m + 1) + kx] = Bg;
+      if (ky < h->nyh) {
+        coefA[(size_t)kx * h->nyh + ky] = A;
+        coefB[(size_t)kx * h->nyh + ky] = Bg;
+      }
+    }
+  }
+  h->lmu0 = p->beta * (p->q0 * p->q0) * (p->q0 * p->q0) + p->epsilon;
+  h->lf0 = (p->beta / 2.0) * (p->q0 * p->q0) * (p->q0 * p->q0);
+
+  // ---- device buffers
+  const size_t specb = h->nspec * h->elt;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMalloc(&h->nhat[i], specb);
+  if (e == cudaSuccess) e = cudaMalloc(&h->W, specb);
+  if (e == cudaSuccess) e = cudaMalloc(&h->V, specb);
+  if (e == cudaSuccess) e = cudaMalloc(&h->coef, (size_t)(m + 1) * h->nyh * h->elt);
+  if (e == cudaSuccess) e = cudaMalloc(&h->tw, tw.size() / 2 * h->elt);
+  h->npartials = 6 * (size_t)h->row_grid + 2 * (size_t)h->col_grid + 2 * 1024;
+  if (e == cudaSuccess) e = cudaMalloc(&h->partials, h->npartials * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&h->scal, kScalCount * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&h->status, sizeof(int));
+  if (e != cudaSuccess)
+    return cleanup_fail(fail(e == cudaErrorMemoryAllocation ? PFC_E_NOMEM : PFC_E_CUDA,
+                             "pfc_plan_create: cudaMalloc failed: %s", cudaGetErrorString(e)));
+
+  // upload tables in the working precision
+  {
+    std::vector<unsigned char> host;
+    const size_t ntw = tw.size() / 2;
+    host.resize(ntw * h->elt);
+    for (size_t i = 0; i < ntw; ++i) {
+      if (h->fp32) { float2 v = make_float2((float)tw[2 * i], (float)tw[2 * i + 1]); memcpy(&host[i * 8], &v, 8); }
+      else { double2 v = make_double2((double)tw[2 * i], (double)tw[2 * i + 1]); memcpy(&host[i * 16], &v, 16); }
+    }
+    e = cudaMemcpy(h->tw, host.data(), host.size(), cudaMemcpyHostToDevice);
+    const size_t nc = (size_t)(m + 1) * h->nyh;
+    host.assign(nc * h->elt, 0);
+    for (size_t i = 0; i < nc; ++i) {
+      if (h->fp32) { float2 v = make_float2((float)coefA[i], (float)coefB[i]); memcpy(&host[i * 8], &v, 8); }
+      else { double2 v = make_double2(coefA[i], coefB[i]); memcpy(&host[i * 16], &v, 16); }
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(h->coef, host.data(), host.size(), cudaMemcpyHostToDevice);
+    std::vector<double> sc(kScalCount, 0.0);
+    if (e == cudaSuccess) e = cudaMemcpy(h->scal, sc.data(), sc.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(h->status, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(h->W, 0, specb);
+    if (e == cudaSuccess) e = cudaMemset(h->nhat[0], 0, specb);
+    if (e == cudaSuccess) e = cudaMemset(h->nhat[1], 0, specb);
+    if (e != cudaSuccess)
+      return cleanup_fail(fail(PFC_E_CUDA, "pfc_plan_create: upload failed: %s", cudaGetErrorString(e)));
+  }
+  int rc = h->fp32 ? set_smem_attrs<float>(h) : set_smem_attrs<double>(h);
+  if (rc) return cleanup_fail(rc);
+  *out = h;
+  return PFC_OK;
+}
+
+int pfc_plan_destroy(pfc_plan* h) {
+  if (!h) return PFC_OK;
+  for (void* p : {h->nhat[0], h->nhat[1], h->W, h->V, h->W2, h->coef, h->tw})
+    if (p) cudaFree(p);
+  if (h->partials) cudaFree(h->partials);
+  if (h->scal) cudaFree(h->scal);
+  if (h->status) cudaFree(h->status);
+  delete h;
+  return PFC_OK;
+}
+
+int pfc_set_state(pfc_plan* h, const double* field, void* stream) {
+  if (!h || !field) return fail(PFC_E_ARG, "pfc_set_state: null argument");
+  if (reinterpret_cast<uintptr_t>(field) % 16)
+    return fail(PFC_E_ARG, "pfc_set_state: field must be 16-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  return h->fp32 ? do_set_state<float>(h, field, s) : do_set_state<double>(h, field, s);
+}
+
+int pfc_get_state(pfc_plan* h, double* field, void* stream) {
+  if (!h || !field) return fail(PFC_E_ARG, "pfc_get_state: null argument");
+  if (!h->state_set) return fail(PFC_E_STATE, "pfc_get_state: no state has been set");
+  if (reinterpret_cast<uintptr_t>(field) % 16)
+    return fail(PFC_E_ARG, "pfc_get_state: field must be 16-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  return h->fp32 ? do_get_state<float>(h, field, s) : do_get_state<double>(h, field, s);
+}
+
+int pfc_step(pfc_plan* h, int64_t nsteps, void* stream) {
+  if (!h) return fail(PFC_E_ARG, "pfc_step: null plan");
+  if (nsteps < 0) return fail(PFC_E_ARG, "pfc_step: negative step count");
+  if (!h->state_set) return fail(PFC_E_STATE, "pfc_step: no state has been set");
+  cudaStream_t s = (cudaStream_t)stream;
+  return h->fp32 ? do_step<float>(h, nsteps, s) : do_step<double>(h, nsteps, s);
+}
+
+int pfc_step_timed(pfc_plan* h, int64_t nsteps, double* ms_row, double* ms_col, void* stream) {
+  if (!h) return fail(PFC_E_ARG, "pfc_step_timed: null plan");
+  if (nsteps < 0) return fail(PFC_E_ARG, "pfc_step_timed: negative step count");
+  if (!h->state_set) return fail(PFC_E_STATE, "pfc_step_timed: no state has been set");
+  cudaStream_t s = (cudaStream_t)stream;
+  return h->fp32 ? do_step_timed<float>(h, nsteps, ms_row, ms_col, s)
+                 : do_step_timed<double>(h, nsteps, ms_row, ms_col, s);
+}
+
+int pfc_reduce(pfc_plan* h, double* out3, void* stream) {
+  if (!h || !out3) return fail(PFC_E_ARG, "pfc_reduce: null argument");
+  if (!h->state_set) return fail(PFC_E_STATE, "pfc_reduce: no state has been set");
+  cudaStream_t s = (cudaStream_t)stream;
+  return h->fp32 ? do_reduce<float>(h, out3, s) : do_reduce<double>(h, out3, s);
+}
+
+int pfc_get_field(pfc_plan* h, int which, double w, double* field, void* stream) {
+  if (!h || !field) return fail(PFC_E_ARG, "pfc_get_field: null argument");
+  if (!h->state_set) return fail(PFC_E_STATE, "pfc_get_field: no state has been set");
+  if (reinterpret_cast<uintptr_t>(field) % 16)
+    return fail(PFC_E_ARG, "pfc_get_field: field must be 16-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  return h->fp32 ? do_get_field<float>(h, which, w, field, s) : do_get_field<double>(h, which, w, field, s);
+}
+
+int pfc_get_spectrum(pfc_plan* h, int which, double* out, void* stream) {
+  if (!h || !out) return fail(PFC_E_ARG, "pfc_get_spectrum: null argument");
+  if (!h->state_set) return fail(PFC_E_STATE, "pfc_get_spectrum: no state has been set");
+  if (which != PFC_SPEC_N_HAT && which != PFC_SPEC_N_HAT_NOW)
+    return fail(PFC_E_ARG, "pfc_get_spectrum: unknown spectrum %d", which);
+  cudaStream_t s = (cudaStream_t)stream;
+  return h->fp32 ? do_get_spectrum<float>(h, which, out, s) : do_get_spectrum<double>(h, which, out, s);
+}
+
+int pfc_get_coefficients(pfc_plan* h, double* a, double* bg) {
+  if (!h) return fail(PFC_E_ARG, "pfc_get_coefficients: null plan");
+  const size_t n = h->hostA.size();
+  if (a) memcpy(a, h->hostA.data(), n * sizeof(double));
+  if (bg) memcpy(bg, h->hostBg.data(), n * sizeof(double));
+  return PFC_OK;
+}
+
+int pfc_status(pfc_plan* h, int32_t* out) {
+  if (!h || !out) return fail(PFC_E_ARG, "pfc_status: null argument");
+  int v = 0;
+  PFC_CUDA(cudaMemcpy(&v, h->status, sizeof(int), cudaMemcpyDeviceToHost));
+  *out = v;
+  return PFC_OK;
+}
+
+int pfc_plan_info(pfc_plan* h, int64_t* o) {
+  if (!h || !o) return fail(PFC_E_ARG, "pfc_plan_info: null argument");
+  o[0] = h->rows; o[1] = h->row_tpf; o[2] = h->row_grid;
+  o[3] = h->cols; o[4] = h->col_tpf; o[5] = h->col_grid;
+  o[6] = (int64_t)h->row_smem; o[7] = (int64_t)h->col_smem;
+  return PFC_OK;
+}
+
+int64_t pfc_launch_count(pfc_plan* h) { return h ? h->launches : 0; }
+
+}  // extern "C"
