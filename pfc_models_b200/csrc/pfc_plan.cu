@@ -515,10 +515,13 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   {
     h->row_tpf = threads_per_fft(rrow, m, h->fp32);
     h->row_ld = m + 1;
-    int rows = std::max(1, 32 / h->row_tpf);                 // whole warps
+    if (h->row_tpf > kBlockMax)
+      return cleanup_fail(fail(PFC_E_ARG, "pfc_plan_create: row transform of %d points needs %d threads", m, h->row_tpf));
+    const int rows_min = std::max(1, 32 / h->row_tpf);       // whole warps
+    const int rows_cap = std::max(rows_min, kBlockMax / h->row_tpf);
     const int coalesce = std::max(1, 64 / cbytes);           // >= 64 B per kx run
-    while (rows < coalesce) rows *= 2;
-    while (2 * rows * h->row_tpf <= kBlockMax && (size_t)(2 * rows) * h->row_ld * cbytes <= (size_t)budget / 2 && rows < p->ny)
+    int rows = std::max(rows_min, std::min(coalesce, rows_cap));
+    while (2 * rows <= rows_cap && (size_t)(2 * rows) * h->row_ld * cbytes <= (size_t)budget / 2 && rows < p->ny)
       rows *= 2;
     while ((size_t)rows * h->row_ld * cbytes > (size_t)budget && rows > std::max(1, 32 / h->row_tpf)) rows /= 2;
     if ((size_t)rows * h->row_ld * cbytes > (size_t)budget || rows * h->row_tpf > kBlockMax)
@@ -530,6 +533,8 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   {
     h->col_tpf = threads_per_fft(rcol, p->ny, h->fp32);
     h->col_ld = p->ny;
+    if (h->col_tpf > kBlockMax)
+      return cleanup_fail(fail(PFC_E_ARG, "pfc_plan_create: column transform of %d points needs %d threads", p->ny, h->col_tpf));
     int cols = std::max(1, 32 / h->col_tpf);
     while (2 * cols * h->col_tpf <= kBlockMax && (size_t)(2 * cols) * h->col_ld * cbytes <= (size_t)budget / 2 && cols < m)
       cols *= 2;
