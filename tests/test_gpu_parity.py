@@ -314,17 +314,20 @@ def test_errors_and_state_order():
 
 
 def test_fp32_log_near_singular():
-    """Mixed-precision log PFC keeps phi > 0 and matches FP64 where phi gets small."""
-    c = _cfg("log_noise")
-    fields_ = {}
-    for precision in ("fp64", "fp32"):
-        sim, _ = _log(c, precision)
-        rng = np.random.default_rng(3)
-        sim.State.phi[...] = 0.3 + 0.25 * rng.uniform(-1, 1, (c["Ny"], c["Nx"]))
-        sim.TimeSteps(200)
-        fields_[precision] = (sim.State.phi.get(), sim.Reduce())
-    a, b = fields_["fp64"], fields_["fp32"]
-    assert a[0].min() < 0.1  # the run visits the near-singular branch
-    assert rel_l2(b[0], a[0]) < 1e-4
-    assert b[1][0] == pytest.approx(a[1][0], rel=1e-5)
-    assert abs(b[1][2] - a[1][2]) < 1e-12
+    """Mixed-precision log PFC where phi/mean - 1 < -0.875 (the FP64 log branch): a
+    one-mode crystal at mean 0.3 whose troughs start at phi = 0.016. FP64 within 1e-12
+    and FP32 within 2e-5 relative L2 of the oracle after 1 and 10 steps."""
+    a_lat, h_lat = 4 * np.pi / 3**0.5, 4 * np.pi
+    geom_o = orc.build_geometry(64, 64, 4 * a_lat, 2 * h_lat)
+    prm = dict(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=0.05)
+    f0 = fields.GeneratePerfectCrystalInitialConditions(geom_o, 0.3, A0=0.095)
+    assert f0.min() / 0.3 - 1 < -0.9
+    for nsteps in (1, 10):
+        ref, _ = orc.run("log", orc.Params(**prm), geom_o, f0, nsteps)
+        for precision, tol in (("fp64", 1e-12), ("fp32", 2e-5)):
+            geom = logpfc.Build2DGeometry(64, 64, 4 * a_lat, 2 * h_lat)
+            sim = logpfc.BuildB200_Simulation(logpfc.BuildLogPFCModelParameters(**prm), geom, precision=precision)
+            sim.State.phi[...] = f0
+            sim.TimeSteps(nsteps)
+            assert rel_l2(sim.State.phi.get(), ref) < tol, (nsteps, precision)
+            assert abs(float(sim.phi.mean()) - f0.mean()) < MASS_TOL
