@@ -128,10 +128,15 @@ int pfc_get_coefficients(pfc_plan* plan, double* host_a, double* host_bg);
 /* Device status bits (PFC_STATUS_*), read synchronously on the plan's last stream. */
 int pfc_status(pfc_plan* plan, int32_t* out_status);
 
-/* Launch configuration chosen for this plan, for reporting: out[0..7] =
- * {row rows/CTA, row threads/FFT, row CTAs, col columns/CTA, col threads/FFT,
- *  col CTAs, row smem bytes, col smem bytes}. */
-int pfc_plan_info(pfc_plan* plan, int64_t* out8);
+/* Launch configuration chosen for this plan, for reporting: out[0..15] =
+ * {generic row: rows/CTA, threads/FFT, CTAs; generic column: columns/CTA,
+ *  threads/FFT, CTAs; generic row smem, column smem bytes;
+ *  1 if the power-of-two step kernels are used; their row rows/CTA, threads/CTA,
+ *  CTAs, smem bytes; column threads/CTA, CTAs, smem bytes}. */
+int pfc_plan_info(pfc_plan* plan, int64_t* out16);
+
+/* problem.flags bits */
+#define PFC_FLAG_GENERIC_ONLY 1   /* do not use the power-of-two step kernels */
 
 /* Kernel launches issued by this plan since creation (for accounting). */
 int64_t pfc_launch_count(pfc_plan* plan);

@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 OUT = os.path.join(HERE, "libpfc_b200.so")
 SOURCES = ["pfc_plan.cu"]
-HEADERS = ["pfc_fft.cuh", "pfc_kernels.cuh"]
+HEADERS = ["pfc_fft.cuh", "pfc_kernels.cuh", "pfc_fast.cuh"]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",

@@ -1,0 +1,428 @@
+// Specialised step kernels for power-of-two grids (compile-time transform sizes).
+//
+// Each transform of length N is owned by a group of TPF = N/EE threads; a thread
+// holds EE complex values in registers. Sequence A runs radices (EE, ..., EE, LAST)
+// and sequence B (LAST, EE, ..., EE), so that the last pass of A and the first pass
+// of B touch the same elements in the same thread: the row kernel applies the
+// nonlinearity between them (inverse A, forward B) and the column kernel applies the
+// ETD1 update between them (forward A, inverse B) without a shared-memory round trip.
+//
+// Shared-memory exchanges between passes use the padded index i + (i >> P) with
+// 2^P = elements per 128 bytes (16 complex floats, 8 complex doubles), which makes
+// the stride-R writes of every Stockham pass with R <= 2^P bank-conflict free.
+// A transform group synchronises with __syncwarp when it fits in a warp, otherwise
+// with its own named barrier, so groups never wait for each other.
+#pragma once
+#include <type_traits>
+
+#include "pfc_kernels.cuh"
+
+namespace pfc {
+
+template <int N, int EE_REQ>
+struct FastSeq {
+  __host__ __device__ static constexpr int lg(int x) { return x <= 1 ? 0 : 1 + lg(x >> 1); }
+  static constexpr int EE = EE_REQ < N ? EE_REQ : N;     // elements per thread
+  static constexpr int TPF = N / EE;                      // threads per transform
+  static constexpr int LN = lg(N), LE = lg(EE);
+  static constexpr int NPASS = (LN + LE - 1) / LE;
+  static constexpr int LAST = 1 << (LN - (NPASS - 1) * LE);
+  __host__ __device__ static constexpr int radA(int p) { return p == NPASS - 1 ? LAST : EE; }
+  __host__ __device__ static constexpr int radB(int p) { return p == 0 ? LAST : EE; }
+  __host__ __device__ static constexpr int nsA(int p) { return p == 0 ? 1 : nsA(p - 1) * radA(p - 1); }
+  __host__ __device__ static constexpr int nsB(int p) { return p == 0 ? 1 : nsB(p - 1) * radB(p - 1); }
+  // offset of pass p's twiddle table ([k][q-1], k < ns, q < R) within the sequence table
+  __host__ __device__ static constexpr int twA(int p) { return p <= 1 ? 0 : twA(p - 1) + nsA(p - 1) * (radA(p - 1) - 1); }
+  __host__ __device__ static constexpr int twB(int p) { return p <= 1 ? 0 : twB(p - 1) + nsB(p - 1) * (radB(p - 1) - 1); }
+  __host__ __device__ static constexpr int sizeA() { return twA(NPASS); }
+  __host__ __device__ static constexpr int sizeB() { return twB(NPASS); }
+};
+
+template <class T> struct PadShift { static constexpr int value = 4; };   // 16 x 8 B per 128 B
+template <> struct PadShift<double> { static constexpr int value = 3; };  // 8 x 16 B per 128 B
+
+template <int P> __device__ __forceinline__ int padi(int i) { return i + (i >> P); }
+
+__device__ __forceinline__ float2 ldg2(const float2* p) { return __ldg(p); }
+__device__ __forceinline__ double2 ldg2(const double2* p) { return __ldg(p); }
+template <class T> __device__ __forceinline__ cplx<T> ldgc(const cplx<T>* p) {
+  using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+  const V v = ldg2(reinterpret_cast<const V*>(p));
+  return mk((T)v.x, (T)v.y);
+}
+
+// Synchronisation of one transform group (TPF threads, group index g within the CTA).
+template <int TPF>
+__device__ __forceinline__ void group_sync(int g) {
+  if constexpr (TPF < 32) {
+    // lanes of this group only, so groups sharing a warp may branch differently
+    const unsigned lane0 = (threadIdx.x & 31u) & ~(unsigned)(TPF - 1);
+    __syncwarp(((1u << TPF) - 1u) << lane0);
+  } else if constexpr (TPF == 32) {
+    __syncwarp();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(TPF) : "memory");
+  }
+}
+
+// One Stockham pass of radix R, stride NS, on a length-N transform whose group has
+// TPF threads holding EE = R * NB values each (v[b * R + q], butterfly j = t + b * TPF).
+template <class T, int N, int EE, int R, int NS, int P>
+struct FastPass {
+  static constexpr int TPF = N / EE, NB = EE / R, NR = N / R;
+  static __device__ __forceinline__ void load(const cplx<T>* buf, cplx<T>* v, int t) {
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const int j = t + b * TPF;
+#pragma unroll
+      for (int q = 0; q < R; ++q) v[b * R + q] = buf[padi<P>(j + q * NR)];
+    }
+  }
+  template <bool INV>
+  static __device__ __forceinline__ void compute(cplx<T>* v, int t, const cplx<T>* __restrict__ tw) {
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      if constexpr (NS > 1) {
+        const int j = t + b * TPF;
+        const int k = j & (NS - 1);
+        const cplx<T>* w = tw + k * (R - 1);
+        cplx<T> wq[R];
+#pragma unroll
+        for (int q = 1; q < R; ++q) wq[q] = ldgc(w + q - 1);
+#pragma unroll
+        for (int q = 1; q < R; ++q) {
+          cplx<T> x = wq[q];
+          if (INV) x.y = -x.y;
+          v[b * R + q] = cmul(v[b * R + q], x);
+        }
+      }
+      dft<R, INV>(v + b * R, (const cplx<T>*)nullptr);
+    }
+  }
+  static __device__ __forceinline__ void store(cplx<T>* buf, const cplx<T>* v, int t) {
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const int j = t + b * TPF;
+      const int k = j & (NS - 1);
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int q = 0; q < R; ++q) buf[padi<P>(base + q * NS)] = v[b * R + q];
+    }
+  }
+  // natural-order index of register v[b * R + q] after the last pass (NS = N / R)
+  static __device__ __forceinline__ int out_index(int t, int b, int q) { return t + b * TPF + q * NR; }
+};
+
+// Middle passes [PA, PB) of sequence A (SEQB = false) or B, in place through buf.
+template <class T, int N, int EE_REQ, bool SEQB, bool INV, int PA, int PB>
+__device__ __forceinline__ void fast_mid(cplx<T>* buf, cplx<T>* v, int t, int g, const cplx<T>* __restrict__ tw) {
+  if constexpr (PA < PB) {
+    using S = FastSeq<N, EE_REQ>;
+    constexpr int P = PadShift<T>::value;
+    constexpr int R = SEQB ? S::radB(PA) : S::radA(PA);
+    constexpr int NS = SEQB ? S::nsB(PA) : S::nsA(PA);
+    constexpr int OFF = SEQB ? S::twB(PA) : S::twA(PA);
+    using PS = FastPass<T, N, S::EE, R, NS, P>;
+    PS::load(buf, v, t);
+    group_sync<S::TPF>(g);
+    PS::template compute<INV>(v, t, tw + OFF);
+    PS::store(buf, v, t);
+    group_sync<S::TPF>(g);
+    fast_mid<T, N, EE_REQ, SEQB, INV, PA + 1, PB>(buf, v, t, g, tw);
+  }
+}
+
+template <class T>
+struct FastRowArgs {
+  int ny, rows, ld;
+  const cplx<T>* in;         // W, column-major [kx][y]
+  cplx<T>* out;              // V, column-major
+  const cplx<T>* twA;        // row sequence A table (inverse uses conjugates)
+  const cplx<T>* twB;        // row sequence B table
+  const cplx<T>* rtw;        // exp(-2 pi i k / nx), k < m
+  const double* scal;
+  int clamp;
+  double g, min_phi, min_log;
+};
+
+template <class T>
+struct FastColArgs {
+  int m, ny, nyh;
+  const cplx<T>* in;         // V
+  const cplx<T>* nin;        // n_hat
+  cplx<T>* nout;             // n_hat'
+  cplx<T>* wout;             // W'
+  const cplx<T>* coef;       // (A, Bg) [kx][ky <= ny/2]
+  const cplx<T>* twA;        // column sequence A (forward)
+  const cplx<T>* twB;        // column sequence B (inverse uses conjugates)
+  T scale;
+};
+
+template <int TPF> struct FastBound { static constexpr int value = TPF > 256 ? TPF : 256; };
+
+// ------------------------------------------------------------------ row kernel
+// CTA: `rows` consecutive rows (tile), groups of TPF threads each process rows
+// g, g + ngroups, ... The tile is staged through shared memory with a transposing
+// load/store (global layout is column-major).
+template <class T, int M, int EE_REQ, int MODEL>
+__global__ void __launch_bounds__(FastBound<FastSeq<M, EE_REQ>::TPF>::value)
+row_step_fast(FastRowArgs<T> a) {
+  using S = FastSeq<M, EE_REQ>;
+  constexpr int P = PadShift<T>::value;
+  constexpr int EE = S::EE, TPF = S::TPF, NP = S::NPASS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int ny = a.ny, rows = a.rows, ld = a.ld;
+  const int y0 = blockIdx.x * rows;
+  const int ngroups = blockDim.x / TPF;
+  const int g = threadIdx.x / TPF, t = threadIdx.x - g * TPF;
+  const bool dev = (sizeof(T) == 4);
+
+  // ---- transposing tile load: element (kx, y0 + r) -> sm[r * ld + pad(kx)]
+  for (int i = threadIdx.x; i < rows * M; i += blockDim.x) {
+    const int r = i % rows, kx = i / rows;
+    cplx<T> v = mk(T(0), T(0));
+    if (y0 + r < ny) v = a.in[(size_t)kx * ny + (y0 + r)];
+    sm[r * ld + padi<P>(kx)] = v;
+  }
+  __syncthreads();
+
+  // nonlinearity parameters
+  float c1 = 0.f, c2 = 0.f, inv = 0.f, lmin = 0.f;
+  double inv_d = 0.0, mphi_rel = 0.0;
+  if (dev) {
+    c1 = (float)a.scal[kScalC1];
+    c2 = (float)a.scal[kScalC2];
+    inv = (float)a.scal[kScalInvMean];
+    inv_d = a.scal[kScalInvMean];
+    mphi_rel = a.min_phi * inv_d;
+    lmin = (float)a.scal[kScalLogMin];
+  }
+
+  for (int r = g; r < rows; r += ngroups) {
+    cplx<T>* row = sm + r * ld;
+    cplx<T> v[EE];
+    // ---- A0 load with the inverse-real pre-twiddle (pairs k, M - k)
+    {
+      constexpr int R = S::radA(0), NR = M / R, NB = EE / R;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int j = t + b * TPF;
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int k = j + q * NR;
+          const cplx<T> xk = row[padi<P>(k)];
+          cplx<T> z;
+          if (k == 0) {
+            z = mk(xk.x + xk.y, xk.x - xk.y);
+          } else {
+            const cplx<T> xm = row[padi<P>(M - k)];
+            const cplx<T> s = xk + conj(xm), d = xk - conj(xm);
+            z = s + mul_i(cmul(conj(ldgc(a.rtw + k)), d));
+          }
+          v[b * R + q] = z;
+        }
+      }
+    }
+    group_sync<TPF>(g);
+    if constexpr (NP == 1) {
+      FastPass<T, M, EE, S::radA(0), 1, P>::template compute<true>(v, t, a.twA);
+    } else {
+      using P0 = FastPass<T, M, EE, S::radA(0), 1, P>;
+      P0::template compute<true>(v, t, a.twA);
+      P0::store(row, v, t);
+      group_sync<TPF>(g);
+      fast_mid<T, M, EE_REQ, false, true, 1, NP - 1>(row, v, t, g, a.twA);
+      using PL = FastPass<T, M, EE, S::radA(NP - 1), S::nsA(NP - 1), P>;
+      PL::load(row, v, t);
+      group_sync<TPF>(g);
+      PL::template compute<true>(v, t, a.twA + S::twA(NP - 1));
+    }
+    // ---- v holds z[e] = n[2e] + i n[2e+1]: the nonlinearity, in registers
+#pragma unroll
+    for (int e = 0; e < EE; ++e) {
+      const cplx<T> z = v[e];
+      if (dev) {
+        v[e] = mk((T)nonlin_dev<MODEL>((float)z.x, c1, c2, inv, inv_d, a.clamp, mphi_rel, lmin),
+                  (T)nonlin_dev<MODEL>((float)z.y, c1, c2, inv, inv_d, a.clamp, mphi_rel, lmin));
+      } else {
+        v[e] = mk((T)nonlin_plain<MODEL>((double)z.x, a.g, a.clamp, a.min_phi, a.min_log),
+                  (T)nonlin_plain<MODEL>((double)z.y, a.g, a.clamp, a.min_phi, a.min_log));
+      }
+    }
+    // ---- forward sequence B
+    constexpr int RL = S::radB(NP - 1);
+    if constexpr (NP == 1) {
+      FastPass<T, M, EE, S::radB(0), 1, P>::template compute<false>(v, t, a.twB);
+    } else {
+      using Q0 = FastPass<T, M, EE, S::radB(0), 1, P>;
+      Q0::template compute<false>(v, t, a.twB);
+      Q0::store(row, v, t);
+      group_sync<TPF>(g);
+      fast_mid<T, M, EE_REQ, true, false, 1, NP - 1>(row, v, t, g, a.twB);
+      using QL = FastPass<T, M, EE, RL, S::nsB(NP - 1), P>;
+      QL::load(row, v, t);
+      group_sync<TPF>(g);
+      QL::template compute<false>(v, t, a.twB + S::twB(NP - 1));
+    }
+    // ---- forward-real post-twiddle: publish Z, read the (k, M - k) partners
+    using QO = FastPass<T, M, EE, RL, M / RL, P>;
+    constexpr int NBL = EE / RL;
+#pragma unroll
+    for (int b = 0; b < NBL; ++b)
+#pragma unroll
+      for (int q = 0; q < RL; ++q) row[padi<P>(QO::out_index(t, b, q))] = v[b * RL + q];
+    group_sync<TPF>(g);
+#pragma unroll
+    for (int b = 0; b < NBL; ++b)
+#pragma unroll
+      for (int q = 0; q < RL; ++q) {
+        const int k = QO::out_index(t, b, q);
+        const cplx<T> zk = v[b * RL + q];
+        cplx<T> y;
+        if (k == 0) {
+          y = mk(zk.x + zk.y, zk.x - zk.y);
+        } else {
+          const cplx<T> zm = row[padi<P>(M - k)];
+          const cplx<T> e = T(0.5) * (zk + conj(zm));
+          const cplx<T> o = T(0.5) * rot4<false>(zk - conj(zm));
+          y = e + cmul(ldgc(a.rtw + k), o);
+        }
+        v[b * RL + q] = y;
+      }
+    group_sync<TPF>(g);
+#pragma unroll
+    for (int b = 0; b < NBL; ++b)
+#pragma unroll
+      for (int q = 0; q < RL; ++q) row[padi<P>(QO::out_index(t, b, q))] = v[b * RL + q];
+  }
+  __syncthreads();
+  // ---- transposing tile store
+  for (int i = threadIdx.x; i < rows * M; i += blockDim.x) {
+    const int r = i % rows, kx = i / rows;
+    if (y0 + r < ny) a.out[(size_t)kx * ny + (y0 + r)] = sm[r * ld + padi<P>(kx)];
+  }
+}
+
+// ------------------------------------------------------------------ column kernel
+// CTA: ngroups consecutive columns, one group of TPF threads per column. Global
+// reads and writes go straight between registers and HBM (the first pass of each
+// sequence reads, and the last pass writes, consecutive elements per lane).
+template <class T, int NY, int EE_REQ>
+__global__ void __launch_bounds__(FastBound<FastSeq<NY, EE_REQ>::TPF>::value)
+col_step_fast(FastColArgs<T> a) {
+  using S = FastSeq<NY, EE_REQ>;
+  constexpr int P = PadShift<T>::value;
+  constexpr int EE = S::EE, TPF = S::TPF, NP = S::NPASS;
+  constexpr int PADN = NY + (NY >> P) + 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int ngroups = blockDim.x / TPF;
+  const int g = threadIdx.x / TPF, t = threadIdx.x - g * TPF;
+  const int kx = blockIdx.x * ngroups + g;      // m is a multiple of ngroups
+  cplx<T>* buf = sm + g * PADN;
+  const int m = a.m, nyh = a.nyh;
+  cplx<T> v[EE];
+
+  // ---- forward sequence A; pass 0 reads the column of V from HBM
+  {
+    constexpr int R = S::radA(0), NR = NY / R, NB = EE / R;
+    const cplx<T>* col = a.in + (size_t)kx * NY;
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+      for (int q = 0; q < R; ++q) v[b * R + q] = col[t + b * TPF + q * NR];
+  }
+  if constexpr (NP == 1) {
+    FastPass<T, NY, EE, S::radA(0), 1, P>::template compute<false>(v, t, a.twA);
+  } else {
+    using P0 = FastPass<T, NY, EE, S::radA(0), 1, P>;
+    P0::template compute<false>(v, t, a.twA);
+    P0::store(buf, v, t);
+    group_sync<TPF>(g);
+    fast_mid<T, NY, EE_REQ, false, false, 1, NP - 1>(buf, v, t, g, a.twA);
+    using PL = FastPass<T, NY, EE, S::radA(NP - 1), S::nsA(NP - 1), P>;
+    PL::load(buf, v, t);
+    group_sync<TPF>(g);
+    PL::template compute<false>(v, t, a.twA + S::twA(NP - 1));
+  }
+
+  // ---- ETD1 update on the natural-order values held in registers
+  constexpr int RL = S::radA(NP - 1), NBL = EE / RL;
+  using PO = FastPass<T, NY, EE, RL, NY / RL, P>;
+  const cplx<T>* nin = a.nin + (size_t)kx * NY;
+  cplx<T>* nout = a.nout + (size_t)kx * NY;
+  if (kx != 0) {
+    const cplx<T>* cf = a.coef + (size_t)kx * nyh;
+#pragma unroll
+    for (int b = 0; b < NBL; ++b)
+#pragma unroll
+      for (int q = 0; q < RL; ++q) {
+        const int ky = PO::out_index(t, b, q);
+        const int kh = ky <= NY / 2 ? ky : NY - ky;
+        const cplx<T> c = cf[kh];
+        const cplx<T> p = nin[ky];
+        const cplx<T> o = c.x * p + c.y * v[b * RL + q];
+        nout[ky] = o;
+        v[b * RL + q] = o;
+      }
+  } else {
+    // packed DC/Nyquist column: unpack from the (ky, -ky) pairs
+#pragma unroll
+    for (int b = 0; b < NBL; ++b)
+#pragma unroll
+      for (int q = 0; q < RL; ++q) buf[padi<P>(PO::out_index(t, b, q))] = v[b * RL + q];
+    group_sync<TPF>(g);
+    const cplx<T>* c0 = a.coef;
+    const cplx<T>* cm = a.coef + (size_t)m * nyh;
+#pragma unroll
+    for (int b = 0; b < NBL; ++b)
+#pragma unroll
+      for (int q = 0; q < RL; ++q) {
+        const int ky = PO::out_index(t, b, q);
+        const int kyp = ky == 0 ? 0 : NY - ky;
+        const int kh = ky <= NY / 2 ? ky : NY - ky;
+        const cplx<T> qk = v[b * RL + q], qkp = buf[padi<P>(kyp)];
+        const cplx<T> pk = nin[ky], pkp = nin[kyp];
+        cplx<T> h0, hm, g0, gm;
+        unpack_pair(pk, pkp, h0, hm);
+        unpack_pair(qk, qkp, g0, gm);
+        const cplx<T> a0 = c0[kh], am = cm[kh];
+        const cplx<T> h0n = a0.x * h0 + a0.y * g0;
+        const cplx<T> hmn = am.x * hm + am.y * gm;
+        const cplx<T> o = h0n + mul_i(hmn);
+        nout[ky] = o;
+        v[b * RL + q] = o;
+      }
+  }
+  group_sync<TPF>(g);
+
+  // ---- inverse sequence B; the last pass writes W to HBM
+  if constexpr (NP == 1) {
+    FastPass<T, NY, EE, S::radB(0), 1, P>::template compute<true>(v, t, a.twB);
+  } else {
+    using Q0 = FastPass<T, NY, EE, S::radB(0), 1, P>;
+    Q0::template compute<true>(v, t, a.twB);
+    Q0::store(buf, v, t);
+    group_sync<TPF>(g);
+    fast_mid<T, NY, EE_REQ, true, true, 1, NP - 1>(buf, v, t, g, a.twB);
+    using QL = FastPass<T, NY, EE, S::radB(NP - 1), S::nsB(NP - 1), P>;
+    QL::load(buf, v, t);
+    QL::template compute<true>(v, t, a.twB + S::twB(NP - 1));
+  }
+  {
+    constexpr int RB = S::radB(NP - 1), NBB = EE / RB;
+    using QO = FastPass<T, NY, EE, RB, NY / RB, P>;
+    cplx<T>* col = a.wout + (size_t)kx * NY;
+    const T s = a.scale;
+#pragma unroll
+    for (int b = 0; b < NBB; ++b)
+#pragma unroll
+      for (int q = 0; q < RB; ++q) {
+        const cplx<T> x = v[b * RB + q];
+        col[QO::out_index(t, b, q)] = mk(s * x.x, s * x.y);
+      }
+  }
+}
+
+}  // namespace pfc

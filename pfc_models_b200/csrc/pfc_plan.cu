@@ -12,6 +12,7 @@
 
 #include "pfc_b200.h"
 #include "pfc_kernels.cuh"
+#include "pfc_fast.cuh"
 
 using namespace pfc;
 
@@ -154,6 +155,14 @@ struct pfc_plan {
   long long steps_since_set = 0;
   long long launches = 0;
   std::vector<double> hostA, hostBg;  // FP64 coefficients, (ny, m+1)
+  // specialised power-of-two step kernels (pfc_fast.cuh)
+  bool fast = false;
+  void* fast_row_fn = nullptr;
+  void* fast_col_fn = nullptr;
+  int fr_rows = 0, fr_threads = 0, fr_ld = 0, fr_grid = 0;
+  int fc_threads = 0, fc_grid = 0;
+  size_t fr_smem = 0, fc_smem = 0;
+  int tw_ra = 0, tw_rb = 0, tw_ca = 0, tw_cb = 0;  // table offsets (complex elements)
   double lmu0 = 0, lf0 = 0;
 };
 
@@ -249,6 +258,170 @@ int set_smem_attrs(pfc_plan* h) {
   return PFC_OK;
 }
 
+// ---- specialised power-of-two path (pfc_fast.cuh)
+template <class T> constexpr int fast_ee() { return sizeof(T) == 4 ? 16 : 8; }
+constexpr int kFastMinLog = 5, kFastMaxLogRow = 12, kFastMaxLogCol = 13;
+
+int ilog2_exact(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return (1 << l) == n ? l : -1;
+}
+
+// Pass tables of sequences A and B for an N-point transform, laid out as FastSeq
+// expects: for p = 1 .. NPASS-1, ns(p) x (R(p) - 1) entries exp(-2 pi i q k / (ns R)).
+template <class T, int N>
+void fast_tables(std::vector<long double>& tw, int& offA, int& offB) {
+  using S = FastSeq<N, fast_ee<T>()>;
+  const long double twopi = 6.283185307179586476925286766559L;
+  for (int seq = 0; seq < 2; ++seq) {
+    (seq == 0 ? offA : offB) = (int)(tw.size() / 2);
+    for (int p = 1; p < S::NPASS; ++p) {
+      const int R = seq == 0 ? S::radA(p) : S::radB(p);
+      const int ns = seq == 0 ? S::nsA(p) : S::nsB(p);
+      for (int k = 0; k < ns; ++k)
+        for (int q = 1; q < R; ++q) {
+          const long double ang = -twopi * (long double)((long long)q * k) / (long double)(ns * R);
+          tw.push_back(cosl(ang));
+          tw.push_back(sinl(ang));
+        }
+    }
+  }
+}
+
+template <class T, int L>
+void fast_tables_l(int lg, std::vector<long double>& tw, int& a, int& b) {
+  if constexpr (L <= kFastMaxLogCol) {
+    if (lg == L) { fast_tables<T, (1 << L)>(tw, a, b); return; }
+    fast_tables_l<T, L + 1>(lg, tw, a, b);
+  }
+}
+
+template <class T, int L>
+int fast_tpf_l(int lg) {
+  if constexpr (L <= kFastMaxLogCol) {
+    if (lg == L) return FastSeq<(1 << L), fast_ee<T>()>::TPF;
+    return fast_tpf_l<T, L + 1>(lg);
+  } else {
+    return 0;
+  }
+}
+
+template <class T, int MODEL, int L>
+void* fast_row_l(int lg) {
+  if constexpr (L <= kFastMaxLogRow) {
+    if (lg == L) return (void*)row_step_fast<T, (1 << L), fast_ee<T>(), MODEL>;
+    return fast_row_l<T, MODEL, L + 1>(lg);
+  } else {
+    return nullptr;
+  }
+}
+
+template <class T, int L>
+void* fast_col_l(int lg) {
+  if constexpr (L <= kFastMaxLogCol) {
+    if (lg == L) return (void*)col_step_fast<T, (1 << L), fast_ee<T>()>;
+    return fast_col_l<T, L + 1>(lg);
+  } else {
+    return nullptr;
+  }
+}
+
+// Chooses the fast kernels and their launch shapes; appends their twiddle tables to tw.
+template <class T>
+int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
+  const int lm = ilog2_exact(h->m), ly = ilog2_exact(h->ny);
+  if ((h->prob.flags & 1) || lm < kFastMinLog || lm > kFastMaxLogRow || ly < kFastMinLog || ly > kFastMaxLogCol)
+    return PFC_OK;
+  constexpr int P = PadShift<T>::value;
+  const int elt = (int)sizeof(cplx<T>);
+  fast_tables_l<T, kFastMinLog>(lm, tw, h->tw_ra, h->tw_rb);
+  fast_tables_l<T, kFastMinLog>(ly, tw, h->tw_ca, h->tw_cb);
+  // row kernel: tile of fr_rows rows (>= 64 B per kx run), groups of tpf threads
+  const int tpr = fast_tpf_l<T, kFastMinLog>(lm);
+  int ngr = std::max(1, 256 / tpr);
+  int rows = sizeof(T) == 4 ? 8 : 4;
+  ngr = std::min(ngr, rows);
+  rows = std::max(rows, ngr);
+  int ld = h->m + (h->m >> P);
+  while (ld % (1 << P) != 2) ++ld;
+  h->fr_rows = rows;
+  h->fr_threads = ngr * tpr;
+  h->fr_ld = ld;
+  h->fr_grid = (h->ny + rows - 1) / rows;
+  h->fr_smem = (size_t)rows * ld * elt;
+  // column kernel: one group of tpc threads per column
+  const int tpc = fast_tpf_l<T, kFastMinLog>(ly);
+  const int ngc = std::min(std::max(1, 256 / tpc), h->m);
+  h->fc_threads = ngc * tpc;
+  h->fc_grid = h->m / ngc;
+  h->fc_smem = (size_t)ngc * (h->ny + (h->ny >> P) + 2) * elt;
+  if (h->fr_threads > 1024 || h->fc_threads > 1024 || h->fr_smem > 200 * 1024 || h->fc_smem > 200 * 1024)
+    return PFC_OK;  // generic path
+  h->fast_row_fn = h->prob.model == kModelLog ? fast_row_l<T, kModelLog, kFastMinLog>(lm)
+                                              : fast_row_l<T, kModelStd, kFastMinLog>(lm);
+  h->fast_col_fn = fast_col_l<T, kFastMinLog>(ly);
+  if (!h->fast_row_fn || !h->fast_col_fn) return PFC_OK;
+  PFC_CUDA(cudaFuncSetAttribute(h->fast_row_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->fr_smem));
+  PFC_CUDA(cudaFuncSetAttribute(h->fast_col_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->fc_smem));
+  h->fast = true;
+  return PFC_OK;
+}
+
+// One row pass of a step: W -> V.
+template <class T>
+int launch_step_row(pfc_plan* h, cudaStream_t s) {
+  if (h->fast) {
+    FastRowArgs<T> a{};
+    a.ny = h->ny; a.rows = h->fr_rows; a.ld = h->fr_ld;
+    a.in = reinterpret_cast<const cplx<T>*>(h->W);
+    a.out = reinterpret_cast<cplx<T>*>(h->V);
+    const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(h->tw);
+    a.twA = tw + h->tw_ra; a.twB = tw + h->tw_rb; a.rtw = tw + h->rt_off;
+    a.scal = h->scal;
+    a.clamp = h->prob.clamp_log;
+    a.g = h->prob.g; a.min_phi = h->prob.min_phi;
+    a.min_log = (h->prob.min_phi > 0) ? std::log(h->prob.min_phi) : -INFINITY;
+    void* args[] = {(void*)&a};
+    cudaError_t e = cudaLaunchKernel(h->fast_row_fn, dim3(h->fr_grid), dim3(h->fr_threads), args, h->fr_smem, s);
+    ++h->launches;
+    if (e != cudaSuccess) return fail(PFC_E_CUDA, "row step launch failed: %s", cudaGetErrorString(e));
+    return PFC_OK;
+  }
+  RowArgs<T> ra = row_args<T>(h);
+  ra.in = reinterpret_cast<const cplx<T>*>(h->W);
+  ra.out = reinterpret_cast<cplx<T>*>(h->V);
+  return launch_row<T, kRowStep>(h, ra, s);
+}
+
+// One column pass of a step: V, n_hat[cur] -> n_hat[cur ^ 1], W.
+template <class T>
+int launch_step_col(pfc_plan* h, cudaStream_t s) {
+  if (h->fast) {
+    FastColArgs<T> a{};
+    a.m = h->m; a.ny = h->ny; a.nyh = h->nyh;
+    a.in = reinterpret_cast<const cplx<T>*>(h->V);
+    a.nin = reinterpret_cast<const cplx<T>*>(h->nhat[h->cur]);
+    a.nout = reinterpret_cast<cplx<T>*>(h->nhat[h->cur ^ 1]);
+    a.wout = reinterpret_cast<cplx<T>*>(h->W);
+    a.coef = reinterpret_cast<const cplx<T>*>(h->coef);
+    const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(h->tw);
+    a.twA = tw + h->tw_ca; a.twB = tw + h->tw_cb;
+    a.scale = (T)(1.0 / ((double)h->nx * (double)h->ny));
+    void* args[] = {(void*)&a};
+    cudaError_t e = cudaLaunchKernel(h->fast_col_fn, dim3(h->fc_grid), dim3(h->fc_threads), args, h->fc_smem, s);
+    ++h->launches;
+    if (e != cudaSuccess) return fail(PFC_E_CUDA, "column step launch failed: %s", cudaGetErrorString(e));
+    return PFC_OK;
+  }
+  ColArgs<T> ca = col_args<T>(h);
+  ca.in = reinterpret_cast<const cplx<T>*>(h->V);
+  ca.wout = reinterpret_cast<cplx<T>*>(h->W);
+  ca.nin = reinterpret_cast<const cplx<T>*>(h->nhat[h->cur]);
+  ca.nout = reinterpret_cast<cplx<T>*>(h->nhat[h->cur ^ 1]);
+  return launch_col<T, kColStep>(h, ca, s);
+}
+
 // ---- entry point bodies, templated on the working precision
 template <class T>
 int do_set_state(pfc_plan* h, const double* field, cudaStream_t s) {
@@ -280,18 +453,10 @@ int do_set_state(pfc_plan* h, const double* field, cudaStream_t s) {
 
 template <class T>
 int do_step(pfc_plan* h, long long nsteps, cudaStream_t s) {
-  RowArgs<T> ra = row_args<T>(h);
-  ra.in = reinterpret_cast<const cplx<T>*>(h->W);
-  ra.out = reinterpret_cast<cplx<T>*>(h->V);
-  ColArgs<T> ca = col_args<T>(h);
-  ca.in = reinterpret_cast<const cplx<T>*>(h->V);
-  ca.wout = reinterpret_cast<cplx<T>*>(h->W);
   for (long long i = 0; i < nsteps; ++i) {
-    int rc = launch_row<T, kRowStep>(h, ra, s);
+    int rc = launch_step_row<T>(h, s);
     if (rc) return rc;
-    ca.nin = reinterpret_cast<const cplx<T>*>(h->nhat[h->cur]);
-    ca.nout = reinterpret_cast<cplx<T>*>(h->nhat[h->cur ^ 1]);
-    rc = launch_col<T, kColStep>(h, ca, s);
+    rc = launch_step_col<T>(h, s);
     if (rc) return rc;
     h->cur ^= 1;
     ++h->steps_since_set;
@@ -305,20 +470,12 @@ int do_step_timed(pfc_plan* h, long long nsteps, double* ms_row, double* ms_col,
   int rc = PFC_OK;
   for (auto& e : ev)
     if (cudaEventCreate(&e) != cudaSuccess) { rc = fail(PFC_E_CUDA, "cudaEventCreate failed"); break; }
-  RowArgs<T> ra = row_args<T>(h);
-  ra.in = reinterpret_cast<const cplx<T>*>(h->W);
-  ra.out = reinterpret_cast<cplx<T>*>(h->V);
-  ColArgs<T> ca = col_args<T>(h);
-  ca.in = reinterpret_cast<const cplx<T>*>(h->V);
-  ca.wout = reinterpret_cast<cplx<T>*>(h->W);
   for (long long i = 0; i < nsteps && rc == PFC_OK; ++i) {
     cudaEventRecord(ev[3 * i], s);
-    rc = launch_row<T, kRowStep>(h, ra, s);
+    rc = launch_step_row<T>(h, s);
     if (rc) break;
     cudaEventRecord(ev[3 * i + 1], s);
-    ca.nin = reinterpret_cast<const cplx<T>*>(h->nhat[h->cur]);
-    ca.nout = reinterpret_cast<cplx<T>*>(h->nhat[h->cur ^ 1]);
-    rc = launch_col<T, kColStep>(h, ca, s);
+    rc = launch_step_col<T>(h, s);
     if (rc) break;
     cudaEventRecord(ev[3 * i + 2], s);
     h->cur ^= 1;
@@ -504,6 +661,10 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
       tw.push_back(cosl(ang));
       tw.push_back(sinl(ang));
     }
+  }
+  {
+    const int rc = h->fp32 ? setup_fast<float>(h, tw) : setup_fast<double>(h, tw);
+    if (rc) return cleanup_fail(rc);
   }
 
   // ---- launch shapes
@@ -716,6 +877,9 @@ int pfc_plan_info(pfc_plan* h, int64_t* o) {
   o[0] = h->rows; o[1] = h->row_tpf; o[2] = h->row_grid;
   o[3] = h->cols; o[4] = h->col_tpf; o[5] = h->col_grid;
   o[6] = (int64_t)h->row_smem; o[7] = (int64_t)h->col_smem;
+  o[8] = h->fast ? 1 : 0;
+  o[9] = h->fr_rows; o[10] = h->fr_threads; o[11] = h->fr_grid; o[12] = (int64_t)h->fr_smem;
+  o[13] = h->fc_threads; o[14] = h->fc_grid; o[15] = (int64_t)h->fc_smem;
   return PFC_OK;
 }
 

@@ -40,16 +40,18 @@ def GetLinearKernel_phi(modelParameters, DerivativeKernels):
 
 
 class Simulation(_Simulation):
-    def __init__(self, modelParameters, geometry, precision="fp64", clamp_log=False, device=None):
-        super().__init__("log", modelParameters, geometry, precision=precision, clamp_log=clamp_log, device=device)
+    def __init__(self, modelParameters, geometry, precision="fp64", clamp_log=False, device=None, kernels="auto"):
+        super().__init__("log", modelParameters, geometry, precision=precision, clamp_log=clamp_log, device=device,
+                         kernels=kernels)
 
     def Get_local_phi(self):
         """Gaussian-coarsened phi (models/logpfc/simulation.py:232-242)."""
         return self._get_local()
 
 
-def BuildB200_Simulation(modelParameters, geometry, precision="fp64", clamp_log=False, device=None):
-    return Simulation(modelParameters, geometry, precision=precision, clamp_log=clamp_log, device=device)
+def BuildB200_Simulation(modelParameters, geometry, precision="fp64", clamp_log=False, device=None, kernels="auto"):
+    return Simulation(modelParameters, geometry, precision=precision, clamp_log=clamp_log, device=device,
+                      kernels=kernels)
 
 
 def BuildCupyGPU_Simulation(modelParameters, geometry, *_, precision="fp64", **__):

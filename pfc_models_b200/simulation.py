@@ -131,10 +131,12 @@ class Plan:
         return v.value
 
     def info(self):
-        o = (ctypes.c_int64 * 8)()
+        o = (ctypes.c_int64 * 16)()
         _lib.check(self.lib.pfc_plan_info(self.handle, o))
         keys = ("rows_per_cta", "row_threads_per_fft", "row_ctas", "cols_per_cta",
-                "col_threads_per_fft", "col_ctas", "row_smem", "col_smem")
+                "col_threads_per_fft", "col_ctas", "row_smem", "col_smem",
+                "fast", "fast_rows_per_cta", "fast_row_threads", "fast_row_ctas", "fast_row_smem",
+                "fast_col_threads", "fast_col_ctas", "fast_col_smem")
         return dict(zip(keys, list(o)))
 
     def launches(self):
@@ -340,7 +342,8 @@ class _SimulationState:
 class Simulation:
     """The reference's Simulation (models/stdpfc/simulation.py:166-268) backed by a plan."""
 
-    def __init__(self, model: str, modelParameters, geometry, precision="fp64", clamp_log=False, device=None):
+    def __init__(self, model: str, modelParameters, geometry, precision="fp64", clamp_log=False, device=None,
+                 kernels="auto"):
         if model not in ("std", "log"):
             raise ValueError(f"model must be 'std' or 'log', got {model!r}")
         if precision not in _PRECISIONS:
@@ -360,6 +363,9 @@ class Simulation:
         prob.small_z_tol = float(getattr(m, "smallZTol", 2e-5))
         prob.min_phi = float(getattr(m, "minPhi", 0.0) or 0.0)
         prob.clamp_log = 1 if clamp_log else 0
+        if kernels not in ("auto", "generic"):
+            raise ValueError(f"kernels must be 'auto' or 'generic', got {kernels!r}")
+        prob.flags = 1 if kernels == "generic" else 0
         self._plan = Plan(prob, device)
         self._version = 0
         self._mu_current = False
