@@ -19,16 +19,17 @@
 
 namespace pfc {
 
-template <int N, int EE_REQ>
+template <int N, int EE_REQ, int RMAX>
 struct FastSeq {
   __host__ __device__ static constexpr int lg(int x) { return x <= 1 ? 0 : 1 + lg(x >> 1); }
   static constexpr int EE = EE_REQ < N ? EE_REQ : N;     // elements per thread
   static constexpr int TPF = N / EE;                      // threads per transform
-  static constexpr int LN = lg(N), LE = lg(EE);
+  static constexpr int RC = RMAX < EE ? RMAX : EE;        // radix of the full passes
+  static constexpr int LN = lg(N), LE = lg(RC);
   static constexpr int NPASS = (LN + LE - 1) / LE;
   static constexpr int LAST = 1 << (LN - (NPASS - 1) * LE);
-  __host__ __device__ static constexpr int radA(int p) { return p == NPASS - 1 ? LAST : EE; }
-  __host__ __device__ static constexpr int radB(int p) { return p == 0 ? LAST : EE; }
+  __host__ __device__ static constexpr int radA(int p) { return p == NPASS - 1 ? LAST : RC; }
+  __host__ __device__ static constexpr int radB(int p) { return p == 0 ? LAST : RC; }
   __host__ __device__ static constexpr int nsA(int p) { return p == 0 ? 1 : nsA(p - 1) * radA(p - 1); }
   __host__ __device__ static constexpr int nsB(int p) { return p == 0 ? 1 : nsB(p - 1) * radB(p - 1); }
   // offset of pass p's twiddle table ([k][q-1], k < ns, q < R) within the sequence table
@@ -38,10 +39,13 @@ struct FastSeq {
   __host__ __device__ static constexpr int sizeB() { return twB(NPASS); }
 };
 
-template <class T> struct PadShift { static constexpr int value = 4; };   // 16 x 8 B per 128 B
-template <> struct PadShift<double> { static constexpr int value = 3; };  // 8 x 16 B per 128 B
+// pad one element per 2^P: P = 5 for complex float (radix-32 passes), 4 for complex double
+template <class T> struct PadShift { static constexpr int value = 5; };
+template <> struct PadShift<double> { static constexpr int value = 4; };
 
 template <int P> __device__ __forceinline__ int padi(int i) { return i + (i >> P); }
+
+template <class T> struct RadixCap { static constexpr int value = 1 << PadShift<T>::value; };
 
 __device__ __forceinline__ float2 ldg2(const float2* p) { return __ldg(p); }
 __device__ __forceinline__ double2 ldg2(const double2* p) { return __ldg(p); }
@@ -65,17 +69,39 @@ __device__ __forceinline__ void group_sync(int g) {
   }
 }
 
+// Issues asynchronous copies of n elements from global to shared memory (all threads
+// of the CTA take part); the caller commits and waits.
+template <class T>
+__device__ __forceinline__ void stage_async(cplx<T>* dst, const cplx<T>* src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst + i);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src + i), "n"(sizeof(cplx<T>))
+                 : "memory");
+  }
+}
+
 // One Stockham pass of radix R, stride NS, on a length-N transform whose group has
 // TPF threads holding EE = R * NB values each (v[b * R + q], butterfly j = t + b * TPF).
 template <class T, int N, int EE, int R, int NS, int P>
 struct FastPass {
   static constexpr int TPF = N / EE, NB = EE / R, NR = N / R;
+  // padi(x + q * S) = padi(x) + q * (S + S / 2^P) whenever 2^P divides S
+  static constexpr int NRP = NR + (NR >> P);
+  static constexpr bool LIN_LOAD = (NR % (1 << P)) == 0;
+  static constexpr bool LIN_STORE = (NS % (1 << P)) == 0 || NS == 1;
+  static constexpr int NSP = NS == 1 ? 1 : NS + (NS >> P);
   static __device__ __forceinline__ void load(const cplx<T>* buf, cplx<T>* v, int t) {
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
       const int j = t + b * TPF;
+      if constexpr (LIN_LOAD) {
+        const cplx<T>* p = buf + padi<P>(j);
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[b * R + q] = buf[padi<P>(j + q * NR)];
+        for (int q = 0; q < R; ++q) v[b * R + q] = p[q * NRP];
+      } else {
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[b * R + q] = buf[padi<P>(j + q * NR)];
+      }
     }
   }
   template <bool INV>
@@ -99,14 +125,22 @@ struct FastPass {
       dft<R, INV>(v + b * R, (const cplx<T>*)nullptr);
     }
   }
+  // NS == 1: the R outputs of a butterfly are consecutive and R divides 2^P, so they
+  // never straddle a pad
   static __device__ __forceinline__ void store(cplx<T>* buf, const cplx<T>* v, int t) {
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
       const int j = t + b * TPF;
       const int k = j & (NS - 1);
       const int base = (j - k) * R + k;
+      if constexpr (LIN_STORE) {
+        cplx<T>* p = buf + padi<P>(base);
 #pragma unroll
-      for (int q = 0; q < R; ++q) buf[padi<P>(base + q * NS)] = v[b * R + q];
+        for (int q = 0; q < R; ++q) p[q * NSP] = v[b * R + q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < R; ++q) buf[padi<P>(base + q * NS)] = v[b * R + q];
+      }
     }
   }
   // natural-order index of register v[b * R + q] after the last pass (NS = N / R)
@@ -117,7 +151,7 @@ struct FastPass {
 template <class T, int N, int EE_REQ, bool SEQB, bool INV, int PA, int PB>
 __device__ __forceinline__ void fast_mid(cplx<T>* buf, cplx<T>* v, int t, int g, const cplx<T>* __restrict__ tw) {
   if constexpr (PA < PB) {
-    using S = FastSeq<N, EE_REQ>;
+    using S = FastSeq<N, EE_REQ, RadixCap<T>::value>;
     constexpr int P = PadShift<T>::value;
     constexpr int R = SEQB ? S::radB(PA) : S::radA(PA);
     constexpr int NS = SEQB ? S::nsB(PA) : S::nsA(PA);
@@ -159,15 +193,19 @@ struct FastColArgs {
 };
 
 template <int TPF> struct FastBound { static constexpr int value = TPF > 256 ? TPF : 256; };
+// minimum resident CTAs per SM requested from the register allocator (256-thread CTAs)
+template <int TPF> struct FastMinBlocks { static constexpr int value = TPF > 256 ? 1 : 2; };
+template <int TPF> struct FastColMinBlocks { static constexpr int value = TPF > 256 ? 1 : 2; };
 
 // ------------------------------------------------------------------ row kernel
 // CTA: `rows` consecutive rows (tile), groups of TPF threads each process rows
 // g, g + ngroups, ... The tile is staged through shared memory with a transposing
 // load/store (global layout is column-major).
 template <class T, int M, int EE_REQ, int MODEL>
-__global__ void __launch_bounds__(FastBound<FastSeq<M, EE_REQ>::TPF>::value)
+__global__ void __launch_bounds__(FastBound<FastSeq<M, EE_REQ, RadixCap<T>::value>::TPF>::value,
+                  FastMinBlocks<FastSeq<M, EE_REQ, RadixCap<T>::value>::TPF>::value)
 row_step_fast(FastRowArgs<T> a) {
-  using S = FastSeq<M, EE_REQ>;
+  using S = FastSeq<M, EE_REQ, RadixCap<T>::value>;
   constexpr int P = PadShift<T>::value;
   constexpr int EE = S::EE, TPF = S::TPF, NP = S::NPASS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -178,13 +216,25 @@ row_step_fast(FastRowArgs<T> a) {
   const int g = threadIdx.x / TPF, t = threadIdx.x - g * TPF;
   const bool dev = (sizeof(T) == 4);
 
-  // ---- transposing tile load: element (kx, y0 + r) -> sm[r * ld + pad(kx)]
+  // ---- transposing tile load: element (kx, y0 + r) -> sm[r * ld + pad(kx)], issued as
+  // asynchronous global->shared copies so that every load of the tile is in flight at once
   for (int i = threadIdx.x; i < rows * M; i += blockDim.x) {
     const int r = i % rows, kx = i / rows;
-    cplx<T> v = mk(T(0), T(0));
-    if (y0 + r < ny) v = a.in[(size_t)kx * ny + (y0 + r)];
-    sm[r * ld + padi<P>(kx)] = v;
+    cplx<T>* dst = sm + r * ld + padi<P>(kx);
+    if (y0 + r < ny) {
+      const unsigned sdst = (unsigned)__cvta_generic_to_shared(dst);
+      const cplx<T>* src = a.in + (size_t)kx * ny + (y0 + r);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sdst), "l"(src), "n"(sizeof(cplx<T>))
+                   : "memory");
+    } else {
+      *dst = mk(T(0), T(0));
+    }
   }
+  // twiddle tables are read through the L1 cache
+  const cplx<T>* twA_s = a.twA;
+  const cplx<T>* twB_s = a.twB;
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
 
   // nonlinearity parameters
@@ -226,17 +276,17 @@ row_step_fast(FastRowArgs<T> a) {
     }
     group_sync<TPF>(g);
     if constexpr (NP == 1) {
-      FastPass<T, M, EE, S::radA(0), 1, P>::template compute<true>(v, t, a.twA);
+      FastPass<T, M, EE, S::radA(0), 1, P>::template compute<true>(v, t, twA_s);
     } else {
       using P0 = FastPass<T, M, EE, S::radA(0), 1, P>;
-      P0::template compute<true>(v, t, a.twA);
+      P0::template compute<true>(v, t, twA_s);
       P0::store(row, v, t);
       group_sync<TPF>(g);
-      fast_mid<T, M, EE_REQ, false, true, 1, NP - 1>(row, v, t, g, a.twA);
+      fast_mid<T, M, EE_REQ, false, true, 1, NP - 1>(row, v, t, g, twA_s);
       using PL = FastPass<T, M, EE, S::radA(NP - 1), S::nsA(NP - 1), P>;
       PL::load(row, v, t);
       group_sync<TPF>(g);
-      PL::template compute<true>(v, t, a.twA + S::twA(NP - 1));
+      PL::template compute<true>(v, t, twA_s + S::twA(NP - 1));
     }
     // ---- v holds z[e] = n[2e] + i n[2e+1]: the nonlinearity, in registers
 #pragma unroll
@@ -253,17 +303,17 @@ row_step_fast(FastRowArgs<T> a) {
     // ---- forward sequence B
     constexpr int RL = S::radB(NP - 1);
     if constexpr (NP == 1) {
-      FastPass<T, M, EE, S::radB(0), 1, P>::template compute<false>(v, t, a.twB);
+      FastPass<T, M, EE, S::radB(0), 1, P>::template compute<false>(v, t, twB_s);
     } else {
       using Q0 = FastPass<T, M, EE, S::radB(0), 1, P>;
-      Q0::template compute<false>(v, t, a.twB);
+      Q0::template compute<false>(v, t, twB_s);
       Q0::store(row, v, t);
       group_sync<TPF>(g);
-      fast_mid<T, M, EE_REQ, true, false, 1, NP - 1>(row, v, t, g, a.twB);
+      fast_mid<T, M, EE_REQ, true, false, 1, NP - 1>(row, v, t, g, twB_s);
       using QL = FastPass<T, M, EE, RL, S::nsB(NP - 1), P>;
       QL::load(row, v, t);
       group_sync<TPF>(g);
-      QL::template compute<false>(v, t, a.twB + S::twB(NP - 1));
+      QL::template compute<false>(v, t, twB_s + S::twB(NP - 1));
     }
     // ---- forward-real post-twiddle: publish Z, read the (k, M - k) partners
     using QO = FastPass<T, M, EE, RL, M / RL, P>;
@@ -309,9 +359,10 @@ row_step_fast(FastRowArgs<T> a) {
 // reads and writes go straight between registers and HBM (the first pass of each
 // sequence reads, and the last pass writes, consecutive elements per lane).
 template <class T, int NY, int EE_REQ>
-__global__ void __launch_bounds__(FastBound<FastSeq<NY, EE_REQ>::TPF>::value)
+__global__ void __launch_bounds__(FastBound<FastSeq<NY, EE_REQ, RadixCap<T>::value>::TPF>::value,
+                                  FastColMinBlocks<FastSeq<NY, EE_REQ, RadixCap<T>::value>::TPF>::value)
 col_step_fast(FastColArgs<T> a) {
-  using S = FastSeq<NY, EE_REQ>;
+  using S = FastSeq<NY, EE_REQ, RadixCap<T>::value>;
   constexpr int P = PadShift<T>::value;
   constexpr int EE = S::EE, TPF = S::TPF, NP = S::NPASS;
   constexpr int PADN = NY + (NY >> P) + 2;
@@ -320,7 +371,9 @@ col_step_fast(FastColArgs<T> a) {
   const int ngroups = blockDim.x / TPF;
   const int g = threadIdx.x / TPF, t = threadIdx.x - g * TPF;
   const int kx = blockIdx.x * ngroups + g;      // m is a multiple of ngroups
-  cplx<T>* buf = sm + g * PADN;
+  const cplx<T>* twA_s = a.twA;                   // twiddle tables, read through L1
+  const cplx<T>* twB_s = a.twB;
+  cplx<T>* buf = sm + g * PADN;                   // exchange buffer of this column
   const int m = a.m, nyh = a.nyh;
   cplx<T> v[EE];
 
@@ -334,17 +387,17 @@ col_step_fast(FastColArgs<T> a) {
       for (int q = 0; q < R; ++q) v[b * R + q] = col[t + b * TPF + q * NR];
   }
   if constexpr (NP == 1) {
-    FastPass<T, NY, EE, S::radA(0), 1, P>::template compute<false>(v, t, a.twA);
+    FastPass<T, NY, EE, S::radA(0), 1, P>::template compute<false>(v, t, twA_s);
   } else {
     using P0 = FastPass<T, NY, EE, S::radA(0), 1, P>;
-    P0::template compute<false>(v, t, a.twA);
+    P0::template compute<false>(v, t, twA_s);
     P0::store(buf, v, t);
     group_sync<TPF>(g);
-    fast_mid<T, NY, EE_REQ, false, false, 1, NP - 1>(buf, v, t, g, a.twA);
+    fast_mid<T, NY, EE_REQ, false, false, 1, NP - 1>(buf, v, t, g, twA_s);
     using PL = FastPass<T, NY, EE, S::radA(NP - 1), S::nsA(NP - 1), P>;
     PL::load(buf, v, t);
     group_sync<TPF>(g);
-    PL::template compute<false>(v, t, a.twA + S::twA(NP - 1));
+    PL::template compute<false>(v, t, twA_s + S::twA(NP - 1));
   }
 
   // ---- ETD1 update on the natural-order values held in registers
@@ -399,16 +452,16 @@ col_step_fast(FastColArgs<T> a) {
 
   // ---- inverse sequence B; the last pass writes W to HBM
   if constexpr (NP == 1) {
-    FastPass<T, NY, EE, S::radB(0), 1, P>::template compute<true>(v, t, a.twB);
+    FastPass<T, NY, EE, S::radB(0), 1, P>::template compute<true>(v, t, twB_s);
   } else {
     using Q0 = FastPass<T, NY, EE, S::radB(0), 1, P>;
-    Q0::template compute<true>(v, t, a.twB);
+    Q0::template compute<true>(v, t, twB_s);
     Q0::store(buf, v, t);
     group_sync<TPF>(g);
-    fast_mid<T, NY, EE_REQ, true, true, 1, NP - 1>(buf, v, t, g, a.twB);
+    fast_mid<T, NY, EE_REQ, true, true, 1, NP - 1>(buf, v, t, g, twB_s);
     using QL = FastPass<T, NY, EE, S::radB(NP - 1), S::nsB(NP - 1), P>;
     QL::load(buf, v, t);
-    QL::template compute<true>(v, t, a.twB + S::twB(NP - 1));
+    QL::template compute<true>(v, t, twB_s + S::twB(NP - 1));
   }
   {
     constexpr int RB = S::radB(NP - 1), NBB = EE / RB;

@@ -105,6 +105,32 @@ template <bool INV, class T> __device__ __forceinline__ void dft16(cplx<T>* v) {
   for (int k = 0; k < 8; ++k) { v[k] = e[k] + o[k]; v[k + 8] = e[k] - o[k]; }
 }
 
+// 32 points: two 16-point DFTs of the even and odd elements, twiddles
+// exp(-+ 2 pi i k / 32), k = 0..15, and a final radix-2 combination.
+template <bool INV, class T> __device__ __forceinline__ void dft32(cplx<T>* v) {
+  cplx<T> e[16], o[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) { e[k] = v[2 * k]; o[k] = v[2 * k + 1]; }
+  dft16<INV>(e); dft16<INV>(o);
+  // cos and sin of k pi / 16, k = 0..15
+  const T cs[16] = {T(1.0), T(0.98078528040323044912618223613424), T(0.92387953251128675612818318939679),
+                    T(0.83146961230254523707878837761791), T(0.70710678118654752440084436210485),
+                    T(0.55557023301960222474283081394853), T(0.38268343236508977172845998403040),
+                    T(0.19509032201612826784828486847702), T(0.0), T(-0.19509032201612826784828486847702),
+                    T(-0.38268343236508977172845998403040), T(-0.55557023301960222474283081394853),
+                    T(-0.70710678118654752440084436210485), T(-0.83146961230254523707878837761791),
+                    T(-0.92387953251128675612818318939679), T(-0.98078528040323044912618223613424)};
+#pragma unroll
+  for (int k = 1; k < 16; ++k) {
+    if (k == 8) { o[k] = rot4<INV>(o[k]); continue; }
+    const T s = cs[(k + 8) & 15] * (k < 8 ? T(-1) : T(1));  // sin(k pi / 16) = -cos((k + 8) pi / 16), k < 8
+    cplx<T> w = mk(cs[k], INV ? s : -s);
+    o[k] = cmul(o[k], w);
+  }
+#pragma unroll
+  for (int k = 0; k < 16; ++k) { v[k] = e[k] + o[k]; v[k + 16] = e[k] - o[k]; }
+}
+
 template <bool INV, class T> __device__ __forceinline__ void dft3(cplx<T>* v) {
   const T h = T(0.86602540378443864676372317075294);  // sqrt(3)/2
   cplx<T> s = v[1] + v[2], d = v[1] - v[2];
@@ -154,6 +180,7 @@ template <int R, bool INV, class T> __device__ __forceinline__ void dft(cplx<T>*
   else if constexpr (R == 4) dft4<INV>(v);
   else if constexpr (R == 8) dft8<INV>(v);
   else if constexpr (R == 16) dft16<INV>(v);
+  else if constexpr (R == 32) dft32<INV>(v);
   else dft_odd<R, INV>(v, roots);
 }
 

@@ -62,7 +62,8 @@ bool factorize(int n, bool fp32, std::vector<int>& radices) {
   return n == 1 && (int)radices.size() <= kMaxPass;
 }
 
-constexpr int kBlockMax = 256;  // PFC_LB in pfc_kernels.cuh
+constexpr int kBlockMax = 256;  // default launch bound of the generic kernels
+constexpr int pfc_block_max = kBlockMax;
 constexpr int kMaxElemsF = PFC_MAXE_F, kMaxElemsD = PFC_MAXE_D;  // as MaxElems in pfc_fft.cuh
 
 // must match MaxBfly in pfc_fft.cuh
@@ -205,20 +206,29 @@ ColArgs<T> col_args(const pfc_plan* h) {
 // The nonlinearity only matters in the step and reduce modes; other modes use the std instance.
 template <int MODE> constexpr bool row_uses_model() { return MODE == kRowStep || MODE == kRowReduce; }
 
-template <class T, int MODE, int MODEL, int RSET>
-void* row_fn() { return (void*)row_kernel<T, MODE, MODEL, RSET>; }
+// Radix-set codes of a plan: kRadixPow2 / kRadixAll select the 256-thread kernels;
+// kRadixPow2Big selects the power-of-two kernels built for 1024-thread blocks,
+// used when one transform needs more than 256 threads (>= 8192 points in FP32).
+constexpr int kRadixPow2Big = 2;
+
+template <class T, int MODE, int MODEL, int RSET, int LB>
+void* row_fn() { return (void*)row_kernel<T, MODE, MODEL, RSET, LB>; }
 
 template <class T, int MODE>
 void* pick_row(int model, int rset) {
   const bool log = row_uses_model<MODE>() && model == kModelLog;
-  if (rset == kRadixPow2) return log ? row_fn<T, MODE, kModelLog, kRadixPow2>() : row_fn<T, MODE, kModelStd, kRadixPow2>();
-  return log ? row_fn<T, MODE, kModelLog, kRadixAll>() : row_fn<T, MODE, kModelStd, kRadixAll>();
+  if (rset == kRadixPow2Big)
+    return log ? row_fn<T, MODE, kModelLog, kRadixPow2, 1024>() : row_fn<T, MODE, kModelStd, kRadixPow2, 1024>();
+  if (rset == kRadixPow2)
+    return log ? row_fn<T, MODE, kModelLog, kRadixPow2, 256>() : row_fn<T, MODE, kModelStd, kRadixPow2, 256>();
+  return log ? row_fn<T, MODE, kModelLog, kRadixAll, 256>() : row_fn<T, MODE, kModelStd, kRadixAll, 256>();
 }
 
 template <class T, int MODE>
 void* pick_col(int rset) {
-  if (MODE == kColParseval || MODE == kColExport || rset == kRadixPow2) return (void*)col_kernel<T, MODE, kRadixPow2>;
-  return (void*)col_kernel<T, MODE, kRadixAll>;
+  if (rset == kRadixPow2Big) return (void*)col_kernel<T, MODE, kRadixPow2, 1024>;
+  if (MODE == kColParseval || MODE == kColExport || rset == kRadixPow2) return (void*)col_kernel<T, MODE, kRadixPow2, 256>;
+  return (void*)col_kernel<T, MODE, kRadixAll, 256>;
 }
 
 template <class T, int MODE>
@@ -259,7 +269,9 @@ int set_smem_attrs(pfc_plan* h) {
 }
 
 // ---- specialised power-of-two path (pfc_fast.cuh)
-template <class T> constexpr int fast_ee() { return sizeof(T) == 4 ? 16 : 8; }
+// elements per thread of the row and column step kernels
+template <class T> constexpr int fast_ee_row() { return sizeof(T) == 4 ? 32 : 16; }
+template <class T> constexpr int fast_ee_col() { return sizeof(T) == 4 ? 32 : 16; }
 constexpr int kFastMinLog = 5, kFastMaxLogRow = 12, kFastMaxLogCol = 13;
 
 int ilog2_exact(int n) {
@@ -270,9 +282,9 @@ int ilog2_exact(int n) {
 
 // Pass tables of sequences A and B for an N-point transform, laid out as FastSeq
 // expects: for p = 1 .. NPASS-1, ns(p) x (R(p) - 1) entries exp(-2 pi i q k / (ns R)).
-template <class T, int N>
+template <class T, int N, int EE>
 void fast_tables(std::vector<long double>& tw, int& offA, int& offB) {
-  using S = FastSeq<N, fast_ee<T>()>;
+  using S = FastSeq<N, EE, RadixCap<T>::value>;
   const long double twopi = 6.283185307179586476925286766559L;
   for (int seq = 0; seq < 2; ++seq) {
     (seq == 0 ? offA : offB) = (int)(tw.size() / 2);
@@ -289,19 +301,31 @@ void fast_tables(std::vector<long double>& tw, int& offA, int& offB) {
   }
 }
 
-template <class T, int L>
+template <class T, bool COL, int L>
 void fast_tables_l(int lg, std::vector<long double>& tw, int& a, int& b) {
   if constexpr (L <= kFastMaxLogCol) {
-    if (lg == L) { fast_tables<T, (1 << L)>(tw, a, b); return; }
-    fast_tables_l<T, L + 1>(lg, tw, a, b);
+    if (lg == L) { fast_tables<T, (1 << L), COL ? fast_ee_col<T>() : fast_ee_row<T>()>(tw, a, b); return; }
+    fast_tables_l<T, COL, L + 1>(lg, tw, a, b);
   }
 }
 
-template <class T, int L>
+template <class T, bool COL, int L>
 int fast_tpf_l(int lg) {
   if constexpr (L <= kFastMaxLogCol) {
-    if (lg == L) return FastSeq<(1 << L), fast_ee<T>()>::TPF;
-    return fast_tpf_l<T, L + 1>(lg);
+    if (lg == L) return FastSeq<(1 << L), COL ? fast_ee_col<T>() : fast_ee_row<T>(), RadixCap<T>::value>::TPF;
+    return fast_tpf_l<T, COL, L + 1>(lg);
+  } else {
+    return 0;
+  }
+}
+
+// elements of the sequence A and B twiddle tables staged in shared memory
+template <class T, bool COL, int L>
+int fast_tw_elems_l(int lg) {
+  if constexpr (L <= kFastMaxLogCol) {
+    using S = FastSeq<(1 << L), COL ? fast_ee_col<T>() : fast_ee_row<T>(), RadixCap<T>::value>;
+    if (lg == L) return S::sizeA() + S::sizeB();
+    return fast_tw_elems_l<T, COL, L + 1>(lg);
   } else {
     return 0;
   }
@@ -310,7 +334,7 @@ int fast_tpf_l(int lg) {
 template <class T, int MODEL, int L>
 void* fast_row_l(int lg) {
   if constexpr (L <= kFastMaxLogRow) {
-    if (lg == L) return (void*)row_step_fast<T, (1 << L), fast_ee<T>(), MODEL>;
+    if (lg == L) return (void*)row_step_fast<T, (1 << L), fast_ee_row<T>(), MODEL>;
     return fast_row_l<T, MODEL, L + 1>(lg);
   } else {
     return nullptr;
@@ -320,7 +344,7 @@ void* fast_row_l(int lg) {
 template <class T, int L>
 void* fast_col_l(int lg) {
   if constexpr (L <= kFastMaxLogCol) {
-    if (lg == L) return (void*)col_step_fast<T, (1 << L), fast_ee<T>()>;
+    if (lg == L) return (void*)col_step_fast<T, (1 << L), fast_ee_col<T>()>;
     return fast_col_l<T, L + 1>(lg);
   } else {
     return nullptr;
@@ -335,26 +359,35 @@ int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
     return PFC_OK;
   constexpr int P = PadShift<T>::value;
   const int elt = (int)sizeof(cplx<T>);
-  fast_tables_l<T, kFastMinLog>(lm, tw, h->tw_ra, h->tw_rb);
-  fast_tables_l<T, kFastMinLog>(ly, tw, h->tw_ca, h->tw_cb);
+  fast_tables_l<T, false, kFastMinLog>(lm, tw, h->tw_ra, h->tw_rb);
+  fast_tables_l<T, true, kFastMinLog>(ly, tw, h->tw_ca, h->tw_cb);
   // row kernel: tile of fr_rows rows (>= 64 B per kx run), groups of tpf threads
-  const int tpr = fast_tpf_l<T, kFastMinLog>(lm);
+  const int tpr = fast_tpf_l<T, false, kFastMinLog>(lm);
   int ngr = std::max(1, 256 / tpr);
-  int rows = sizeof(T) == 4 ? 8 : 4;
+  int rows = sizeof(T) == 4 ? 8 : 4;  // 64 B of a column per tile
+  const size_t row_tables = 0;  // twiddle tables stay in global memory (L1-cached)
+  // smaller tiles for long rows so that the tile fits the shared-memory budget
+  while (rows > 1 && (size_t)rows * (h->m + (h->m >> P) + (1 << P)) * elt + row_tables > 200 * 1024) rows /= 2;
   ngr = std::min(ngr, rows);
   rows = std::max(rows, ngr);
+  // row stride in shared memory: with S = 128 B / element slots per bank cycle,
+  // ld = S / rows (mod S) makes the transposing loads and stores of a warp hit
+  // distinct banks
+  const int slots = 128 / elt;
+  const int want = (slots / rows) % slots;
   int ld = h->m + (h->m >> P);
-  while (ld % (1 << P) != 2) ++ld;
+  while (ld % slots != want) ++ld;
   h->fr_rows = rows;
   h->fr_threads = ngr * tpr;
   h->fr_ld = ld;
   h->fr_grid = (h->ny + rows - 1) / rows;
-  h->fr_smem = (size_t)rows * ld * elt;
+  h->fr_smem = (size_t)rows * ld * elt + row_tables;
   // column kernel: one group of tpc threads per column
-  const int tpc = fast_tpf_l<T, kFastMinLog>(ly);
+  const int tpc = fast_tpf_l<T, true, kFastMinLog>(ly);
   const int ngc = std::min(std::max(1, 256 / tpc), h->m);
   h->fc_threads = ngc * tpc;
   h->fc_grid = h->m / ngc;
+  // one exchange buffer per column
   h->fc_smem = (size_t)ngc * (h->ny + (h->ny >> P) + 2) * elt;
   if (h->fr_threads > 1024 || h->fc_threads > 1024 || h->fr_smem > 200 * 1024 || h->fc_smem > 200 * 1024)
     return PFC_OK;  // generic path
@@ -676,6 +709,8 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   {
     h->row_tpf = threads_per_fft(rrow, m, h->fp32);
     h->row_ld = m + 1;
+    if (h->row_tpf > kBlockMax && h->row_rset == kRadixPow2 && h->row_tpf <= 1024) h->row_rset = kRadixPow2Big;
+    const int kBlockMax = h->row_rset == kRadixPow2Big ? 1024 : pfc_block_max;
     if (h->row_tpf > kBlockMax)
       return cleanup_fail(fail(PFC_E_ARG, "pfc_plan_create: row transform of %d points needs %d threads", m, h->row_tpf));
     const int rows_min = std::max(1, 32 / h->row_tpf);       // whole warps
@@ -694,6 +729,8 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   {
     h->col_tpf = threads_per_fft(rcol, p->ny, h->fp32);
     h->col_ld = p->ny;
+    if (h->col_tpf > kBlockMax && h->col_rset == kRadixPow2 && h->col_tpf <= 1024) h->col_rset = kRadixPow2Big;
+    const int kBlockMax = h->col_rset == kRadixPow2Big ? 1024 : pfc_block_max;
     if (h->col_tpf > kBlockMax)
       return cleanup_fail(fail(PFC_E_ARG, "pfc_plan_create: column transform of %d points needs %d threads", p->ny, h->col_tpf));
     int cols = std::max(1, 32 / h->col_tpf);

@@ -171,7 +171,15 @@ class DeviceArray:
 
     # host views
     def get(self):
-        return self._tensor().cpu().numpy()
+        """Host copy (a new NumPy array), staged through a pinned buffer."""
+        t = self._tensor()
+        stage = getattr(self, "_stage", None)
+        if stage is None or stage.shape != t.shape or stage.dtype != t.dtype:
+            import torch
+            stage = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            self._stage = stage
+        stage.copy_(t)
+        return stage.numpy().copy()
 
     def __array__(self, dtype=None, copy=None):
         a = self.get()

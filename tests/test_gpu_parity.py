@@ -334,8 +334,8 @@ def test_fp32_log_near_singular():
 
 
 # ------------------------------------------------------------------ power-of-two kernels vs the generic kernels
-FAST_SIZES = [(64, 64), (128, 32), (32, 128), (256, 256), (512, 128), (1024, 1024), (2048, 256), (256, 2048),
-              (8192, 64), (64, 8192)]
+FAST_SIZES = [(64, 64), (128, 32), (64, 128), (256, 256), (512, 128), (1024, 1024), (2048, 256), (256, 2048),
+              (4096, 64)]
 
 
 @pytest.mark.parametrize("nx,ny", FAST_SIZES)
@@ -365,3 +365,21 @@ def test_fast_kernels_match_generic(nx, ny, precision, model):
     tol = 1e-13 if precision == "fp64" else 1e-5
     assert rel_l2(out["auto"][0] - mean, out["generic"][0] - mean) < tol
     assert out["auto"][1][0] == pytest.approx(out["generic"][1][0], rel=1e-12 if precision == "fp64" else 1e-6)
+
+
+@pytest.mark.parametrize("nx,ny", [(64, 8192), (8192, 32)])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_fast_kernels_long_transforms(nx, ny, precision):
+    """8192-point transforms (beyond the mixed-radix kernels' block size) against the
+    oracle: 6 steps, FP64 within 1e-12, FP32 within 2e-5 relative L2."""
+    prm = dict(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.3, g=0.2, dt=0.3)
+    geom_o = orc.build_geometry(nx, ny, nx * np.pi / 4, ny * np.pi / 4)
+    f0 = -0.3 + 0.05 * np.random.default_rng(nx + ny).uniform(-1, 1, (ny, nx))
+    ref, _ = orc.run("std", orc.Params(**prm), geom_o, f0, 6)
+    geom = stdpfc.Build2DGeometry(nx, ny, nx * np.pi / 4, ny * np.pi / 4)
+    sim = stdpfc.BuildB200_Simulation(stdpfc.BuildStdPFCModelParameters(**prm), geom, precision=precision)
+    assert sim.plan.info()["fast"] == 1
+    sim.State.n[...] = f0
+    sim.TimeSteps(6)
+    tol = 1e-12 if precision == "fp64" else 2e-5
+    assert rel_l2(sim.State.n.get() + 0.3, ref + 0.3) < tol
