@@ -141,6 +141,22 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
 /* Kernel launches issued by this plan since creation (for accounting). */
 int64_t pfc_launch_count(pfc_plan* plan);
 
+/* The mean of `count` FP64 values at dev_field, summed with compensation
+ * (Neumaier) on the device, written as one double to dev_mean. This entry point
+ * has no counterpart in the reference. It exists for callers that must not
+ * allocate device memory: code running while another allocator (a caching pool
+ * such as PyTorch's) has reserved the GPU's memory, where an allocation here
+ * could fail part-way through a run, and loops that cannot afford cudaFree,
+ * which waits for all work on the device. It allocates nothing: its partial sums
+ * live in a fixed array of 128 KiB that every GPU loading this library holds
+ * until the process exits, so count may be at most 2^26 (an 8192 x 8192
+ * field); larger counts return PFC_E_ARG. The first call on each device looks
+ * up that array's device address; make that first call before any stream
+ * capture. All calls share the array: calls whose kernels overlap on the GPU
+ * (other streams, other host threads) race and give wrong results. Needs no
+ * plan. Stream-ordered. */
+int pfc_field_mean_noalloc(const double* dev_field, int64_t count, double* dev_mean, void* stream);
+
 /* Copies the last error message of this thread into buf (NUL-terminated). */
 int pfc_last_error(char* buf, size_t len);
 

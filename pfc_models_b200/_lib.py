@@ -38,6 +38,7 @@ SIGNATURES = {
     "pfc_status": (ctypes.c_int, [_vp, ctypes.POINTER(_i32)]),
     "pfc_plan_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64)]),
     "pfc_launch_count": (_i64, [_vp]),
+    "pfc_field_mean_noalloc": (ctypes.c_int, [_vp, _i64, _vp, _vp]),
 }
 
 

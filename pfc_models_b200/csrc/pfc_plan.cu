@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -923,3 +924,91 @@ int pfc_plan_info(pfc_plan* h, int64_t* o) {
 int64_t pfc_launch_count(pfc_plan* h) { return h ? h->launches : 0; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// pfc_field_mean_noalloc: the compensated mean of a real FP64 field, with its
+// per-CTA partial sums in a fixed device array instead of memory it allocates.
+namespace {
+
+constexpr int kNoallocThreads = 256;
+constexpr int kNoallocChunk = kNoallocThreads * 32;     // contiguous sites per CTA
+constexpr int kNoallocMaxBlocks = 8192;                 // CTA partials the array holds
+constexpr long long kNoallocMaxSites = (long long)kNoallocChunk * kNoallocMaxBlocks;  // 2^26 = 8192 x 8192
+constexpr int kNoallocMaxDevices = 64;
+
+// (sum, compensation) of CTA b at [2b, 2b + 2); the completion counter (an unsigned
+// int) at [2 * kNoallocMaxBlocks]. 128 KiB + 256 B on every GPU that loads the library.
+static __device__ __align__(256) double g_noalloc_scratch[2 * kNoallocMaxBlocks + 32];
+
+// Each CTA sums one chunk, the last CTA to finish merges the partials in CTA order
+// (the result does not depend on which CTA that is) and puts the counter back to 0.
+__global__ void __launch_bounds__(kNoallocThreads)
+noalloc_mean_kernel(const double* __restrict__ x, long long n, double inv_n, double* scratch, double* out) {
+  KSum acc[1] = {{0.0, 0.0}};
+  const long long base = (long long)blockIdx.x * kNoallocChunk;
+  const long long end = base + kNoallocChunk < n ? base + kNoallocChunk : n;
+  for (long long i = base + threadIdx.x; i < end; i += kNoallocThreads) ksum_add(acc[0], x[i]);
+  block_reduce_store<1>(acc, scratch + 2 * blockIdx.x);  // thread 0 writes the pair
+  unsigned int* done = reinterpret_cast<unsigned int*>(scratch + 2 * kNoallocMaxBlocks);
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  const volatile double* p = scratch;
+  KSum tot = {0.0, 0.0};
+  for (unsigned int b = 0; b < gridDim.x; ++b) {
+    KSum o = {p[2 * b], p[2 * b + 1]};
+    tot = ksum_merge(tot, o);
+  }
+  out[0] = (tot.s + tot.c) * inv_n;
+  *done = 0u;
+}
+
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device.
+int noalloc_scratch(double** out) {
+  int dev = 0;
+  PFC_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoallocMaxDevices)
+    return fail(PFC_E_ARG, "pfc_field_mean_noalloc: device %d is beyond the %d devices it supports", dev,
+                kNoallocMaxDevices);
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(PFC_E_CUDA, "pfc_field_mean_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
+                  cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return PFC_OK;
+}
+
+}  // namespace
+
+extern "C" int pfc_field_mean_noalloc(const double* dev_field, int64_t count, double* dev_mean, void* stream) {
+  if (!dev_field || !dev_mean) return fail(PFC_E_ARG, "pfc_field_mean_noalloc: null argument");
+  if (count <= 0) return fail(PFC_E_ARG, "pfc_field_mean_noalloc: count must be positive, got %lld", (long long)count);
+  if (count > kNoallocMaxSites)
+    return fail(PFC_E_ARG,
+                "pfc_field_mean_noalloc: %lld sites exceed the maximum of %lld (an 8192 x 8192 field) "
+                "that its fixed scratch array holds",
+                (long long)count, kNoallocMaxSites);
+  double* scratch = nullptr;
+  if (int rc = noalloc_scratch(&scratch)) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  // the completion counter must start at zero
+  PFC_CUDA(cudaMemsetAsync(scratch + 2 * kNoallocMaxBlocks, 0, sizeof(unsigned int), s));
+  const int blocks = (int)((count + kNoallocChunk - 1) / kNoallocChunk);
+  noalloc_mean_kernel<<<blocks, kNoallocThreads, 0, s>>>(dev_field, (long long)count, 1.0 / (double)count, scratch,
+                                                         dev_mean);
+  PFC_LAUNCHED();
+  return PFC_OK;
+}
