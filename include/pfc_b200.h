@@ -73,7 +73,7 @@ typedef struct pfc_problem {
   double small_z_tol;      /* ETD1 series threshold, kernels.py:55 (default 2e-5) */
   double min_phi;          /* log model: clamp floor when clamp_log != 0 */
   int32_t clamp_log;       /* 0: unclamped log, as the reference (logpfc/simulation.py:296) */
-  int32_t flags;           /* reserved, 0 */
+  int32_t flags;           /* PFC_FLAG_* bits, normally 0 */
 } pfc_problem;
 
 typedef struct pfc_plan pfc_plan;
@@ -98,7 +98,10 @@ int pfc_set_state(pfc_plan* plan, const double* dev_field, void* stream);
 int pfc_get_state(pfc_plan* plan, double* dev_field, void* stream);
 
 /* Replaces `for _ in range(nsteps): sim.TimeStep()` (models/stdpfc/simulation.py:225-235,
- * models/logpfc/simulation.py:220-230). Stream-ordered, no host synchronisation. */
+ * models/logpfc/simulation.py:220-230). Stream-ordered, no host synchronisation.
+ * Whole blocks of 16 steps are replayed from a CUDA graph that the plan records
+ * the first time it needs one (once per starting ping-pong parity; not with
+ * PFC_FLAG_NO_GRAPHS); the remaining steps are launched directly. */
 int pfc_step(pfc_plan* plan, int64_t nsteps, void* stream);
 
 /* pfc_step with instrumentation: also returns the summed device time (ms) of
@@ -137,9 +140,38 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
 
 /* problem.flags bits */
 #define PFC_FLAG_GENERIC_ONLY 1   /* do not use the power-of-two step kernels */
+#define PFC_FLAG_NO_GRAPHS 2      /* pfc_step launches every kernel directly */
 
 /* Kernel launches issued by this plan since creation (for accounting). */
 int64_t pfc_launch_count(pfc_plan* plan);
+
+/*
+ * Batches: many independent plans stepped in lockstep, as a phase-diagram scan
+ * steps hundreds of small simulations (the `ad.step(sim)` loop of
+ * phase_diagram/q0star.py:271-272, run once per point of a scan; adapter step,
+ * models/stdpfc_cpu/phase_diagram.py:278-279). Plans with the same sizes, step
+ * kernels and nonlinearity parameters (g, clamp, min_phi) form a class; each pass
+ * of a step is one launch per class with one grid row per plan, reading that
+ * plan's buffers from a device table. Whole blocks of 16 steps replay a recorded
+ * CUDA graph. All plans must use the power-of-two step kernels, one precision and
+ * one device (current when the batch is created); at most 65535 plans. The batch
+ * borrows the plans: destroy it before them. Each plan keeps its own state, so
+ * pfc_reduce / pfc_get_state work on any of them between batch steps.
+ */
+typedef struct pfc_batch pfc_batch;
+
+int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out);
+
+/* Advances every plan of the batch by nsteps. Every plan must hold a state and
+ * all must be at the same step parity (the same number of steps since their
+ * states were set, mod 2), else PFC_E_STATE. Stream-ordered. */
+int pfc_batch_step(pfc_batch* batch, int64_t nsteps, void* stream);
+
+int pfc_batch_destroy(pfc_batch* batch);
+
+/* Kernel launches issued by pfc_batch_step so far; number of classes. */
+int64_t pfc_batch_launch_count(pfc_batch* batch);
+int pfc_batch_classes(pfc_batch* batch);
 
 /* The mean of `count` FP64 values at dev_field, summed with compensation
  * (Neumaier) on the device, written as one double to dev_mean. This entry point

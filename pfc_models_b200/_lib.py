@@ -19,6 +19,7 @@ FP64_PLAIN, FP32_MIXED = 0, 1
 FIELD_N, FIELD_MU, FIELD_LOCAL_MU, FIELD_LOCAL_N, FIELD_NONLIN_MU = range(5)
 FIELD_OF_CURRENT = 0x100
 SPEC_N_HAT, SPEC_N_HAT_NOW = 0, 1
+FLAG_GENERIC_ONLY, FLAG_NO_GRAPHS = 1, 2
 
 # every symbol include/pfc_b200.h declares, with (restype, argtypes)
 _vp, _i32, _i64, _dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
@@ -39,6 +40,11 @@ SIGNATURES = {
     "pfc_plan_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64)]),
     "pfc_launch_count": (_i64, [_vp]),
     "pfc_field_mean_noalloc": (ctypes.c_int, [_vp, _i64, _vp, _vp]),
+    "pfc_batch_create": (ctypes.c_int, [ctypes.POINTER(_vp), _i32, ctypes.POINTER(_vp)]),
+    "pfc_batch_step": (ctypes.c_int, [_vp, _i64, _vp]),
+    "pfc_batch_destroy": (ctypes.c_int, [_vp]),
+    "pfc_batch_launch_count": (_i64, [_vp]),
+    "pfc_batch_classes": (ctypes.c_int, [_vp]),
 }
 
 

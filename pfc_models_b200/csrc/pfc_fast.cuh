@@ -166,9 +166,21 @@ __device__ __forceinline__ void fast_mid(cplx<T>* buf, cplx<T>* v, int t, int g,
   }
 }
 
+// Buffers of one plan of a batch (pfc_batch_*): the step kernels of a batched launch
+// take their per-plan pointers from entry blockIdx.y of a device table of these.
+struct BatchBufs {
+  const void* w;        // W (row input, column output)
+  void* v;              // V (row output, column input)
+  const void* nin;      // n_hat of the current state
+  void* nout;           // n_hat of the next state
+  const void* coef;     // (A, Bg)
+  const double* scal;   // deviation-form scalars
+};
+
 template <class T>
 struct FastRowArgs {
   int ny, rows, ld;
+  const BatchBufs* batch;    // null: one plan, the pointers below
   const cplx<T>* in;         // W, column-major [kx][y]
   cplx<T>* out;              // V, column-major
   const cplx<T>* twA;        // row sequence A table (inverse uses conjugates)
@@ -182,6 +194,7 @@ struct FastRowArgs {
 template <class T>
 struct FastColArgs {
   int m, ny, nyh;
+  const BatchBufs* batch;    // null: one plan, the pointers below
   const cplx<T>* in;         // V
   const cplx<T>* nin;        // n_hat
   cplx<T>* nout;             // n_hat'
@@ -215,6 +228,15 @@ row_step_fast(FastRowArgs<T> a) {
   const int ngroups = blockDim.x / TPF;
   const int g = threadIdx.x / TPF, t = threadIdx.x - g * TPF;
   const bool dev = (sizeof(T) == 4);
+  const cplx<T>* gin = a.in;
+  cplx<T>* gout = a.out;
+  const double* scal = a.scal;
+  if (a.batch) {
+    const BatchBufs& b = a.batch[blockIdx.y];
+    gin = static_cast<const cplx<T>*>(b.w);
+    gout = static_cast<cplx<T>*>(b.v);
+    scal = b.scal;
+  }
 
   // ---- transposing tile load: element (kx, y0 + r) -> sm[r * ld + pad(kx)], issued as
   // asynchronous global->shared copies so that every load of the tile is in flight at once
@@ -223,7 +245,7 @@ row_step_fast(FastRowArgs<T> a) {
     cplx<T>* dst = sm + r * ld + padi<P>(kx);
     if (y0 + r < ny) {
       const unsigned sdst = (unsigned)__cvta_generic_to_shared(dst);
-      const cplx<T>* src = a.in + (size_t)kx * ny + (y0 + r);
+      const cplx<T>* src = gin + (size_t)kx * ny + (y0 + r);
       asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sdst), "l"(src), "n"(sizeof(cplx<T>))
                    : "memory");
     } else {
@@ -241,12 +263,12 @@ row_step_fast(FastRowArgs<T> a) {
   float c1 = 0.f, c2 = 0.f, inv = 0.f, lmin = 0.f;
   double inv_d = 0.0, mphi_rel = 0.0;
   if (dev) {
-    c1 = (float)a.scal[kScalC1];
-    c2 = (float)a.scal[kScalC2];
-    inv = (float)a.scal[kScalInvMean];
-    inv_d = a.scal[kScalInvMean];
+    c1 = (float)scal[kScalC1];
+    c2 = (float)scal[kScalC2];
+    inv = (float)scal[kScalInvMean];
+    inv_d = scal[kScalInvMean];
     mphi_rel = a.min_phi * inv_d;
-    lmin = (float)a.scal[kScalLogMin];
+    lmin = (float)scal[kScalLogMin];
   }
 
   for (int r = g; r < rows; r += ngroups) {
@@ -350,7 +372,7 @@ row_step_fast(FastRowArgs<T> a) {
   // ---- transposing tile store
   for (int i = threadIdx.x; i < rows * M; i += blockDim.x) {
     const int r = i % rows, kx = i / rows;
-    if (y0 + r < ny) a.out[(size_t)kx * ny + (y0 + r)] = sm[r * ld + padi<P>(kx)];
+    if (y0 + r < ny) gout[(size_t)kx * ny + (y0 + r)] = sm[r * ld + padi<P>(kx)];
   }
 }
 
@@ -375,12 +397,25 @@ col_step_fast(FastColArgs<T> a) {
   const cplx<T>* twB_s = a.twB;
   cplx<T>* buf = sm + g * PADN;                   // exchange buffer of this column
   const int m = a.m, nyh = a.nyh;
+  const cplx<T>* gin = a.in;
+  const cplx<T>* gnin = a.nin;
+  cplx<T>* gnout = a.nout;
+  cplx<T>* gwout = a.wout;
+  const cplx<T>* gcoef = a.coef;
+  if (a.batch) {
+    const BatchBufs& b = a.batch[blockIdx.y];
+    gin = static_cast<const cplx<T>*>(b.v);
+    gnin = static_cast<const cplx<T>*>(b.nin);
+    gnout = static_cast<cplx<T>*>(b.nout);
+    gwout = static_cast<cplx<T>*>(const_cast<void*>(b.w));
+    gcoef = static_cast<const cplx<T>*>(b.coef);
+  }
   cplx<T> v[EE];
 
   // ---- forward sequence A; pass 0 reads the column of V from HBM
   {
     constexpr int R = S::radA(0), NR = NY / R, NB = EE / R;
-    const cplx<T>* col = a.in + (size_t)kx * NY;
+    const cplx<T>* col = gin + (size_t)kx * NY;
 #pragma unroll
     for (int b = 0; b < NB; ++b)
 #pragma unroll
@@ -403,10 +438,10 @@ col_step_fast(FastColArgs<T> a) {
   // ---- ETD1 update on the natural-order values held in registers
   constexpr int RL = S::radA(NP - 1), NBL = EE / RL;
   using PO = FastPass<T, NY, EE, RL, NY / RL, P>;
-  const cplx<T>* nin = a.nin + (size_t)kx * NY;
-  cplx<T>* nout = a.nout + (size_t)kx * NY;
+  const cplx<T>* nin = gnin + (size_t)kx * NY;
+  cplx<T>* nout = gnout + (size_t)kx * NY;
   if (kx != 0) {
-    const cplx<T>* cf = a.coef + (size_t)kx * nyh;
+    const cplx<T>* cf = gcoef + (size_t)kx * nyh;
 #pragma unroll
     for (int b = 0; b < NBL; ++b)
 #pragma unroll
@@ -426,8 +461,8 @@ col_step_fast(FastColArgs<T> a) {
 #pragma unroll
       for (int q = 0; q < RL; ++q) buf[padi<P>(PO::out_index(t, b, q))] = v[b * RL + q];
     group_sync<TPF>(g);
-    const cplx<T>* c0 = a.coef;
-    const cplx<T>* cm = a.coef + (size_t)m * nyh;
+    const cplx<T>* c0 = gcoef;
+    const cplx<T>* cm = gcoef + (size_t)m * nyh;
 #pragma unroll
     for (int b = 0; b < NBL; ++b)
 #pragma unroll
@@ -466,7 +501,7 @@ col_step_fast(FastColArgs<T> a) {
   {
     constexpr int RB = S::radB(NP - 1), NBB = EE / RB;
     using QO = FastPass<T, NY, EE, RB, NY / RB, P>;
-    cplx<T>* col = a.wout + (size_t)kx * NY;
+    cplx<T>* col = gwout + (size_t)kx * NY;
     const T s = a.scale;
 #pragma unroll
     for (int b = 0; b < NBB; ++b)

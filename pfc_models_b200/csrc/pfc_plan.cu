@@ -166,6 +166,23 @@ struct pfc_plan {
   size_t fr_smem = 0, fc_smem = 0;
   int tw_ra = 0, tw_rb = 0, tw_ca = 0, tw_cb = 0;  // table offsets (complex elements)
   double lmu0 = 0, lf0 = 0;
+  // CUDA graphs of kGraphBlock steps, one per starting ping-pong parity
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+};
+
+// A batch of plans stepped in lockstep: plans with the same step kernels, sizes and
+// nonlinearity parameters form a class, stepped by one launch per pass with
+// gridDim.y = plans in the class.
+struct pfc_batch_class {
+  std::vector<pfc_plan*> plans;
+  pfc::BatchBufs* table[2] = {nullptr, nullptr};  // device tables, by parity of cur
+};
+
+struct pfc_batch {
+  std::vector<pfc_batch_class> classes;
+  bool fp32 = false;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long long launches = 0;
 };
 
 namespace {
@@ -252,9 +269,20 @@ int launch_col(pfc_plan* h, const ColArgs<T>& a, cudaStream_t s) {
   return PFC_OK;
 }
 
+// The dynamic shared-memory limit belongs to the kernel function on the device and is
+// shared by every plan that launches it: only ever raise it, so that creating a plan
+// that needs less cannot break the launches of one that needs more.
+int raise_smem_limit(const void* fn, size_t bytes) {
+  cudaFuncAttributes fa{};
+  PFC_CUDA(cudaFuncGetAttributes(&fa, fn));
+  if ((size_t)fa.maxDynamicSharedSizeBytes < bytes)
+    PFC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return PFC_OK;
+}
+
 template <class T>
 int set_smem_attrs(pfc_plan* h) {
-#define PFC_ATTR(fn, bytes) PFC_CUDA(cudaFuncSetAttribute((const void*)(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(bytes)))
+#define PFC_ATTR(fn, bytes) do { int rc_ = raise_smem_limit((const void*)(fn), (bytes)); if (rc_) return rc_; } while (0)
   const int md = h->prob.model, rr = h->row_rset, cr = h->col_rset;
   PFC_ATTR((pick_row<T, kRowStep>(md, rr)), h->row_smem);
   PFC_ATTR((pick_row<T, kRowForward>(md, rr)), h->row_smem);
@@ -396,17 +424,18 @@ int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
                                               : fast_row_l<T, kModelStd, kFastMinLog>(lm);
   h->fast_col_fn = fast_col_l<T, kFastMinLog>(ly);
   if (!h->fast_row_fn || !h->fast_col_fn) return PFC_OK;
-  PFC_CUDA(cudaFuncSetAttribute(h->fast_row_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->fr_smem));
-  PFC_CUDA(cudaFuncSetAttribute(h->fast_col_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->fc_smem));
+  if (int rc = raise_smem_limit(h->fast_row_fn, h->fr_smem)) return rc;
+  if (int rc = raise_smem_limit(h->fast_col_fn, h->fc_smem)) return rc;
   h->fast = true;
   return PFC_OK;
 }
 
-// One row pass of a step: W -> V.
+// One row pass of a step: W -> V (of every plan in `table` when batched).
 template <class T>
-int launch_step_row(pfc_plan* h, cudaStream_t s) {
+int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullptr, int count = 1) {
   if (h->fast) {
     FastRowArgs<T> a{};
+    a.batch = table;
     a.ny = h->ny; a.rows = h->fr_rows; a.ld = h->fr_ld;
     a.in = reinterpret_cast<const cplx<T>*>(h->W);
     a.out = reinterpret_cast<cplx<T>*>(h->V);
@@ -417,7 +446,7 @@ int launch_step_row(pfc_plan* h, cudaStream_t s) {
     a.g = h->prob.g; a.min_phi = h->prob.min_phi;
     a.min_log = (h->prob.min_phi > 0) ? std::log(h->prob.min_phi) : -INFINITY;
     void* args[] = {(void*)&a};
-    cudaError_t e = cudaLaunchKernel(h->fast_row_fn, dim3(h->fr_grid), dim3(h->fr_threads), args, h->fr_smem, s);
+    cudaError_t e = cudaLaunchKernel(h->fast_row_fn, dim3(h->fr_grid, count), dim3(h->fr_threads), args, h->fr_smem, s);
     ++h->launches;
     if (e != cudaSuccess) return fail(PFC_E_CUDA, "row step launch failed: %s", cudaGetErrorString(e));
     return PFC_OK;
@@ -428,11 +457,12 @@ int launch_step_row(pfc_plan* h, cudaStream_t s) {
   return launch_row<T, kRowStep>(h, ra, s);
 }
 
-// One column pass of a step: V, n_hat[cur] -> n_hat[cur ^ 1], W.
+// One column pass of a step: V, n_hat[cur] -> n_hat[cur ^ 1], W (batched as above).
 template <class T>
-int launch_step_col(pfc_plan* h, cudaStream_t s) {
+int launch_step_col(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullptr, int count = 1) {
   if (h->fast) {
     FastColArgs<T> a{};
+    a.batch = table;
     a.m = h->m; a.ny = h->ny; a.nyh = h->nyh;
     a.in = reinterpret_cast<const cplx<T>*>(h->V);
     a.nin = reinterpret_cast<const cplx<T>*>(h->nhat[h->cur]);
@@ -443,7 +473,7 @@ int launch_step_col(pfc_plan* h, cudaStream_t s) {
     a.twA = tw + h->tw_ca; a.twB = tw + h->tw_cb;
     a.scale = (T)(1.0 / ((double)h->nx * (double)h->ny));
     void* args[] = {(void*)&a};
-    cudaError_t e = cudaLaunchKernel(h->fast_col_fn, dim3(h->fc_grid), dim3(h->fc_threads), args, h->fc_smem, s);
+    cudaError_t e = cudaLaunchKernel(h->fast_col_fn, dim3(h->fc_grid, count), dim3(h->fc_threads), args, h->fc_smem, s);
     ++h->launches;
     if (e != cudaSuccess) return fail(PFC_E_CUDA, "column step launch failed: %s", cudaGetErrorString(e));
     return PFC_OK;
@@ -485,8 +515,34 @@ int do_set_state(pfc_plan* h, const double* field, cudaStream_t s) {
   return PFC_OK;
 }
 
+constexpr int kGraphBlock = 16;   // steps per captured graph (even: the parity returns)
+
+// Records `fn(capture_stream)` into an executable graph.
+template <class F>
+int capture_graph(F&& fn, cudaGraphExec_t* out) {
+  cudaStream_t cs = nullptr;
+  PFC_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t g = nullptr;
+  int rc = PFC_OK;
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    rc = fn(cs);
+    cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+    if (rc == PFC_OK && e2 != cudaSuccess) rc = fail(PFC_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e2));
+  } else {
+    rc = fail(PFC_E_CUDA, "cudaStreamBeginCapture failed: %s", cudaGetErrorString(e));
+  }
+  if (rc == PFC_OK) {
+    e = cudaGraphInstantiate(out, g, 0);
+    if (e != cudaSuccess) rc = fail(PFC_E_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(e));
+  }
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cs);
+  return rc;
+}
+
 template <class T>
-int do_step(pfc_plan* h, long long nsteps, cudaStream_t s) {
+int step_direct(pfc_plan* h, long long nsteps, cudaStream_t s) {
   for (long long i = 0; i < nsteps; ++i) {
     int rc = launch_step_row<T>(h, s);
     if (rc) return rc;
@@ -495,6 +551,85 @@ int do_step(pfc_plan* h, long long nsteps, cudaStream_t s) {
     h->cur ^= 1;
     ++h->steps_since_set;
   }
+  return PFC_OK;
+}
+
+// Whole blocks of kGraphBlock steps replay a graph captured once per starting
+// parity; the remainder is launched directly.
+template <class T>
+int do_step(pfc_plan* h, long long nsteps, cudaStream_t s) {
+  const bool graphs = !(h->prob.flags & PFC_FLAG_NO_GRAPHS);
+  const long long blocks = graphs ? nsteps / kGraphBlock : 0;
+  if (blocks > 0) {
+    const int p = h->cur;
+    if (!h->graph[p]) {
+      const long long launches = h->launches, since = h->steps_since_set;
+      int rc = capture_graph([&](cudaStream_t cs) { return step_direct<T>(h, kGraphBlock, cs); }, &h->graph[p]);
+      h->launches = launches;
+      h->steps_since_set = since;
+      h->cur = p;
+      if (rc) return rc;
+    }
+    for (long long b = 0; b < blocks; ++b) {
+      cudaError_t e = cudaGraphLaunch(h->graph[p], s);
+      if (e != cudaSuccess) return fail(PFC_E_CUDA, "cudaGraphLaunch failed: %s", cudaGetErrorString(e));
+    }
+    h->launches += 2 * kGraphBlock * blocks;
+    h->steps_since_set += kGraphBlock * blocks;
+  }
+  return step_direct<T>(h, nsteps - blocks * kGraphBlock, s);
+}
+
+// ---- batches
+template <class T>
+int batch_step_direct(pfc_batch* b, int parity, long long nsteps, cudaStream_t s) {
+  for (long long i = 0; i < nsteps; ++i) {
+    for (auto& c : b->classes) {
+      pfc_plan* h = c.plans[0];
+      const int n = (int)c.plans.size();
+      int rc = launch_step_row<T>(h, s, c.table[parity], n);
+      if (rc) return rc;
+      rc = launch_step_col<T>(h, s, c.table[parity], n);
+      if (rc) return rc;
+      b->launches += 2;
+    }
+    parity ^= 1;
+  }
+  return PFC_OK;
+}
+
+template <class T>
+int do_batch_step(pfc_batch* b, long long nsteps, cudaStream_t s) {
+  const int parity = b->classes[0].plans[0]->cur;
+  for (auto& c : b->classes)
+    for (pfc_plan* h : c.plans) {
+      if (!h->state_set) return fail(PFC_E_STATE, "pfc_batch_step: a plan has no state");
+      if (h->cur != parity)
+        return fail(PFC_E_STATE, "pfc_batch_step: plans must have taken the same number of steps mod 2");
+    }
+  const long long blocks = nsteps / kGraphBlock;
+  if (blocks > 0) {
+    if (!b->graph[parity]) {
+      const long long launches = b->launches;
+      int rc = capture_graph([&](cudaStream_t cs) { return batch_step_direct<T>(b, parity, kGraphBlock, cs); },
+                             &b->graph[parity]);
+      b->launches = launches;
+      if (rc) return rc;
+    }
+    for (long long k = 0; k < blocks; ++k) {
+      cudaError_t e = cudaGraphLaunch(b->graph[parity], s);
+      if (e != cudaSuccess) return fail(PFC_E_CUDA, "cudaGraphLaunch failed: %s", cudaGetErrorString(e));
+    }
+    b->launches += 2LL * (long long)b->classes.size() * kGraphBlock * blocks;
+  }
+  const long long rest = nsteps - blocks * kGraphBlock;
+  int rc = batch_step_direct<T>(b, parity, rest, s);   // kGraphBlock is even: parity unchanged
+  if (rc) return rc;
+  for (auto& c : b->classes)
+    for (pfc_plan* h : c.plans) {
+      h->cur ^= (int)(nsteps & 1);
+      h->steps_since_set += nsteps;
+    }
   return PFC_OK;
 }
 
@@ -826,6 +961,8 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
 
 int pfc_plan_destroy(pfc_plan* h) {
   if (!h) return PFC_OK;
+  for (auto& g : h->graph)
+    if (g) cudaGraphExecDestroy(g);
   for (void* p : {h->nhat[0], h->nhat[1], h->W, h->V, h->W2, h->coef, h->tw})
     if (p) cudaFree(p);
   if (h->partials) cudaFree(h->partials);
@@ -922,6 +1059,88 @@ int pfc_plan_info(pfc_plan* h, int64_t* o) {
 }
 
 int64_t pfc_launch_count(pfc_plan* h) { return h ? h->launches : 0; }
+
+int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out) {
+  if (!plans || count <= 0 || !out) return fail(PFC_E_ARG, "pfc_batch_create: need plans and an output");
+  *out = nullptr;
+  for (int i = 0; i < count; ++i) {
+    if (!plans[i]) return fail(PFC_E_ARG, "pfc_batch_create: null plan %d", i);
+    if (!plans[i]->fast)
+      return fail(PFC_E_ARG, "pfc_batch_create: plan %d does not use the power-of-two step kernels", i);
+    if (plans[i]->fp32 != plans[0]->fp32) return fail(PFC_E_ARG, "pfc_batch_create: plans mix precisions");
+    if (plans[i]->device != plans[0]->device) return fail(PFC_E_ARG, "pfc_batch_create: plans on different devices");
+    for (int j = 0; j < i; ++j)
+      if (plans[j] == plans[i]) return fail(PFC_E_ARG, "pfc_batch_create: plan %d appears twice", i);
+  }
+  if (count > 65535) return fail(PFC_E_ARG, "pfc_batch_create: at most 65535 plans");
+  pfc_batch* b = new pfc_batch();
+  b->fp32 = plans[0]->fp32;
+  for (int i = 0; i < count; ++i) {
+    pfc_plan* h = plans[i];
+    pfc_batch_class* cls = nullptr;
+    for (auto& c : b->classes) {
+      // everything the step kernels take from the plan besides the per-plan table entries
+      const pfc_plan* r = c.plans[0];
+      if (r->fast_row_fn == h->fast_row_fn && r->fast_col_fn == h->fast_col_fn && r->nx == h->nx &&
+          r->ny == h->ny && r->prob.g == h->prob.g && r->prob.clamp_log == h->prob.clamp_log &&
+          r->prob.min_phi == h->prob.min_phi) {
+        cls = &c;
+        break;
+      }
+    }
+    if (!cls) {
+      b->classes.emplace_back();
+      cls = &b->classes.back();
+    }
+    cls->plans.push_back(h);
+  }
+  for (auto& c : b->classes) {
+    const size_t n = c.plans.size();
+    std::vector<BatchBufs> host(n);
+    for (int p = 0; p < 2; ++p) {
+      for (size_t i = 0; i < n; ++i) {
+        pfc_plan* h = c.plans[i];
+        host[i].w = h->W;
+        host[i].v = h->V;
+        host[i].nin = h->nhat[p];
+        host[i].nout = h->nhat[p ^ 1];
+        host[i].coef = h->coef;
+        host[i].scal = h->scal;
+      }
+      cudaError_t e = cudaMalloc(&c.table[p], n * sizeof(BatchBufs));
+      if (e == cudaSuccess) e = cudaMemcpy(c.table[p], host.data(), n * sizeof(BatchBufs), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        pfc_batch_destroy(b);
+        return fail(PFC_E_CUDA, "pfc_batch_create: %s", cudaGetErrorString(e));
+      }
+    }
+  }
+  *out = b;
+  return PFC_OK;
+}
+
+int pfc_batch_step(pfc_batch* b, int64_t nsteps, void* stream) {
+  if (!b) return fail(PFC_E_ARG, "pfc_batch_step: null batch");
+  if (nsteps < 0) return fail(PFC_E_ARG, "pfc_batch_step: negative step count");
+  if (nsteps == 0) return PFC_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  return b->fp32 ? do_batch_step<float>(b, nsteps, s) : do_batch_step<double>(b, nsteps, s);
+}
+
+int pfc_batch_destroy(pfc_batch* b) {
+  if (!b) return PFC_OK;
+  for (auto& g : b->graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto& c : b->classes)
+    for (auto& tb : c.table)
+      if (tb) cudaFree(tb);
+  delete b;
+  return PFC_OK;
+}
+
+int64_t pfc_batch_launch_count(pfc_batch* b) { return b ? b->launches : 0; }
+
+int pfc_batch_classes(pfc_batch* b) { return b ? (int)b->classes.size() : 0; }
 
 }  // extern "C"
 

@@ -40,18 +40,20 @@ def GetLinearKernel_phi(modelParameters, DerivativeKernels):
 
 
 class Simulation(_Simulation):
-    def __init__(self, modelParameters, geometry, precision="fp64", clamp_log=False, device=None, kernels="auto"):
+    def __init__(self, modelParameters, geometry, precision="fp64", clamp_log=False, device=None, kernels="auto",
+                 graphs=True):
         super().__init__("log", modelParameters, geometry, precision=precision, clamp_log=clamp_log, device=device,
-                         kernels=kernels)
+                         kernels=kernels, graphs=graphs)
 
     def Get_local_phi(self):
         """Gaussian-coarsened phi (models/logpfc/simulation.py:232-242)."""
         return self._get_local()
 
 
-def BuildB200_Simulation(modelParameters, geometry, precision="fp64", clamp_log=False, device=None, kernels="auto"):
+def BuildB200_Simulation(modelParameters, geometry, precision="fp64", clamp_log=False, device=None, kernels="auto",
+                         graphs=True):
     return Simulation(modelParameters, geometry, precision=precision, clamp_log=clamp_log, device=device,
-                      kernels=kernels)
+                      kernels=kernels, graphs=graphs)
 
 
 def BuildCupyGPU_Simulation(modelParameters, geometry, *_, precision="fp64", **__):

@@ -351,7 +351,7 @@ class Simulation:
     """The reference's Simulation (models/stdpfc/simulation.py:166-268) backed by a plan."""
 
     def __init__(self, model: str, modelParameters, geometry, precision="fp64", clamp_log=False, device=None,
-                 kernels="auto"):
+                 kernels="auto", graphs=True):
         if model not in ("std", "log"):
             raise ValueError(f"model must be 'std' or 'log', got {model!r}")
         if precision not in _PRECISIONS:
@@ -373,7 +373,7 @@ class Simulation:
         prob.clamp_log = 1 if clamp_log else 0
         if kernels not in ("auto", "generic"):
             raise ValueError(f"kernels must be 'auto' or 'generic', got {kernels!r}")
-        prob.flags = 1 if kernels == "generic" else 0
+        prob.flags = (_lib.FLAG_GENERIC_ONLY if kernels == "generic" else 0) | (0 if graphs else _lib.FLAG_NO_GRAPHS)
         self._plan = Plan(prob, device)
         self._version = 0
         self._mu_current = False
@@ -450,6 +450,66 @@ class Simulation:
 
     def Status(self):
         return self._plan.status()
+
+
+class Batch:
+    """Independent simulations stepped in lockstep through pfc_batch_* (one launch per
+    class and pass). Accepts `Simulation` objects or `Plan`s; they must all use the
+    power-of-two step kernels, one precision and one device. The batch borrows the
+    plans: close it before them."""
+
+    def __init__(self, items):
+        self.items = list(items)
+        if not self.items:
+            raise ValueError("Batch needs at least one simulation")
+        self.plans = [s.plan if isinstance(s, Simulation) else s for s in self.items]
+        self.lib = self.plans[0].lib
+        self.torch = self.plans[0].torch
+        self.device = self.plans[0].device
+        arr = (ctypes.c_void_p * len(self.plans))(*[p.handle.value for p in self.plans])
+        self.handle = ctypes.c_void_p()
+        with self.torch.cuda.device(self.device):
+            _lib.check(self.lib.pfc_batch_create(arr, len(self.plans), ctypes.byref(self.handle)))
+
+    def step(self, nsteps=1):
+        """Advances every simulation by `nsteps` (stream-ordered on the current stream)."""
+        nsteps = int(nsteps)
+        if nsteps <= 0:
+            return
+        _lib.check(self.lib.pfc_batch_step(self.handle, nsteps, _stream_ptr(self.torch, self.device)))
+        for s in self.items:
+            if isinstance(s, Simulation):
+                s._version += 1
+                s._mu_current = False
+                for _ in range(nsteps):
+                    s.State.t += s.Model.dt
+
+    def reduce(self):
+        """(F per site, mu per site, mean density) of every simulation as an (n, 3) FP64
+        array, with one device-to-host copy for the whole batch."""
+        t = self.torch
+        out = t.empty((len(self.plans), 3), dtype=t.float64, device=self.device)
+        for i, p in enumerate(self.plans):
+            p.reduce(out[i])
+        return out.cpu().numpy()
+
+    @property
+    def classes(self):
+        return int(self.lib.pfc_batch_classes(self.handle))
+
+    def launches(self):
+        return int(self.lib.pfc_batch_launch_count(self.handle))
+
+    def close(self):
+        if self.handle and self.handle.value:
+            self.lib.pfc_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def make_parameters(**kw):

@@ -44,8 +44,9 @@ def GetLinearKernel_n(modelParameters, DerivativeKernels):
 
 
 class Simulation(_Simulation):
-    def __init__(self, modelParameters, geometry, precision="fp64", device=None, kernels="auto"):
-        super().__init__("std", modelParameters, geometry, precision=precision, device=device, kernels=kernels)
+    def __init__(self, modelParameters, geometry, precision="fp64", device=None, kernels="auto", graphs=True):
+        super().__init__("std", modelParameters, geometry, precision=precision, device=device, kernels=kernels,
+                         graphs=graphs)
 
     def Get_local_n(self):
         """Gaussian-coarsened n of the state at the start of the last step, on the host
@@ -53,10 +54,11 @@ class Simulation(_Simulation):
         return self._get_local()
 
 
-def BuildB200_Simulation(modelParameters, geometry, precision="fp64", device=None, kernels="auto"):
+def BuildB200_Simulation(modelParameters, geometry, precision="fp64", device=None, kernels="auto", graphs=True):
     """precision: "fp64" (plain) or "fp32" (mixed); kernels: "auto" (power-of-two step
-    kernels where the grid allows) or "generic" (mixed-radix kernels everywhere)."""
-    return Simulation(modelParameters, geometry, precision=precision, device=device, kernels=kernels)
+    kernels where the grid allows) or "generic" (mixed-radix kernels everywhere);
+    graphs: replay blocks of 16 steps from a recorded CUDA graph."""
+    return Simulation(modelParameters, geometry, precision=precision, device=device, kernels=kernels, graphs=graphs)
 
 
 def BuildCupyGPU_Simulation(modelParameters, geometry, *_, precision="fp64", **__):

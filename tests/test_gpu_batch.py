@@ -1,0 +1,127 @@
+"""Batched stepping (pfc_batch_*) and CUDA-graph replay of step blocks.
+
+Both only change how the step kernels are launched, never what they compute, so
+the results must be bit-identical to stepping each plan on its own with every
+kernel launched directly.
+"""
+import numpy as np
+import pytest
+
+from pfc_models_b200 import _lib, logpfc, stdpfc
+from pfc_models_b200.simulation import Batch
+
+pytestmark = pytest.mark.gpu
+
+
+def _std_sim(nx, ny, eps, mean, precision, seed, graphs=True):
+    prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=eps, g=0.0, dt=0.5)
+    geom = stdpfc.Build2DGeometry(nx, ny, nx * np.pi / 4, ny * np.pi / 4)
+    sim = stdpfc.BuildB200_Simulation(prm, geom, precision=precision, graphs=graphs)
+    sim.State.n[...] = mean + 0.05 * np.random.default_rng(seed).uniform(-1, 1, (ny, nx))
+    return sim
+
+
+def _log_sim(nx, ny, precision, seed, graphs=True):
+    prm = logpfc.BuildLogPFCModelParameters(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=0.05)
+    geom = logpfc.Build2DGeometry(nx, ny, nx * np.pi / 4, ny * np.pi / 4)
+    sim = logpfc.BuildB200_Simulation(prm, geom, precision=precision, graphs=graphs)
+    sim.State.phi[...] = 0.55 + 0.05 * np.random.default_rng(seed).uniform(-1, 1, (ny, nx))
+    return sim
+
+
+def _mixed(precision, graphs):
+    """Six plans in four classes: 64^2 std (x2), 128^2 std (x2), 64^2 log, 128x64 std."""
+    specs = [("std", 64, 64, -0.3, -0.3), ("std", 128, 128, -0.25, -0.2), ("std", 64, 64, -0.6, -0.45),
+             ("log", 64, 64, None, None), ("std", 128, 64, -0.1, -0.05), ("std", 128, 128, -0.5, -0.4)]
+    sims = []
+    for i, (m, nx, ny, eps, mean) in enumerate(specs):
+        if m == "std":
+            sims.append(_std_sim(nx, ny, eps, mean, precision, seed=i, graphs=graphs))
+        else:
+            sims.append(_log_sim(nx, ny, precision, seed=i, graphs=graphs))
+    return sims
+
+
+def _field(sim):
+    return (sim.State.phi if sim.model == "log" else sim.State.n).get()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_matches_individual_plans(precision):
+    """37 steps (two replayed 16-step blocks and 5 direct steps) of a batch equal the
+    same plans stepped one by one; a second call continues from the other parity."""
+    ref = _mixed(precision, graphs=False)
+    for s in ref:
+        s.TimeSteps(37)
+    sims = _mixed(precision, graphs=True)
+    b = Batch(sims)
+    assert b.classes == 4
+    b.step(37)
+    red = b.reduce()
+    for i, (s, r) in enumerate(zip(sims, ref)):
+        assert np.array_equal(_field(s), _field(r)), i
+        assert s.t == pytest.approx(r.t)
+        assert tuple(red[i]) == pytest.approx(r.Reduce(), rel=1e-15, abs=1e-300)
+    assert b.launches() == 2 * 4 * 37
+    b.step(21)
+    for s in ref:
+        s.TimeSteps(21)
+    for s, r in zip(sims, ref):
+        assert np.array_equal(_field(s), _field(r))
+    b.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_graph_replay_matches_direct_launches(precision):
+    a = _std_sim(256, 128, -0.25, -0.25, precision, seed=3, graphs=True)
+    d = _std_sim(256, 128, -0.25, -0.25, precision, seed=3, graphs=False)
+    for n in (40, 1, 16, 33):
+        a.TimeSteps(n)
+        d.TimeSteps(n)
+        assert np.array_equal(a.State.n.get(), d.State.n.get())
+    # the count includes the launches that materialise the fields read above
+    assert a.plan.launches() == d.plan.launches() >= 2 * 90
+
+
+def test_batch_rejects_mixed_parity_and_unsupported_plans():
+    s1 = _std_sim(64, 64, -0.3, -0.3, "fp32", seed=0)
+    s2 = _std_sim(64, 64, -0.3, -0.3, "fp32", seed=1)
+    s1.TimeStep()
+    b = Batch([s1, s2])
+    with pytest.raises(_lib.PfcError) as e:
+        b.step(2)
+    assert e.value.code == _lib.PFC_E_STATE
+    s2.TimeStep()
+    b.step(2)
+    b.close()
+    prm = stdpfc.BuildStdPFCModelParameters(epsilon=-0.3, g=0.0, dt=0.5)
+    geom = stdpfc.Build2DGeometry(64, 64, 16 * np.pi, 16 * np.pi)
+    gen = stdpfc.BuildB200_Simulation(prm, geom, precision="fp32", kernels="generic")
+    with pytest.raises(_lib.PfcError) as e:
+        Batch([s1, gen])
+    assert e.value.code == _lib.PFC_E_ARG
+    f64 = _std_sim(64, 64, -0.3, -0.3, "fp64", seed=0)
+    with pytest.raises(_lib.PfcError) as e:
+        Batch([s1, f64])
+    assert e.value.code == _lib.PFC_E_ARG
+    with pytest.raises(_lib.PfcError) as e:
+        Batch([s1, s1])
+    assert e.value.code == _lib.PFC_E_ARG
+
+
+@pytest.mark.parametrize("kernels", ["auto", "generic"])
+def test_smaller_plan_created_later_leaves_earlier_plan_launchable(kernels):
+    """Kernel functions are shared between plans; a plan that needs less shared
+    memory must not lower the limit an earlier, larger plan launches with."""
+    prm = stdpfc.BuildStdPFCModelParameters(epsilon=-0.25, g=0.0, dt=0.5)
+    big = stdpfc.BuildB200_Simulation(prm, stdpfc.Build2DGeometry(1024, 512, 256 * np.pi, 128 * np.pi),
+                                      precision="fp64", kernels=kernels)
+    f0 = -0.25 + 0.01 * np.random.default_rng(0).uniform(-1, 1, (512, 1024))
+    big.State.n[...] = f0
+    small = stdpfc.BuildB200_Simulation(prm, stdpfc.Build2DGeometry(64, 64, 16 * np.pi, 16 * np.pi),
+                                        precision="fp64", kernels=kernels)
+    small.State.n[...] = -0.25
+    big.TimeSteps(3)
+    f, mu, mean = big.Reduce()
+    assert np.isfinite(f) and mean == pytest.approx(f0.mean(), abs=1e-14)
+    assert big.Get_local_n().shape == (512, 1024)
