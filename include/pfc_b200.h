@@ -141,6 +141,21 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
 /* problem.flags bits */
 #define PFC_FLAG_GENERIC_ONLY 1   /* do not use the power-of-two step kernels */
 #define PFC_FLAG_NO_GRAPHS 2      /* pfc_step launches every kernel directly */
+/* Variant of the power-of-two step kernels (0 in a field = the precision's default):
+ * complex values per thread of the row and of the column kernel (FP32: 16 or 32,
+ * default 32; FP64: 8 or 16, default 16) and rows per CTA of the row kernel
+ * (1, 2, 4, 8 or 16). Other values make pfc_plan_create return PFC_E_ARG. The
+ * autotuner (pfc_models_b200/tune.py) measures these per grid and caches the best. */
+#define PFC_FLAG_ROW_EE(e) ((int32_t)(e) << 8)
+#define PFC_FLAG_COL_EE(e) ((int32_t)(e) << 16)
+#define PFC_FLAG_ROW_TILE(r) ((int32_t)(r) << 24)
+#define PFC_FLAG_ROW_EE_OF(f) (((f) >> 8) & 0xff)
+#define PFC_FLAG_COL_EE_OF(f) (((f) >> 16) & 0xff)
+#define PFC_FLAG_ROW_TILE_OF(f) (((f) >> 24) & 0x1f)
+
+/* The variant a plan uses: out4 = {row values per thread, column values per thread,
+ * row tile rows, 1 if the power-of-two step kernels are used} (zeros when not). */
+int pfc_plan_variant(pfc_plan* plan, int32_t* out4);
 
 /* Kernel launches issued by this plan since creation (for accounting). */
 int64_t pfc_launch_count(pfc_plan* plan);

@@ -21,6 +21,11 @@ FIELD_OF_CURRENT = 0x100
 SPEC_N_HAT, SPEC_N_HAT_NOW = 0, 1
 FLAG_GENERIC_ONLY, FLAG_NO_GRAPHS = 1, 2
 
+
+def flag_variant(ee_row=0, ee_col=0, row_tile=0):
+    """problem.flags bits selecting a step-kernel variant (PFC_FLAG_ROW_EE & co.)."""
+    return (int(ee_row) << 8) | (int(ee_col) << 16) | (int(row_tile) << 24)
+
 # every symbol include/pfc_b200.h declares, with (restype, argtypes)
 _vp, _i32, _i64, _dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
 SIGNATURES = {
@@ -39,6 +44,7 @@ SIGNATURES = {
     "pfc_status": (ctypes.c_int, [_vp, ctypes.POINTER(_i32)]),
     "pfc_plan_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64)]),
     "pfc_launch_count": (_i64, [_vp]),
+    "pfc_plan_variant": (ctypes.c_int, [_vp, ctypes.POINTER(_i32)]),
     "pfc_field_mean_noalloc": (ctypes.c_int, [_vp, _i64, _vp, _vp]),
     "pfc_batch_create": (ctypes.c_int, [ctypes.POINTER(_vp), _i32, ctypes.POINTER(_vp)]),
     "pfc_batch_step": (ctypes.c_int, [_vp, _i64, _vp]),

@@ -69,17 +69,6 @@ __device__ __forceinline__ void group_sync(int g) {
   }
 }
 
-// Issues asynchronous copies of n elements from global to shared memory (all threads
-// of the CTA take part); the caller commits and waits.
-template <class T>
-__device__ __forceinline__ void stage_async(cplx<T>* dst, const cplx<T>* src, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst + i);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src + i), "n"(sizeof(cplx<T>))
-                 : "memory");
-  }
-}
-
 // One Stockham pass of radix R, stride NS, on a length-N transform whose group has
 // TPF threads holding EE = R * NB values each (v[b * R + q], butterfly j = t + b * TPF).
 template <class T, int N, int EE, int R, int NS, int P>
@@ -207,8 +196,12 @@ struct FastColArgs {
 
 template <int TPF> struct FastBound { static constexpr int value = TPF > 256 ? TPF : 256; };
 // minimum resident CTAs per SM requested from the register allocator (256-thread CTAs)
-template <int TPF> struct FastMinBlocks { static constexpr int value = TPF > 256 ? 1 : 2; };
-template <int TPF> struct FastColMinBlocks { static constexpr int value = TPF > 256 ? 1 : 2; };
+// from an estimate of the registers a thread needs: 2 per real held, plus ~40
+template <class T, int EE, int TPF> struct FastMinBlocks {
+  static constexpr int regs = 2 * EE * (int)(sizeof(T) / 4) + 40;
+  static constexpr int fit = 65536 / (256 * regs);
+  static constexpr int value = TPF > 256 ? 1 : (fit < 1 ? 1 : (fit > 4 ? 4 : fit));
+};
 
 // ------------------------------------------------------------------ row kernel
 // CTA: `rows` consecutive rows (tile), groups of TPF threads each process rows
@@ -216,7 +209,8 @@ template <int TPF> struct FastColMinBlocks { static constexpr int value = TPF > 
 // load/store (global layout is column-major).
 template <class T, int M, int EE_REQ, int MODEL>
 __global__ void __launch_bounds__(FastBound<FastSeq<M, EE_REQ, RadixCap<T>::value>::TPF>::value,
-                  FastMinBlocks<FastSeq<M, EE_REQ, RadixCap<T>::value>::TPF>::value)
+                  FastMinBlocks<T, FastSeq<M, EE_REQ, RadixCap<T>::value>::EE,
+                                FastSeq<M, EE_REQ, RadixCap<T>::value>::TPF>::value)
 row_step_fast(FastRowArgs<T> a) {
   using S = FastSeq<M, EE_REQ, RadixCap<T>::value>;
   constexpr int P = PadShift<T>::value;
@@ -274,28 +268,23 @@ row_step_fast(FastRowArgs<T> a) {
   for (int r = g; r < rows; r += ngroups) {
     cplx<T>* row = sm + r * ld;
     cplx<T> v[EE];
-    // ---- A0 load with the inverse-real pre-twiddle (pairs k, M - k)
-    {
-      constexpr int R = S::radA(0), NR = M / R, NB = EE / R;
-#pragma unroll
-      for (int b = 0; b < NB; ++b) {
-        const int j = t + b * TPF;
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const int k = j + q * NR;
-          const cplx<T> xk = row[padi<P>(k)];
-          cplx<T> z;
-          if (k == 0) {
-            z = mk(xk.x + xk.y, xk.x - xk.y);
-          } else {
-            const cplx<T> xm = row[padi<P>(M - k)];
-            const cplx<T> s = xk + conj(xm), d = xk - conj(xm);
-            z = s + mul_i(cmul(conj(ldgc(a.rtw + k)), d));
-          }
-          v[b * R + q] = z;
-        }
+    // ---- inverse-real pre-twiddle, in place, one (k, M - k) pair per step:
+    // Z[k] = S + U, Z[M - k] = conj(S - U), S = X[k] + conj X[M-k], U = i conj(r_k) (X[k] - conj X[M-k])
+#pragma unroll 2
+    for (int k = t; k <= M / 2; k += TPF) {
+      if (k == 0) {
+        const cplx<T> x0 = row[0];
+        row[0] = mk(x0.x + x0.y, x0.x - x0.y);
+      } else {
+        const cplx<T> xk = row[padi<P>(k)], xm = row[padi<P>(M - k)];
+        const cplx<T> s = xk + conj(xm), d = xk - conj(xm);
+        const cplx<T> u = mul_i(cmul(conj(ldgc(a.rtw + k)), d));
+        row[padi<P>(k)] = s + u;
+        if (k != M / 2) row[padi<P>(M - k)] = conj(s - u);
       }
     }
+    group_sync<TPF>(g);
+    FastPass<T, M, EE, S::radA(0), 1, P>::load(row, v, t);
     group_sync<TPF>(g);
     if constexpr (NP == 1) {
       FastPass<T, M, EE, S::radA(0), 1, P>::template compute<true>(v, t, twA_s);
@@ -337,7 +326,8 @@ row_step_fast(FastRowArgs<T> a) {
       group_sync<TPF>(g);
       QL::template compute<false>(v, t, twB_s + S::twB(NP - 1));
     }
-    // ---- forward-real post-twiddle: publish Z, read the (k, M - k) partners
+    // ---- forward-real post-twiddle: publish Z, then one (k, M - k) pair per step in place:
+    // Y[k] = E + r_k O, Y[M - k] = conj(E - r_k O), E = (Z[k] + conj Z[M-k]) / 2, O = -i (Z[k] - conj Z[M-k]) / 2
     using QO = FastPass<T, M, EE, RL, M / RL, P>;
     constexpr int NBL = EE / RL;
 #pragma unroll
@@ -345,28 +335,19 @@ row_step_fast(FastRowArgs<T> a) {
 #pragma unroll
       for (int q = 0; q < RL; ++q) row[padi<P>(QO::out_index(t, b, q))] = v[b * RL + q];
     group_sync<TPF>(g);
-#pragma unroll
-    for (int b = 0; b < NBL; ++b)
-#pragma unroll
-      for (int q = 0; q < RL; ++q) {
-        const int k = QO::out_index(t, b, q);
-        const cplx<T> zk = v[b * RL + q];
-        cplx<T> y;
-        if (k == 0) {
-          y = mk(zk.x + zk.y, zk.x - zk.y);
-        } else {
-          const cplx<T> zm = row[padi<P>(M - k)];
-          const cplx<T> e = T(0.5) * (zk + conj(zm));
-          const cplx<T> o = T(0.5) * rot4<false>(zk - conj(zm));
-          y = e + cmul(ldgc(a.rtw + k), o);
-        }
-        v[b * RL + q] = y;
+#pragma unroll 2
+    for (int k = t; k <= M / 2; k += TPF) {
+      if (k == 0) {
+        const cplx<T> z0 = row[0];
+        row[0] = mk(z0.x + z0.y, z0.x - z0.y);
+      } else {
+        const cplx<T> zk = row[padi<P>(k)], zm = row[padi<P>(M - k)];
+        const cplx<T> e = T(0.5) * (zk + conj(zm));
+        const cplx<T> o = cmul(ldgc(a.rtw + k), T(0.5) * rot4<false>(zk - conj(zm)));
+        row[padi<P>(k)] = e + o;
+        if (k != M / 2) row[padi<P>(M - k)] = conj(e - o);
       }
-    group_sync<TPF>(g);
-#pragma unroll
-    for (int b = 0; b < NBL; ++b)
-#pragma unroll
-      for (int q = 0; q < RL; ++q) row[padi<P>(QO::out_index(t, b, q))] = v[b * RL + q];
+    }
   }
   __syncthreads();
   // ---- transposing tile store
@@ -382,7 +363,8 @@ row_step_fast(FastRowArgs<T> a) {
 // sequence reads, and the last pass writes, consecutive elements per lane).
 template <class T, int NY, int EE_REQ>
 __global__ void __launch_bounds__(FastBound<FastSeq<NY, EE_REQ, RadixCap<T>::value>::TPF>::value,
-                                  FastColMinBlocks<FastSeq<NY, EE_REQ, RadixCap<T>::value>::TPF>::value)
+                                  FastMinBlocks<T, FastSeq<NY, EE_REQ, RadixCap<T>::value>::EE,
+                                                FastSeq<NY, EE_REQ, RadixCap<T>::value>::TPF>::value)
 col_step_fast(FastColArgs<T> a) {
   using S = FastSeq<NY, EE_REQ, RadixCap<T>::value>;
   constexpr int P = PadShift<T>::value;

@@ -12,8 +12,10 @@
 #include <cuda_runtime.h>
 
 #include "pfc_b200.h"
-#include "pfc_kernels.cuh"
 #include "pfc_fast.cuh"
+#include "pfc_kernels.cuh"
+#include "pfc_registry.h"
+#include "pfc_small.cuh"
 
 using namespace pfc;
 
@@ -162,6 +164,7 @@ struct pfc_plan {
   void* fast_row_fn = nullptr;
   void* fast_col_fn = nullptr;
   int fr_rows = 0, fr_threads = 0, fr_ld = 0, fr_grid = 0;
+  int ee_row = 0, ee_col = 0;  // elements per thread of the fast kernels
   int fc_threads = 0, fc_grid = 0;
   size_t fr_smem = 0, fc_smem = 0;
   int tw_ra = 0, tw_rb = 0, tw_ca = 0, tw_cb = 0;  // table offsets (complex elements)
@@ -221,33 +224,11 @@ ColArgs<T> col_args(const pfc_plan* h) {
   return a;
 }
 
-// The nonlinearity only matters in the step and reduce modes; other modes use the std instance.
-template <int MODE> constexpr bool row_uses_model() { return MODE == kRowStep || MODE == kRowReduce; }
-
-// Radix-set codes of a plan: kRadixPow2 / kRadixAll select the 256-thread kernels;
-// kRadixPow2Big selects the power-of-two kernels built for 1024-thread blocks,
-// used when one transform needs more than 256 threads (>= 8192 points in FP32).
-constexpr int kRadixPow2Big = 2;
-
-template <class T, int MODE, int MODEL, int RSET, int LB>
-void* row_fn() { return (void*)row_kernel<T, MODE, MODEL, RSET, LB>; }
+template <class T, int MODE>
+void* pick_row(int model, int rset) { return GenericInst<T>::row(MODE, model, rset); }
 
 template <class T, int MODE>
-void* pick_row(int model, int rset) {
-  const bool log = row_uses_model<MODE>() && model == kModelLog;
-  if (rset == kRadixPow2Big)
-    return log ? row_fn<T, MODE, kModelLog, kRadixPow2, 1024>() : row_fn<T, MODE, kModelStd, kRadixPow2, 1024>();
-  if (rset == kRadixPow2)
-    return log ? row_fn<T, MODE, kModelLog, kRadixPow2, 256>() : row_fn<T, MODE, kModelStd, kRadixPow2, 256>();
-  return log ? row_fn<T, MODE, kModelLog, kRadixAll, 256>() : row_fn<T, MODE, kModelStd, kRadixAll, 256>();
-}
-
-template <class T, int MODE>
-void* pick_col(int rset) {
-  if (rset == kRadixPow2Big) return (void*)col_kernel<T, MODE, kRadixPow2, 1024>;
-  if (MODE == kColParseval || MODE == kColExport || rset == kRadixPow2) return (void*)col_kernel<T, MODE, kRadixPow2, 256>;
-  return (void*)col_kernel<T, MODE, kRadixAll, 256>;
-}
+void* pick_col(int rset) { return GenericInst<T>::col(MODE, rset); }
 
 template <class T, int MODE>
 int launch_row(pfc_plan* h, const RowArgs<T>& a, cudaStream_t s) {
@@ -298,105 +279,60 @@ int set_smem_attrs(pfc_plan* h) {
 }
 
 // ---- specialised power-of-two path (pfc_fast.cuh)
-// elements per thread of the row and column step kernels
-template <class T> constexpr int fast_ee_row() { return sizeof(T) == 4 ? 32 : 16; }
-template <class T> constexpr int fast_ee_col() { return sizeof(T) == 4 ? 32 : 16; }
-constexpr int kFastMinLog = 5, kFastMaxLogRow = 12, kFastMaxLogCol = 13;
-
 int ilog2_exact(int n) {
   int l = 0;
   while ((1 << l) < n) ++l;
   return (1 << l) == n ? l : -1;
 }
 
-// Pass tables of sequences A and B for an N-point transform, laid out as FastSeq
-// expects: for p = 1 .. NPASS-1, ns(p) x (R(p) - 1) entries exp(-2 pi i q k / (ns R)).
-template <class T, int N, int EE>
-void fast_tables(std::vector<long double>& tw, int& offA, int& offB) {
-  using S = FastSeq<N, EE, RadixCap<T>::value>;
-  const long double twopi = 6.283185307179586476925286766559L;
-  for (int seq = 0; seq < 2; ++seq) {
-    (seq == 0 ? offA : offB) = (int)(tw.size() / 2);
-    for (int p = 1; p < S::NPASS; ++p) {
-      const int R = seq == 0 ? S::radA(p) : S::radB(p);
-      const int ns = seq == 0 ? S::nsA(p) : S::nsB(p);
-      for (int k = 0; k < ns; ++k)
-        for (int q = 1; q < R; ++q) {
-          const long double ang = -twopi * (long double)((long long)q * k) / (long double)(ns * R);
-          tw.push_back(cosl(ang));
-          tw.push_back(sinl(ang));
-        }
-    }
+// Elements per thread of the step kernels built for each precision (the first is the default).
+template <class T> constexpr int fast_ee_default() { return sizeof(T) == 4 ? 32 : 16; }
+template <class T> bool fast_ee_valid(int ee) { return sizeof(T) == 4 ? (ee == 16 || ee == 32) : (ee == 8 || ee == 16); }
+
+template <class T>
+bool fast_lookup(bool col, int lg, int ee, int model, FastKernel* k) {
+  if (sizeof(T) == 4) {
+    if (ee == 16) return col ? FastInst<float, 16>::col(lg, k) : FastInst<float, 16>::row(lg, model, k);
+    return col ? FastInst<float, 32>::col(lg, k) : FastInst<float, 32>::row(lg, model, k);
   }
+  if (ee == 8) return col ? FastInst<double, 8>::col(lg, k) : FastInst<double, 8>::row(lg, model, k);
+  return col ? FastInst<double, 16>::col(lg, k) : FastInst<double, 16>::row(lg, model, k);
 }
 
-template <class T, bool COL, int L>
-void fast_tables_l(int lg, std::vector<long double>& tw, int& a, int& b) {
-  if constexpr (L <= kFastMaxLogCol) {
-    if (lg == L) { fast_tables<T, (1 << L), COL ? fast_ee_col<T>() : fast_ee_row<T>()>(tw, a, b); return; }
-    fast_tables_l<T, COL, L + 1>(lg, tw, a, b);
-  }
-}
-
-template <class T, bool COL, int L>
-int fast_tpf_l(int lg) {
-  if constexpr (L <= kFastMaxLogCol) {
-    if (lg == L) return FastSeq<(1 << L), COL ? fast_ee_col<T>() : fast_ee_row<T>(), RadixCap<T>::value>::TPF;
-    return fast_tpf_l<T, COL, L + 1>(lg);
-  } else {
-    return 0;
-  }
-}
-
-// elements of the sequence A and B twiddle tables staged in shared memory
-template <class T, bool COL, int L>
-int fast_tw_elems_l(int lg) {
-  if constexpr (L <= kFastMaxLogCol) {
-    using S = FastSeq<(1 << L), COL ? fast_ee_col<T>() : fast_ee_row<T>(), RadixCap<T>::value>;
-    if (lg == L) return S::sizeA() + S::sizeB();
-    return fast_tw_elems_l<T, COL, L + 1>(lg);
-  } else {
-    return 0;
-  }
-}
-
-template <class T, int MODEL, int L>
-void* fast_row_l(int lg) {
-  if constexpr (L <= kFastMaxLogRow) {
-    if (lg == L) return (void*)row_step_fast<T, (1 << L), fast_ee_row<T>(), MODEL>;
-    return fast_row_l<T, MODEL, L + 1>(lg);
-  } else {
-    return nullptr;
-  }
-}
-
-template <class T, int L>
-void* fast_col_l(int lg) {
-  if constexpr (L <= kFastMaxLogCol) {
-    if (lg == L) return (void*)col_step_fast<T, (1 << L), fast_ee_col<T>()>;
-    return fast_col_l<T, L + 1>(lg);
-  } else {
-    return nullptr;
-  }
+template <class T>
+bool fast_seq_tables(int lg, int ee, std::vector<long double>& tw, int& a, int& b) {
+  if (sizeof(T) == 4) return ee == 16 ? FastInst<float, 16>::tables(lg, tw, a, b) : FastInst<float, 32>::tables(lg, tw, a, b);
+  return ee == 8 ? FastInst<double, 8>::tables(lg, tw, a, b) : FastInst<double, 16>::tables(lg, tw, a, b);
 }
 
 // Chooses the fast kernels and their launch shapes; appends their twiddle tables to tw.
+// problem.flags may pick the elements per thread of each kernel and the row tile.
 template <class T>
 int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
+  const int flags = h->prob.flags;
+  const int ee_r = PFC_FLAG_ROW_EE_OF(flags) ? PFC_FLAG_ROW_EE_OF(flags) : fast_ee_default<T>();
+  const int ee_c = PFC_FLAG_COL_EE_OF(flags) ? PFC_FLAG_COL_EE_OF(flags) : fast_ee_default<T>();
+  const int tile = PFC_FLAG_ROW_TILE_OF(flags);
+  if (!fast_ee_valid<T>(ee_r) || !fast_ee_valid<T>(ee_c))
+    return fail(PFC_E_ARG, "pfc_plan_create: elements per thread (%d, %d) not built for this precision "
+                "(FP32: 16 or 32, FP64: 8 or 16)", ee_r, ee_c);
+  if (tile && (tile > 16 || (tile & (tile - 1))))
+    return fail(PFC_E_ARG, "pfc_plan_create: row tile %d is not a power of two <= 16", tile);
   const int lm = ilog2_exact(h->m), ly = ilog2_exact(h->ny);
-  if ((h->prob.flags & 1) || lm < kFastMinLog || lm > kFastMaxLogRow || ly < kFastMinLog || ly > kFastMaxLogCol)
+  if ((flags & PFC_FLAG_GENERIC_ONLY) || lm < kFastMinLog || lm > kFastMaxLogRow || ly < kFastMinLog ||
+      ly > kFastMaxLogCol)
+    return PFC_OK;
+  FastKernel kr, kc;
+  if (!fast_lookup<T>(false, lm, ee_r, h->prob.model, &kr) || !fast_lookup<T>(true, ly, ee_c, h->prob.model, &kc))
     return PFC_OK;
   constexpr int P = PadShift<T>::value;
   const int elt = (int)sizeof(cplx<T>);
-  fast_tables_l<T, false, kFastMinLog>(lm, tw, h->tw_ra, h->tw_rb);
-  fast_tables_l<T, true, kFastMinLog>(ly, tw, h->tw_ca, h->tw_cb);
-  // row kernel: tile of fr_rows rows (>= 64 B per kx run), groups of tpf threads
-  const int tpr = fast_tpf_l<T, false, kFastMinLog>(lm);
+  // row kernel: tile of fr_rows rows (>= 64 B per kx run by default), groups of tpf threads
+  const int tpr = kr.tpf;
   int ngr = std::max(1, 256 / tpr);
-  int rows = sizeof(T) == 4 ? 8 : 4;  // 64 B of a column per tile
-  const size_t row_tables = 0;  // twiddle tables stay in global memory (L1-cached)
+  int rows = tile ? tile : (sizeof(T) == 4 ? 8 : 4);
   // smaller tiles for long rows so that the tile fits the shared-memory budget
-  while (rows > 1 && (size_t)rows * (h->m + (h->m >> P) + (1 << P)) * elt + row_tables > 200 * 1024) rows /= 2;
+  while (rows > 1 && (size_t)rows * (h->m + (h->m >> P) + (1 << P)) * elt > 200 * 1024) rows /= 2;
   ngr = std::min(ngr, rows);
   rows = std::max(rows, ngr);
   // row stride in shared memory: with S = 128 B / element slots per bank cycle,
@@ -406,24 +342,27 @@ int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
   const int want = (slots / rows) % slots;
   int ld = h->m + (h->m >> P);
   while (ld % slots != want) ++ld;
+  // column kernel: one group of tpc threads per column
+  const int tpc = kc.tpf;
+  const int ngc = std::min(std::max(1, 256 / tpc), h->m);
+  const size_t fr_smem = (size_t)rows * ld * elt;
+  const size_t fc_smem = (size_t)ngc * (h->ny + (h->ny >> P) + 2) * elt;   // one exchange buffer per column
+  if (ngr * tpr > 1024 || ngc * tpc > 1024 || fr_smem > 200 * 1024 || fc_smem > 200 * 1024)
+    return PFC_OK;  // generic path
   h->fr_rows = rows;
   h->fr_threads = ngr * tpr;
   h->fr_ld = ld;
   h->fr_grid = (h->ny + rows - 1) / rows;
-  h->fr_smem = (size_t)rows * ld * elt + row_tables;
-  // column kernel: one group of tpc threads per column
-  const int tpc = fast_tpf_l<T, true, kFastMinLog>(ly);
-  const int ngc = std::min(std::max(1, 256 / tpc), h->m);
+  h->fr_smem = fr_smem;
   h->fc_threads = ngc * tpc;
   h->fc_grid = h->m / ngc;
-  // one exchange buffer per column
-  h->fc_smem = (size_t)ngc * (h->ny + (h->ny >> P) + 2) * elt;
-  if (h->fr_threads > 1024 || h->fc_threads > 1024 || h->fr_smem > 200 * 1024 || h->fc_smem > 200 * 1024)
-    return PFC_OK;  // generic path
-  h->fast_row_fn = h->prob.model == kModelLog ? fast_row_l<T, kModelLog, kFastMinLog>(lm)
-                                              : fast_row_l<T, kModelStd, kFastMinLog>(lm);
-  h->fast_col_fn = fast_col_l<T, kFastMinLog>(ly);
-  if (!h->fast_row_fn || !h->fast_col_fn) return PFC_OK;
+  h->fc_smem = fc_smem;
+  h->fast_row_fn = kr.fn;
+  h->fast_col_fn = kc.fn;
+  h->ee_row = ee_r;
+  h->ee_col = ee_c;
+  fast_seq_tables<T>(lm, ee_r, tw, h->tw_ra, h->tw_rb);
+  fast_seq_tables<T>(ly, ee_c, tw, h->tw_ca, h->tw_cb);
   if (int rc = raise_smem_limit(h->fast_row_fn, h->fr_smem)) return rc;
   if (int rc = raise_smem_limit(h->fast_col_fn, h->fc_smem)) return rc;
   h->fast = true;
@@ -1059,6 +998,15 @@ int pfc_plan_info(pfc_plan* h, int64_t* o) {
 }
 
 int64_t pfc_launch_count(pfc_plan* h) { return h ? h->launches : 0; }
+
+int pfc_plan_variant(pfc_plan* h, int32_t* o) {
+  if (!h || !o) return fail(PFC_E_ARG, "pfc_plan_variant: null argument");
+  o[0] = h->fast ? h->ee_row : 0;
+  o[1] = h->fast ? h->ee_col : 0;
+  o[2] = h->fast ? h->fr_rows : 0;
+  o[3] = h->fast ? 1 : 0;
+  return PFC_OK;
+}
 
 int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out) {
   if (!plans || count <= 0 || !out) return fail(PFC_E_ARG, "pfc_batch_create: need plans and an output");

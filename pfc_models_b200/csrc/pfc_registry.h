@@ -1,0 +1,39 @@
+// Kernel lookup across translation units. The step kernels are instantiated in
+// several .cu files (one per precision and variant) that compile in parallel; the
+// plan code finds them through these functions.
+#pragma once
+#include <vector>
+
+namespace pfc {
+
+// Radix-set code of the generic kernels built for 1024-thread blocks, used when one
+// transform needs more than 256 threads (>= 8192 points in FP32); kRadixPow2 and
+// kRadixAll (pfc_fft.cuh) select the 256-thread kernels.
+constexpr int kRadixPow2Big = 2;
+
+// log2 sizes of the power-of-two step kernels: row transforms of M = nx/2 points,
+// column transforms of ny points
+constexpr int kFastMinLog = 5, kFastMaxLogRow = 12, kFastMaxLogCol = 13;
+
+struct FastKernel {
+  void* fn = nullptr;  // kernel entry, for cudaLaunchKernel
+  int tpf = 0;         // threads per transform
+};
+
+// Power-of-two step kernels with EE complex values per thread (pfc_fast.cuh).
+template <class T, int EE>
+struct FastInst {
+  static bool row(int lg, int model, FastKernel* out);
+  static bool col(int lg, FastKernel* out);
+  // appends the pass tables of sequences A and B of a 2^lg-point transform
+  static bool tables(int lg, std::vector<long double>& tw, int& offA, int& offB);
+};
+
+// Mixed-radix kernels (pfc_kernels.cuh), by mode (kRow* / kCol*) and radix set.
+template <class T>
+struct GenericInst {
+  static void* row(int mode, int model, int rset);
+  static void* col(int mode, int rset);
+};
+
+}  // namespace pfc

@@ -142,6 +142,12 @@ class Plan:
     def launches(self):
         return int(self.lib.pfc_launch_count(self.handle))
 
+    def variant(self):
+        """{"ee_row", "ee_col", "row_tile", "fast"} of the step kernels this plan uses."""
+        o = (ctypes.c_int32 * 4)()
+        _lib.check(self.lib.pfc_plan_variant(self.handle, o))
+        return dict(zip(("ee_row", "ee_col", "row_tile", "fast"), list(o)))
+
     def close(self):
         if self.handle and self.handle.value:
             self.lib.pfc_plan_destroy(self.handle)
@@ -347,6 +353,23 @@ class _SimulationState:
         raise AttributeError(name)
 
 
+def _kernel_flags(kernels, prob):
+    """problem.flags bits for the `kernels` choice of a Simulation: "auto" (the variant
+    the autotuner cached for this grid, else the defaults), "default", "generic" (the
+    mixed-radix kernels everywhere), or a dict {"ee_row", "ee_col", "row_tile"}."""
+    if isinstance(kernels, dict):
+        return _lib.flag_variant(kernels.get("ee_row", 0), kernels.get("ee_col", 0), kernels.get("row_tile", 0))
+    if kernels == "generic":
+        return _lib.FLAG_GENERIC_ONLY
+    if kernels == "default":
+        return 0
+    if kernels == "auto":
+        from . import tune
+        v = tune.lookup(prob.nx, prob.ny, prob.precision, prob.model)
+        return _lib.flag_variant(**v) if v else 0
+    raise ValueError(f"kernels must be 'auto', 'default', 'generic' or a variant dict, got {kernels!r}")
+
+
 class Simulation:
     """The reference's Simulation (models/stdpfc/simulation.py:166-268) backed by a plan."""
 
@@ -371,9 +394,7 @@ class Simulation:
         prob.small_z_tol = float(getattr(m, "smallZTol", 2e-5))
         prob.min_phi = float(getattr(m, "minPhi", 0.0) or 0.0)
         prob.clamp_log = 1 if clamp_log else 0
-        if kernels not in ("auto", "generic"):
-            raise ValueError(f"kernels must be 'auto' or 'generic', got {kernels!r}")
-        prob.flags = (_lib.FLAG_GENERIC_ONLY if kernels == "generic" else 0) | (0 if graphs else _lib.FLAG_NO_GRAPHS)
+        prob.flags = _kernel_flags(kernels, prob) | (0 if graphs else _lib.FLAG_NO_GRAPHS)
         self._plan = Plan(prob, device)
         self._version = 0
         self._mu_current = False

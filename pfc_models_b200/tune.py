@@ -1,0 +1,168 @@
+"""Autotuner of the power-of-two step kernels, with an on-disk cache.
+
+    python -m pfc_models_b200.tune --sizes 256,2048 --precision fp32,fp64 [--model std] [--save]
+
+For one grid, precision and model it times every built variant of the two step
+kernels (complex values per thread of the row and the column kernel, rows per
+CTA of the row kernel) with CUDA events on a seeded noisy-liquid state, and keeps
+the fastest row and the fastest column variant. Results are cached as JSON, keyed
+by GPU name, grid, precision and model, in the file named by $PFC_TUNE_CACHE
+(default ~/.cache/pfc_models_b200/tune.json). `Simulation(kernels="auto")` looks
+a grid up there first, then in the table measured on B200 that ships with the
+package (tuned_b200.json), and otherwise uses the precision's defaults.
+"""
+from __future__ import annotations
+
+import argparse
+import itertools
+import json
+import math
+import os
+import threading
+
+from . import _lib
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PACKAGED = os.path.join(HERE, "tuned_b200.json")
+EE_CHOICES = {_lib.FP32_MIXED: (16, 32), _lib.FP64_PLAIN: (8, 16)}
+TILE_CHOICES = (1, 2, 4, 8, 16)
+_lock = threading.Lock()
+_memo: dict = {}
+
+
+def cache_path() -> str:
+    return os.environ.get("PFC_TUNE_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "pfc_models_b200",
+                                                           "tune.json")
+
+
+def _key(device_name, nx, ny, precision, model):
+    prec = "fp32" if precision == _lib.FP32_MIXED else "fp64"
+    mod = "log" if model == _lib.MODEL_LOG else "std"
+    return f"{device_name}|{nx}x{ny}|{prec}|{mod}"
+
+
+def _load(path):
+    with _lock:
+        if path in _memo:
+            return _memo[path]
+        try:
+            with open(path) as f:
+                d = json.load(f)
+        except (OSError, ValueError):
+            d = {}
+        _memo[path] = d
+        return d
+
+
+def _device_name():
+    import torch
+    return torch.cuda.get_device_name()
+
+
+def lookup(nx, ny, precision, model, device_name=None):
+    """The cached variant {"ee_row", "ee_col", "row_tile"} for this grid, or None."""
+    if device_name is None:
+        try:
+            device_name = _device_name()
+        except Exception:
+            return None
+    key = _key(device_name, nx, ny, precision, model)
+    for path in (cache_path(), PACKAGED):
+        e = _load(path).get(key)
+        if e:
+            return {k: int(e[k]) for k in ("ee_row", "ee_col", "row_tile")}
+    return None
+
+
+def _store(path, key, entry):
+    d = dict(_load(path))
+    d[key] = entry
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+    with _lock:
+        _memo[path] = d
+
+
+def tune(nx, ny, precision="fp32", model="std", steps=20, warmup=3, save=True, path=None):
+    """Times the variants for one grid; returns the chosen entry (and caches it)."""
+    import numpy as np
+    import torch
+
+    from . import fields, logpfc, stdpfc
+    from .simulation import _PRECISIONS
+    prec = _PRECISIONS[precision]
+    mod = logpfc if model == "log" else stdpfc
+    geom = mod.Build2DGeometry(nx, ny, nx * math.pi / 4, ny * math.pi / 4)
+    if model == "log":
+        prm = logpfc.BuildLogPFCModelParameters(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=0.1)
+        mean = 0.55
+    else:
+        prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.3, g=0.0, dt=0.5)
+        mean = -0.3
+    f0 = fields.GenerateNoisyLiquid(geom, mean, 0.01, seed=0)
+    ees = EE_CHOICES[prec]
+    rows, cols = {}, {}
+    combos = list(itertools.product(ees, TILE_CHOICES))
+    for i, (ee_r, tile) in enumerate(combos):
+        ee_c = ees[i % len(ees)]
+        variant = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile}
+        sim = mod.BuildB200_Simulation(prm, geom, precision=precision, kernels=variant)
+        v = sim.plan.variant()
+        if not v["fast"]:
+            sim.plan.close()
+            continue
+        field = sim.State.phi if model == "log" else sim.State.n
+        field[...] = f0
+        sim.plan.step_timed(warmup)
+        ms_r, ms_c = sim.plan.step_timed(steps)
+        torch.cuda.synchronize()
+        ok = np.isfinite(sim.CalculateFreeEnergy())
+        sim.plan.close()
+        if not ok:
+            continue
+        rk = (v["ee_row"], v["row_tile"])
+        rows[rk] = min(rows.get(rk, math.inf), 1e3 * ms_r / steps)
+        cols.setdefault(v["ee_col"], []).append(1e3 * ms_c / steps)
+    if not rows or not cols:
+        return None
+    (ee_r, tile), row_us = min(rows.items(), key=lambda kv: kv[1])
+    col_avg = {k: sum(v) / len(v) for k, v in cols.items()}
+    ee_c, col_us = min(col_avg.items(), key=lambda kv: kv[1])
+    entry = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile, "row_us": row_us, "col_us": col_us,
+             "rows_us": {f"{a}/{b}": u for (a, b), u in sorted(rows.items())},
+             "cols_us": {str(k): u for k, u in sorted(col_avg.items())}}
+    if save:
+        _store(path or cache_path(), _key(_device_name(), nx, ny, prec,
+                                          _lib.MODEL_LOG if model == "log" else _lib.MODEL_STD), entry)
+    return entry
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--sizes", default="2048", help="comma list of n (n x n grids) or nx x ny items like 512x256")
+    ap.add_argument("--precision", default="fp32")
+    ap.add_argument("--model", default="std")
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--save", action="store_true", help="write the user cache")
+    ap.add_argument("--out", default=None, help="also write all entries to this JSON file")
+    a = ap.parse_args()
+    allres = {}
+    for s in a.sizes.split(","):
+        nx, ny = (int(v) for v in s.split("x")) if "x" in s else (int(s), int(s))
+        for precision in a.precision.split(","):
+            for model in a.model.split(","):
+                e = tune(nx, ny, precision, model, steps=a.steps, save=a.save)
+                key = _key(_device_name(), nx, ny, _lib.FP32_MIXED if precision == "fp32" else _lib.FP64_PLAIN,
+                           _lib.MODEL_LOG if model == "log" else _lib.MODEL_STD)
+                allres[key] = e
+                print(json.dumps({key: e}), flush=True)
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(allres, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()

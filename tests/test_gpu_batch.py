@@ -125,3 +125,17 @@ def test_smaller_plan_created_later_leaves_earlier_plan_launchable(kernels):
     f, mu, mean = big.Reduce()
     assert np.isfinite(f) and mean == pytest.approx(f0.mean(), abs=1e-14)
     assert big.Get_local_n().shape == (512, 1024)
+
+
+def test_auto_kernels_use_the_packaged_table():
+    import json
+    import torch
+    from pfc_models_b200 import tune
+    table = json.load(open(tune.PACKAGED))
+    key = f"{torch.cuda.get_device_name()}|256x256|fp32|std"
+    sim = _std_sim(256, 256, -0.25, -0.25, "fp32", seed=0)
+    v = sim.plan.variant()
+    if key in table and tune.lookup(256, 256, _lib.FP32_MIXED, _lib.MODEL_STD) == \
+            {k: table[key][k] for k in ("ee_row", "ee_col", "row_tile")}:
+        assert (v["ee_row"], v["ee_col"]) == (table[key]["ee_row"], table[key]["ee_col"])
+    assert v["fast"] == 1

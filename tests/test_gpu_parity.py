@@ -383,3 +383,43 @@ def test_fast_kernels_long_transforms(nx, ny, precision):
     sim.TimeSteps(6)
     tol = 1e-12 if precision == "fp64" else 2e-5
     assert rel_l2(sim.State.n.get() + 0.3, ref + 0.3) < tol
+
+
+VARIANT_SIZES = [(256, 256), (1024, 512), (64, 2048)]
+
+
+@pytest.mark.parametrize("nx,ny", VARIANT_SIZES)
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_kernel_variants_match_generic(nx, ny, precision):
+    """Every built variant of the power-of-two step kernels (values per thread of the
+    row and column kernels, rows per CTA) against the mixed-radix kernels, 8 steps."""
+    prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.3, g=0.2, dt=0.3)
+    geom = stdpfc.Build2DGeometry(nx, ny, nx * np.pi / 4, ny * np.pi / 4)
+    f0 = -0.3 + 0.05 * np.random.default_rng(nx + ny).uniform(-1, 1, (ny, nx))
+    gen = stdpfc.BuildB200_Simulation(prm, geom, precision=precision, kernels="generic")
+    gen.State.n[...] = f0
+    gen.TimeSteps(8)
+    ref = gen.State.n.get()
+    ees = (16, 32) if precision == "fp32" else (8, 16)
+    tol = 1e-13 if precision == "fp64" else 1e-5
+    for ee_r in ees:
+        for ee_c in ees:
+            for tile in (1, 4, 16):
+                v = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile}
+                sim = stdpfc.BuildB200_Simulation(prm, geom, precision=precision, kernels=v)
+                got = sim.plan.variant()
+                assert got["fast"] == 1 and got["ee_row"] == ee_r and got["ee_col"] == ee_c, (v, got)
+                sim.State.n[...] = f0
+                sim.TimeSteps(8)
+                assert rel_l2(sim.State.n.get() + 0.3, ref + 0.3) < tol, v
+                sim.plan.close()
+
+
+def test_kernel_variant_errors():
+    from pfc_models_b200 import _lib
+    prm = stdpfc.BuildStdPFCModelParameters(epsilon=-0.3, g=0.0, dt=0.5)
+    geom = stdpfc.Build2DGeometry(128, 128, 32 * np.pi, 32 * np.pi)
+    for bad in ({"ee_row": 8}, {"ee_col": 64}, {"row_tile": 3}):
+        with pytest.raises(_lib.PfcError) as e:
+            stdpfc.BuildB200_Simulation(prm, geom, precision="fp32", kernels=bad)
+        assert e.value.code == _lib.PFC_E_ARG

@@ -1,0 +1,40 @@
+"""Autotuner cache: lookup order (user cache, then the packaged B200 table) and the
+JSON round trip. No GPU: the device name is passed explicitly."""
+import json
+
+from pfc_models_b200 import _lib, tune
+
+
+def test_packaged_table_is_used_without_a_user_cache(tmp_path, monkeypatch):
+    monkeypatch.setenv("PFC_TUNE_CACHE", str(tmp_path / "none.json"))
+    table = json.load(open(tune.PACKAGED))
+    assert table, "the packaged table is empty"
+    key = "NVIDIA B200|2048x2048|fp32|std"
+    assert key in table
+    v = tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200")
+    assert v == {k: table[key][k] for k in ("ee_row", "ee_col", "row_tile")}
+    for e in table.values():
+        assert e["ee_row"] in (8, 16, 32) and e["ee_col"] in (8, 16, 32) and e["row_tile"] in (1, 2, 4, 8, 16)
+    assert tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="other GPU") is None
+
+
+def test_user_cache_overrides_and_round_trips(tmp_path, monkeypatch):
+    path = tmp_path / "sub" / "tune.json"
+    monkeypatch.setenv("PFC_TUNE_CACHE", str(path))
+    key = tune._key("NVIDIA B200", 2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD)
+    tune._store(str(path), key, {"ee_row": 16, "ee_col": 32, "row_tile": 2, "row_us": 1.0, "col_us": 2.0})
+    tune._memo.clear()
+    assert json.load(open(path))[key]["ee_col"] == 32
+    assert tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200") == \
+        {"ee_row": 16, "ee_col": 32, "row_tile": 2}
+    tune._memo.clear()
+
+
+def test_flag_encoding_matches_header():
+    import re
+    from tests.conftest import ROOT
+    import os
+    src = open(os.path.join(ROOT, "include", "pfc_b200.h")).read()
+    shifts = dict(re.findall(r"#define PFC_FLAG_(ROW_EE|COL_EE|ROW_TILE)\(\w\) \(\(int32_t\)\(\w\) << (\d+)\)", src))
+    assert shifts == {"ROW_EE": "8", "COL_EE": "16", "ROW_TILE": "24"}
+    assert _lib.flag_variant(16, 32, 4) == (16 << 8) | (32 << 16) | (4 << 24)
