@@ -13,6 +13,7 @@
 // A transform group synchronises with __syncwarp when it fits in a warp, otherwise
 // with its own named barrier, so groups never wait for each other.
 #pragma once
+#include <cstdint>
 #include <type_traits>
 
 #include "pfc_kernels.cuh"
@@ -185,14 +186,25 @@ struct FastColArgs {
   int m, ny, nyh;
   const BatchBufs* batch;    // null: one plan, the pointers below
   const cplx<T>* in;         // V
-  const cplx<T>* nin;        // n_hat
-  cplx<T>* nout;             // n_hat'
+  const cplx<double>* nin;   // n_hat (FP64 in both precision forms)
+  cplx<double>* nout;        // n_hat'
   cplx<T>* wout;             // W'
-  const cplx<T>* coef;       // (A, Bg) [kx][ky <= ny/2]
+  const cplx<double>* coef;  // (A - 1, Bg) [kx][ky <= ny/2], FP64
   const cplx<T>* twA;        // column sequence A (forward)
   const cplx<T>* twB;        // column sequence B (inverse uses conjugates)
   T scale;
 };
+
+// Bulk prefetch of [p, p + bytes) into L2 (p and bytes multiples of 16), in chunks
+// issued by the threads of a transform group.
+__device__ __forceinline__ void l2_prefetch_range(const void* p, unsigned bytes, int t, int nthreads) {
+  constexpr unsigned kChunk = 4096;
+  const char* c = static_cast<const char*>(p);
+  for (unsigned off = (unsigned)t * kChunk; off < bytes; off += (unsigned)nthreads * kChunk) {
+    const unsigned n = bytes - off < kChunk ? bytes - off : kChunk;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c + off), "r"(n) : "memory");
+  }
+}
 
 template <int TPF> struct FastBound { static constexpr int value = TPF > 256 ? TPF : 256; };
 // minimum resident CTAs per SM requested from the register allocator (256-thread CTAs)
@@ -380,19 +392,29 @@ col_step_fast(FastColArgs<T> a) {
   cplx<T>* buf = sm + g * PADN;                   // exchange buffer of this column
   const int m = a.m, nyh = a.nyh;
   const cplx<T>* gin = a.in;
-  const cplx<T>* gnin = a.nin;
-  cplx<T>* gnout = a.nout;
+  const cplx<double>* gnin = a.nin;
+  cplx<double>* gnout = a.nout;
   cplx<T>* gwout = a.wout;
-  const cplx<T>* gcoef = a.coef;
+  const cplx<double>* gcoef = a.coef;
   if (a.batch) {
     const BatchBufs& b = a.batch[blockIdx.y];
     gin = static_cast<const cplx<T>*>(b.v);
-    gnin = static_cast<const cplx<T>*>(b.nin);
-    gnout = static_cast<cplx<T>*>(b.nout);
+    gnin = static_cast<const cplx<double>*>(b.nin);
+    gnout = static_cast<cplx<double>*>(b.nout);
     gwout = static_cast<cplx<T>*>(const_cast<void*>(b.w));
-    gcoef = static_cast<const cplx<T>*>(b.coef);
+    gcoef = static_cast<const cplx<double>*>(b.coef);
   }
   cplx<T> v[EE];
+
+  // ---- start this column's n_hat and coefficients towards L2 while the forward
+  // transform runs (the coefficient range is widened to 16-byte boundaries; it stays
+  // inside the table, which has a row after every column a CTA handles)
+  l2_prefetch_range(gnin + (size_t)kx * NY, NY * (unsigned)sizeof(cplx<double>), t, TPF);
+  {
+    const uintptr_t c0 = reinterpret_cast<uintptr_t>(gcoef + (size_t)kx * nyh) & ~(uintptr_t)15;
+    const uintptr_t c1 = (reinterpret_cast<uintptr_t>(gcoef + (size_t)(kx + 1) * nyh) + 15) & ~(uintptr_t)15;
+    l2_prefetch_range(reinterpret_cast<const void*>(c0), (unsigned)(c1 - c0), t, TPF);
+  }
 
   // ---- forward sequence A; pass 0 reads the column of V from HBM
   {
@@ -417,54 +439,57 @@ col_step_fast(FastColArgs<T> a) {
     PL::template compute<false>(v, t, twA_s + S::twA(NP - 1));
   }
 
-  // ---- ETD1 update on the natural-order values held in registers
+  // ---- ETD1 update in FP64 through the exchange buffer: publish the natural-order
+  // spectrum, update it in a loop of bounded register use with coalesced n_hat and
+  // coefficient accesses, then reload it for sequence B
   constexpr int RL = S::radA(NP - 1), NBL = EE / RL;
   using PO = FastPass<T, NY, EE, RL, NY / RL, P>;
-  const cplx<T>* nin = gnin + (size_t)kx * NY;
-  cplx<T>* nout = gnout + (size_t)kx * NY;
+#pragma unroll
+  for (int b = 0; b < NBL; ++b)
+#pragma unroll
+    for (int q = 0; q < RL; ++q) buf[padi<P>(PO::out_index(t, b, q))] = v[b * RL + q];
+  group_sync<TPF>(g);
+  const cplx<double>* nin = gnin + (size_t)kx * NY;
+  cplx<double>* nout = gnout + (size_t)kx * NY;
   if (kx != 0) {
-    const cplx<T>* cf = gcoef + (size_t)kx * nyh;
-#pragma unroll
-    for (int b = 0; b < NBL; ++b)
-#pragma unroll
-      for (int q = 0; q < RL; ++q) {
-        const int ky = PO::out_index(t, b, q);
-        const int kh = ky <= NY / 2 ? ky : NY - ky;
-        const cplx<T> c = cf[kh];
-        const cplx<T> p = nin[ky];
-        const cplx<T> o = c.x * p + c.y * v[b * RL + q];
-        nout[ky] = o;
-        v[b * RL + q] = o;
-      }
+    const cplx<double>* cf = gcoef + (size_t)kx * nyh;
+#pragma unroll 4
+    for (int ky = t; ky < NY; ky += TPF) {
+      const int kh = ky <= NY / 2 ? ky : NY - ky;
+      const cplx<double> c = cf[kh];
+      const cplx<double> p = nin[ky];
+      const cplx<T> gv = buf[padi<P>(ky)];
+      const cplx<double> o = p + c.x * p + c.y * mk((double)gv.x, (double)gv.y);
+      nout[ky] = o;
+      buf[padi<P>(ky)] = mk((T)o.x, (T)o.y);
+    }
   } else {
-    // packed DC/Nyquist column: unpack from the (ky, -ky) pairs
-#pragma unroll
-    for (int b = 0; b < NBL; ++b)
-#pragma unroll
-      for (int q = 0; q < RL; ++q) buf[padi<P>(PO::out_index(t, b, q))] = v[b * RL + q];
-    group_sync<TPF>(g);
-    const cplx<T>* c0 = gcoef;
-    const cplx<T>* cm = gcoef + (size_t)m * nyh;
-#pragma unroll
-    for (int b = 0; b < NBL; ++b)
-#pragma unroll
-      for (int q = 0; q < RL; ++q) {
-        const int ky = PO::out_index(t, b, q);
-        const int kyp = ky == 0 ? 0 : NY - ky;
-        const int kh = ky <= NY / 2 ? ky : NY - ky;
-        const cplx<T> qk = v[b * RL + q], qkp = buf[padi<P>(kyp)];
-        const cplx<T> pk = nin[ky], pkp = nin[kyp];
-        cplx<T> h0, hm, g0, gm;
-        unpack_pair(pk, pkp, h0, hm);
-        unpack_pair(qk, qkp, g0, gm);
-        const cplx<T> a0 = c0[kh], am = cm[kh];
-        const cplx<T> h0n = a0.x * h0 + a0.y * g0;
-        const cplx<T> hmn = am.x * hm + am.y * gm;
-        const cplx<T> o = h0n + mul_i(hmn);
-        nout[ky] = o;
-        v[b * RL + q] = o;
+    // packed DC/Nyquist column: one (ky, -ky) pair per step
+    const cplx<double>* c0 = gcoef;
+    const cplx<double>* cm = gcoef + (size_t)m * nyh;
+#pragma unroll 2
+    for (int ky = t; ky <= NY / 2; ky += TPF) {
+      const int kyp = ky == 0 ? 0 : NY - ky;
+      const cplx<T> qkt = buf[padi<P>(ky)], qkpt = buf[padi<P>(kyp)];
+      const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
+      const cplx<double> pk = nin[ky], pkp = nin[kyp];
+      cplx<double> h0, hm, g0, gm;
+      unpack_pair(pk, pkp, h0, hm);
+      unpack_pair(qk, qkp, g0, gm);
+      const cplx<double> a0 = c0[ky], am = cm[ky];
+      const cplx<double> h0n = h0 + a0.x * h0 + a0.y * g0;
+      const cplx<double> hmn = hm + am.x * hm + am.y * gm;
+      const cplx<double> ok = h0n + mul_i(hmn), okp = conj(h0n) + mul_i(conj(hmn));
+      nout[ky] = ok;
+      buf[padi<P>(ky)] = mk((T)ok.x, (T)ok.y);
+      if (kyp != ky) {
+        nout[kyp] = okp;
+        buf[padi<P>(kyp)] = mk((T)okp.x, (T)okp.y);
       }
+    }
   }
+  group_sync<TPF>(g);
+  FastPass<T, NY, EE, S::radB(0), 1, P>::load(buf, v, t);
   group_sync<TPF>(g);
 
   // ---- inverse sequence B; the last pass writes W to HBM

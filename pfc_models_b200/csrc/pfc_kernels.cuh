@@ -141,16 +141,20 @@ struct RowArgs {
   double g, min_phi, min_log, epsilon;
 };
 
+// The spectral state n_hat is FP64 in both precision forms and the update
+// n_hat' = n_hat + (A - 1) n_hat + Bg N_hat runs in FP64: slow modes (A near 1)
+// neither lose their increments to rounding of the state nor drift by a rounded A.
 template <class T>
 struct ColArgs {
   int nx, ny, m, cols, tpf, ld, nyh;
   FftDesc fft;
   const cplx<T>* tw;
-  const cplx<T>* in;        // V (step/init/combine), n_hat (parseval/export)
-  const cplx<T>* nin;       // n_hat (step/combine)
-  cplx<T>* nout;            // n_hat' (step/init)
+  const cplx<T>* in;        // V (step/init/combine)
+  const cplx<double>* sin;  // n_hat (parseval/export)
+  const cplx<double>* nin;  // n_hat (step/combine)
+  cplx<double>* nout;       // n_hat' (step/init)
   cplx<T>* wout;            // W' (step/init/combine)
-  const cplx<T>* coef;      // (A, Bg) pairs [kx][ky], kx <= m, ky <= ny/2
+  const cplx<double>* coef; // (A - 1, Bg) [kx][ky], kx <= m, ky <= ny/2, FP64
   double* partials;
   double* out_c128;         // export: (ny, m+1) complex128
   int dev_form;             // deviation form: keep the DC of column 0 at zero
@@ -341,11 +345,11 @@ __global__ void __launch_bounds__(LB) col_kernel(ColArgs<T> a) {
     // no transform: direct pass over n_hat
     KSum acc[1] = {{0.0, 0.0}};
     if (valid) {
-      const cplx<T>* col = a.in + (size_t)kx * ny;
+      const cplx<double>* col = a.sin + (size_t)kx * ny;
       for (int ky = lt; ky < ny; ky += tpf) {
         const int kyp = ky == 0 ? 0 : ny - ky;
         if (kx == 0) {
-          cplx<T> h0, hm;
+          cplx<double> h0, hm;
           unpack_pair(col[ky], col[kyp], h0, hm);
           if (MODE == kColParseval) {
             const double k0 = ksq(0, ky, ny, a.fx, a.fy), kM = ksq(m, ky, ny, a.fx, a.fy);
@@ -361,7 +365,7 @@ __global__ void __launch_bounds__(LB) col_kernel(ColArgs<T> a) {
             o[2 * m] = hm.x; o[2 * m + 1] = hm.y;
           }
         } else {
-          const cplx<T> v = col[ky];
+          const cplx<double> v = col[ky];
           if (MODE == kColParseval) {
             const double k2 = ksq(kx, ky, ny, a.fx, a.fy);
             const double l = (a.beta / 2.0) * (a.q0 * a.q0 - k2) * (a.q0 * a.q0 - k2);
@@ -392,47 +396,48 @@ __global__ void __launch_bounds__(LB) col_kernel(ColArgs<T> a) {
 
   if (MODE == kColInit) {
     if (valid) {
-      cplx<T>* out = a.nout + (size_t)kx * ny;
+      cplx<double>* out = a.nout + (size_t)kx * ny;
       for (int ky = lt; ky < ny; ky += tpf) {
         cplx<T> v = buf[ky];
         if (a.dev_form && kx == 0 && ky == 0) { v.x = T(0); buf[0] = v; }
-        out[ky] = v;
+        out[ky] = mk((double)v.x, (double)v.y);
       }
     }
     __syncthreads();
   } else if (MODE == kColStep) {
     if (valid) {
-      const cplx<T>* nin = a.nin + (size_t)kx * ny;
-      cplx<T>* nout = a.nout + (size_t)kx * ny;
+      const cplx<double>* nin = a.nin + (size_t)kx * ny;
+      cplx<double>* nout = a.nout + (size_t)kx * ny;
       for (int ky = lt; ky <= ny / 2; ky += tpf) {
         const int kyp = ky == 0 ? 0 : ny - ky;
-        const cplx<T> qk = buf[ky], qkp = buf[kyp];
-        const cplx<T> pk = nin[ky], pkp = nin[kyp];
-        cplx<T> ok, okp;
+        const cplx<T> qkt = buf[ky], qkpt = buf[kyp];
+        const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
+        const cplx<double> pk = nin[ky], pkp = nin[kyp];
+        cplx<double> ok, okp;
         if (kx == 0) {
-          const cplx<T> c0v = a.coef[ky], cMv = a.coef[(size_t)m * nyh + ky];
-          cplx<T> h0, hm, g0, gm;
+          const cplx<double> c0v = a.coef[ky], cMv = a.coef[(size_t)m * nyh + ky];
+          cplx<double> h0, hm, g0, gm;
           unpack_pair(pk, pkp, h0, hm);
           unpack_pair(qk, qkp, g0, gm);
-          const cplx<T> h0n = c0v.x * h0 + c0v.y * g0;
-          const cplx<T> hmn = cMv.x * hm + cMv.y * gm;
+          const cplx<double> h0n = h0 + c0v.x * h0 + c0v.y * g0;
+          const cplx<double> hmn = hm + cMv.x * hm + cMv.y * gm;
           ok = h0n + mul_i(hmn);
           okp = conj(h0n) + mul_i(conj(hmn));
         } else {
-          const cplx<T> c = a.coef[(size_t)kx * nyh + ky];
-          ok = c.x * pk + c.y * qk;
-          okp = c.x * pkp + c.y * qkp;
+          const cplx<double> c = a.coef[(size_t)kx * nyh + ky];
+          ok = pk + c.x * pk + c.y * qk;
+          okp = pkp + c.x * pkp + c.y * qkp;
         }
         nout[ky] = ok;
-        buf[ky] = ok;
-        if (kyp != ky) { nout[kyp] = okp; buf[kyp] = okp; }
+        buf[ky] = mk((T)ok.x, (T)ok.y);
+        if (kyp != ky) { nout[kyp] = okp; buf[kyp] = mk((T)okp.x, (T)okp.y); }
       }
     }
     __syncthreads();
   } else if (MODE == kColCombine) {
     // mu_hat = L_mu n_hat + N_hat (optionally Gaussian-filtered), or G n_hat, or N_hat
     if (valid) {
-      const cplx<T>* nin = a.nin + (size_t)kx * ny;
+      const cplx<double>* nin = a.nin + (size_t)kx * ny;
       const double q2 = a.q0 * a.q0;
       for (int ky = lt; ky <= ny / 2; ky += tpf) {
         const int kyp = ky == 0 ? 0 : ny - ky;
@@ -451,24 +456,27 @@ __global__ void __launch_bounds__(LB) col_kernel(ColArgs<T> a) {
             default: mn[h] = 1.0; mq[h] = 0.0; break;
           }
         }
-        const cplx<T> pk = nin[ky], pkp = nin[kyp];
-        cplx<T> qk = mk(T(0), T(0)), qkp = qk;
-        if (need_v) { qk = buf[ky]; qkp = buf[kyp]; }
-        cplx<T> ok, okp;
+        const cplx<double> pk = nin[ky], pkp = nin[kyp];
+        cplx<double> qk = mk(0.0, 0.0), qkp = qk;
+        if (need_v) {
+          qk = mk((double)buf[ky].x, (double)buf[ky].y);
+          qkp = mk((double)buf[kyp].x, (double)buf[kyp].y);
+        }
+        cplx<double> ok, okp;
         if (kx == 0) {
-          cplx<T> h0, hm, g0, gm;
+          cplx<double> h0, hm, g0, gm;
           unpack_pair(pk, pkp, h0, hm);
           unpack_pair(qk, qkp, g0, gm);
-          const cplx<T> h0n = (T)mn[0] * h0 + (T)mq[0] * g0;
-          const cplx<T> hmn = (T)mn[1] * hm + (T)mq[1] * gm;
+          const cplx<double> h0n = mn[0] * h0 + mq[0] * g0;
+          const cplx<double> hmn = mn[1] * hm + mq[1] * gm;
           ok = h0n + mul_i(hmn);
           okp = conj(h0n) + mul_i(conj(hmn));
         } else {
-          ok = (T)mn[0] * pk + (T)mq[0] * qk;
-          okp = (T)mn[0] * pkp + (T)mq[0] * qkp;
+          ok = mn[0] * pk + mq[0] * qk;
+          okp = mn[0] * pkp + mq[0] * qkp;
         }
-        buf[ky] = ok;
-        if (kyp != ky) buf[kyp] = okp;
+        buf[ky] = mk((T)ok.x, (T)ok.y);
+        if (kyp != ky) buf[kyp] = mk((T)okp.x, (T)okp.y);
       }
     }
     __syncthreads();

@@ -213,7 +213,7 @@ ColArgs<T> col_args(const pfc_plan* h) {
   a.nyh = h->nyh;
   a.fft = h->colfft;
   a.tw = reinterpret_cast<const cplx<T>*>(h->tw);
-  a.coef = reinterpret_cast<const cplx<T>*>(h->coef);
+  a.coef = static_cast<const cplx<double>*>(h->coef);
   a.dev_form = h->fp32 ? 1 : 0;
   a.scale = 1.0 / ((double)h->nx * (double)h->ny);
   const double dx = h->prob.lx / h->nx, dy = h->prob.ly / h->ny;
@@ -404,10 +404,10 @@ int launch_step_col(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
     a.batch = table;
     a.m = h->m; a.ny = h->ny; a.nyh = h->nyh;
     a.in = reinterpret_cast<const cplx<T>*>(h->V);
-    a.nin = reinterpret_cast<const cplx<T>*>(h->nhat[h->cur]);
-    a.nout = reinterpret_cast<cplx<T>*>(h->nhat[h->cur ^ 1]);
+    a.nin = reinterpret_cast<const cplx<double>*>(h->nhat[h->cur]);
+    a.nout = reinterpret_cast<cplx<double>*>(h->nhat[h->cur ^ 1]);
     a.wout = reinterpret_cast<cplx<T>*>(h->W);
-    a.coef = reinterpret_cast<const cplx<T>*>(h->coef);
+    a.coef = static_cast<const cplx<double>*>(h->coef);
     const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(h->tw);
     a.twA = tw + h->tw_ca; a.twB = tw + h->tw_cb;
     a.scale = (T)(1.0 / ((double)h->nx * (double)h->ny));
@@ -420,8 +420,8 @@ int launch_step_col(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
   ColArgs<T> ca = col_args<T>(h);
   ca.in = reinterpret_cast<const cplx<T>*>(h->V);
   ca.wout = reinterpret_cast<cplx<T>*>(h->W);
-  ca.nin = reinterpret_cast<const cplx<T>*>(h->nhat[h->cur]);
-  ca.nout = reinterpret_cast<cplx<T>*>(h->nhat[h->cur ^ 1]);
+  ca.nin = reinterpret_cast<const cplx<double>*>(h->nhat[h->cur]);
+  ca.nout = reinterpret_cast<cplx<double>*>(h->nhat[h->cur ^ 1]);
   return launch_col<T, kColStep>(h, ca, s);
 }
 
@@ -445,7 +445,7 @@ int do_set_state(pfc_plan* h, const double* field, cudaStream_t s) {
   if (rc) return rc;
   ColArgs<T> ca = col_args<T>(h);
   ca.in = reinterpret_cast<const cplx<T>*>(h->V);
-  ca.nout = reinterpret_cast<cplx<T>*>(h->nhat[h->cur]);
+  ca.nout = reinterpret_cast<cplx<double>*>(h->nhat[h->cur]);
   ca.wout = reinterpret_cast<cplx<T>*>(h->W);
   rc = launch_col<T, kColInit>(h, ca, s);
   if (rc) return rc;
@@ -644,7 +644,7 @@ int do_reduce(pfc_plan* h, double* out3, cudaStream_t s) {
   int rc = launch_row<T, kRowReduce>(h, ra, s);
   if (rc) return rc;
   ColArgs<T> ca = col_args<T>(h);
-  ca.in = reinterpret_cast<const cplx<T>*>(h->nhat[h->cur]);
+  ca.sin = reinterpret_cast<const cplx<double>*>(h->nhat[h->cur]);
   ca.partials = colp;
   rc = launch_col<T, kColParseval>(h, ca, s);
   if (rc) return rc;
@@ -685,7 +685,7 @@ int do_get_field(pfc_plan* h, int which, double w, double* out, cudaStream_t s) 
   if (rc) return rc;
   ColArgs<T> ca = col_args<T>(h);
   ca.in = reinterpret_cast<const cplx<T>*>(h->V);
-  ca.nin = reinterpret_cast<const cplx<T>*>(nold);
+  ca.nin = reinterpret_cast<const cplx<double>*>(nold);
   ca.wout = reinterpret_cast<cplx<T>*>(h->W2);
   ca.w = w;
   int addslot = kScalZero;
@@ -706,7 +706,7 @@ int do_get_spectrum(pfc_plan* h, int which, double* out, cudaStream_t s) {
   const void* src = h->nhat[h->cur];
   if (which == PFC_SPEC_N_HAT && h->steps_since_set > 0) src = h->nhat[h->cur ^ 1];
   ColArgs<T> ca = col_args<T>(h);
-  ca.in = reinterpret_cast<const cplx<T>*>(src);
+  ca.sin = reinterpret_cast<const cplx<double>*>(src);
   ca.out_c128 = out;
   int rc = launch_col<T, kColExport>(h, ca, s);
   if (rc) return rc;
@@ -824,7 +824,7 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   const double twopi = 6.283185307179586;
   h->hostA.assign((size_t)p->ny * (m + 1), 0.0);
   h->hostBg.assign((size_t)p->ny * (m + 1), 0.0);
-  std::vector<double> coefA((size_t)(m + 1) * h->nyh), coefB((size_t)(m + 1) * h->nyh);
+  std::vector<double> coefA(2 * (size_t)(m + 1) * h->nyh);   // (A - 1, Bg) pairs
   for (int ky = 0; ky < p->ny; ++ky) {
     const int kys = (ky <= (p->ny - 1) / 2) ? ky : ky - p->ny;
     const double kyp = twopi * ((double)kys * fy);
@@ -841,9 +841,10 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
       const double Bg = B * gl;
       h->hostA[(size_t)ky * (m + 1) + kx] = A;
       h->hostBg[(size_t)ky * (m + 1) + kx] = Bg;
+      // the device applies n' = n + (A - 1) n + Bg N in FP64, with A - 1 = expm1(z)
       if (ky < h->nyh) {
-        coefA[(size_t)kx * h->nyh + ky] = A;
-        coefB[(size_t)kx * h->nyh + ky] = Bg;
+        coefA[2 * ((size_t)kx * h->nyh + ky)] = std::expm1(z);
+        coefA[2 * ((size_t)kx * h->nyh + ky) + 1] = Bg;
       }
     }
   }
@@ -852,11 +853,13 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
 
   // ---- device buffers
   const size_t specb = h->nspec * h->elt;
+  // the spectral state is FP64 in both forms
+  const size_t stateb = h->nspec * sizeof(double2);
   cudaError_t e = cudaSuccess;
-  for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMalloc(&h->nhat[i], specb);
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMalloc(&h->nhat[i], stateb);
   if (e == cudaSuccess) e = cudaMalloc(&h->W, specb);
   if (e == cudaSuccess) e = cudaMalloc(&h->V, specb);
-  if (e == cudaSuccess) e = cudaMalloc(&h->coef, (size_t)(m + 1) * h->nyh * h->elt);
+  if (e == cudaSuccess) e = cudaMalloc(&h->coef, (size_t)(m + 1) * h->nyh * sizeof(double2));
   if (e == cudaSuccess) e = cudaMalloc(&h->tw, tw.size() / 2 * h->elt);
   h->npartials = 6 * (size_t)h->row_grid + 2 * (size_t)h->col_grid + 2 * 1024;
   if (e == cudaSuccess) e = cudaMalloc(&h->partials, h->npartials * sizeof(double));
@@ -866,7 +869,7 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
     return cleanup_fail(fail(e == cudaErrorMemoryAllocation ? PFC_E_NOMEM : PFC_E_CUDA,
                              "pfc_plan_create: cudaMalloc failed: %s", cudaGetErrorString(e)));
 
-  // upload tables in the working precision
+  // upload the twiddle tables in the working precision, the coefficients (A - 1, Bg) in FP64
   {
     std::vector<unsigned char> host;
     const size_t ntw = tw.size() / 2;
@@ -876,19 +879,14 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
       else { double2 v = make_double2((double)tw[2 * i], (double)tw[2 * i + 1]); memcpy(&host[i * 16], &v, 16); }
     }
     e = cudaMemcpy(h->tw, host.data(), host.size(), cudaMemcpyHostToDevice);
-    const size_t nc = (size_t)(m + 1) * h->nyh;
-    host.assign(nc * h->elt, 0);
-    for (size_t i = 0; i < nc; ++i) {
-      if (h->fp32) { float2 v = make_float2((float)coefA[i], (float)coefB[i]); memcpy(&host[i * 8], &v, 8); }
-      else { double2 v = make_double2(coefA[i], coefB[i]); memcpy(&host[i * 16], &v, 16); }
-    }
-    if (e == cudaSuccess) e = cudaMemcpy(h->coef, host.data(), host.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(h->coef, coefA.data(), coefA.size() * sizeof(double), cudaMemcpyHostToDevice);
     std::vector<double> sc(kScalCount, 0.0);
     if (e == cudaSuccess) e = cudaMemcpy(h->scal, sc.data(), sc.size() * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(h->status, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->W, 0, specb);
-    if (e == cudaSuccess) e = cudaMemset(h->nhat[0], 0, specb);
-    if (e == cudaSuccess) e = cudaMemset(h->nhat[1], 0, specb);
+    if (e == cudaSuccess) e = cudaMemset(h->nhat[0], 0, stateb);
+    if (e == cudaSuccess) e = cudaMemset(h->nhat[1], 0, stateb);
     if (e != cudaSuccess)
       return cleanup_fail(fail(PFC_E_CUDA, "pfc_plan_create: upload failed: %s", cudaGetErrorString(e)));
   }
