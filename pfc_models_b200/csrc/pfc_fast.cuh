@@ -208,11 +208,11 @@ __device__ __forceinline__ void l2_prefetch_range(const void* p, unsigned bytes,
 
 template <int TPF> struct FastBound { static constexpr int value = TPF > 256 ? TPF : 256; };
 // minimum resident CTAs per SM requested from the register allocator (256-thread CTAs)
-// from an estimate of the registers a thread needs: 2 per real held, plus ~40
+// from the registers the values held take (2 per real): with up to 32 of them the
+// kernels fit 64 registers without spilling (4 CTAs per SM), with 64 they need 128
 template <class T, int EE, int TPF> struct FastMinBlocks {
-  static constexpr int regs = 2 * EE * (int)(sizeof(T) / 4) + 40;
-  static constexpr int fit = 65536 / (256 * regs);
-  static constexpr int value = TPF > 256 ? 1 : (fit < 1 ? 1 : (fit > 4 ? 4 : fit));
+  static constexpr int data_regs = 2 * EE * (int)(sizeof(T) / 4);
+  static constexpr int value = TPF > 256 ? 1 : (data_regs <= 32 ? 4 : 2);
 };
 
 // ------------------------------------------------------------------ row kernel
