@@ -170,6 +170,7 @@ struct BatchBufs {
 template <class T>
 struct FastRowArgs {
   int ny, rows, ld;
+  int rows_log2;             // rows = 1 << rows_log2
   const BatchBufs* batch;    // null: one plan, the pointers below
   const cplx<T>* in;         // W, column-major [kx][y]
   cplx<T>* out;              // V, column-major
@@ -229,7 +230,7 @@ row_step_fast(FastRowArgs<T> a) {
   constexpr int EE = S::EE, TPF = S::TPF, NP = S::NPASS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
-  const int ny = a.ny, rows = a.rows, ld = a.ld;
+  const int ny = a.ny, rows = a.rows, ld = a.ld, rl2 = a.rows_log2;
   const int y0 = blockIdx.x * rows;
   const int ngroups = blockDim.x / TPF;
   const int g = threadIdx.x / TPF, t = threadIdx.x - g * TPF;
@@ -247,7 +248,7 @@ row_step_fast(FastRowArgs<T> a) {
   // ---- transposing tile load: element (kx, y0 + r) -> sm[r * ld + pad(kx)], issued as
   // asynchronous global->shared copies so that every load of the tile is in flight at once
   for (int i = threadIdx.x; i < rows * M; i += blockDim.x) {
-    const int r = i % rows, kx = i / rows;
+    const int r = i & (rows - 1), kx = i >> rl2;
     cplx<T>* dst = sm + r * ld + padi<P>(kx);
     if (y0 + r < ny) {
       const unsigned sdst = (unsigned)__cvta_generic_to_shared(dst);
@@ -364,7 +365,7 @@ row_step_fast(FastRowArgs<T> a) {
   __syncthreads();
   // ---- transposing tile store
   for (int i = threadIdx.x; i < rows * M; i += blockDim.x) {
-    const int r = i % rows, kx = i / rows;
+    const int r = i & (rows - 1), kx = i >> rl2;
     if (y0 + r < ny) gout[(size_t)kx * ny + (y0 + r)] = sm[r * ld + padi<P>(kx)];
   }
 }

@@ -347,7 +347,8 @@ int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
   const int ngc = std::min(std::max(1, 256 / tpc), h->m);
   const size_t fr_smem = (size_t)rows * ld * elt;
   const size_t fc_smem = (size_t)ngc * (h->ny + (h->ny >> P) + 2) * elt;   // one exchange buffer per column
-  if (ngr * tpr > 1024 || ngc * tpc > 1024 || fr_smem > 200 * 1024 || fc_smem > 200 * 1024)
+  if (ngr * tpr > 1024 || ngc * tpc > 1024 || fr_smem > 200 * 1024 || fc_smem > 200 * 1024 ||
+      ilog2_exact(rows) < 0)
     return PFC_OK;  // generic path
   h->fr_rows = rows;
   h->fr_threads = ngr * tpr;
@@ -375,7 +376,7 @@ int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
   if (h->fast) {
     FastRowArgs<T> a{};
     a.batch = table;
-    a.ny = h->ny; a.rows = h->fr_rows; a.ld = h->fr_ld;
+    a.ny = h->ny; a.rows = h->fr_rows; a.ld = h->fr_ld; a.rows_log2 = ilog2_exact(h->fr_rows);
     a.in = reinterpret_cast<const cplx<T>*>(h->W);
     a.out = reinterpret_cast<cplx<T>*>(h->V);
     const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(h->tw);
