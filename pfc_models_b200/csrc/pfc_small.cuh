@@ -1,4 +1,4 @@
-// Single-thread and grid-stride helper kernels of the plan's entry points
+// One-warp and grid-stride helper kernels of the plan's entry points
 // (reductions' final merges, mean handling). Included by one translation unit only.
 #pragma once
 #include "pfc_kernels.cuh"
@@ -6,24 +6,38 @@
 namespace pfc {
 
 // ---------------------------------------------------------------- small kernels
-// Final reduction of per-CTA compensated partials, in a fixed order.
+// Merge of n compensated (sum, compensation) pairs at p[stride * b], b < n, by one
+// warp in a fixed order: lane l merges b = l, l + 32, ... in turn, then the lanes
+// combine in a fixed shuffle tree. The result (valid in lane 0) is deterministic.
+__device__ KSum warp_merge(const double* p, int n, int stride) {
+  const int lane = threadIdx.x & 31;
+  KSum acc = {0.0, 0.0};
+  for (int b = lane; b < n; b += 32) {
+    const KSum o = {p[(size_t)stride * b], p[(size_t)stride * b + 1]};
+    acc = ksum_merge(acc, o);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    KSum o;
+    o.s = __shfl_down_sync(0xffffffffu, acc.s, off);
+    o.c = __shfl_down_sync(0xffffffffu, acc.c, off);
+    acc = ksum_merge(acc, o);
+  }
+  return acc;
+}
+
+// Final reduction of per-CTA compensated partials (one warp), in a fixed order.
 // row partials: 3 sums (raw, fpoly, nonlin) x nrow; col partials: 1 sum x ncol.
 // out3 = {F per site, mu per site, mean}.
 __global__ void finalize_reduce_kernel(const double* rowp, int nrow, const double* colp, int ncol,
                                        const double* scal, double inv_sites, double lmu0, double lf0,
                                        int dev_form, double* out3, int* status) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  KSum q[3] = {{0, 0}, {0, 0}, {0, 0}};
-  for (int b = 0; b < nrow; ++b)
-    for (int k = 0; k < 3; ++k) {
-      KSum o = {rowp[6 * b + 2 * k], rowp[6 * b + 2 * k + 1]};
-      q[k] = ksum_merge(q[k], o);
-    }
-  KSum p = {0, 0};
-  for (int b = 0; b < ncol; ++b) {
-    KSum o = {colp[2 * b], colp[2 * b + 1]};
-    p = ksum_merge(p, o);
-  }
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  KSum q[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) q[k] = warp_merge(rowp + 2 * k, nrow, 6);
+  const KSum p = warp_merge(colp, ncol, 2);
+  if (threadIdx.x != 0) return;
   const double mean_dev = dev_form ? scal[kScalMean] : 0.0;
   const double raw_mean = (q[0].s + q[0].c) * inv_sites;
   double grad = (p.s + p.c) * inv_sites * inv_sites;
@@ -39,13 +53,9 @@ __global__ void finalize_reduce_kernel(const double* rowp, int nrow, const doubl
 
 // Sum of materialise partials -> scal[kScalCorr] = sum / sites (deviation mean correction).
 __global__ void finalize_mean_kernel(const double* p, int nb, double inv_sites, double* scal) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  KSum acc = {0, 0};
-  for (int b = 0; b < nb; ++b) {
-    KSum o = {p[2 * b], p[2 * b + 1]};
-    acc = ksum_merge(acc, o);
-  }
-  scal[kScalCorr] = (acc.s + acc.c) * inv_sites;
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  const KSum acc = warp_merge(p, nb, 2);
+  if (threadIdx.x == 0) scal[kScalCorr] = (acc.s + acc.c) * inv_sites;
 }
 
 __global__ void shift_kernel(double* x, size_t n, const double* by) {
@@ -65,12 +75,9 @@ __global__ void field_sum_kernel(const double* x, size_t n, double* partials) {
 // Deviation-form scalars from the mean (std and log nonlinearities).
 __global__ void set_scalars_kernel(const double* p, int nb, double inv_sites, int model, double g,
                                    double min_phi, double lmu0, double* scal) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  KSum acc = {0, 0};
-  for (int b = 0; b < nb; ++b) {
-    KSum o = {p[2 * b], p[2 * b + 1]};
-    acc = ksum_merge(acc, o);
-  }
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  const KSum acc = warp_merge(p, nb, 2);
+  if (threadIdx.x != 0) return;
   const double mu = (acc.s + acc.c) * inv_sites;
   scal[kScalMean] = mu;
   scal[kScalC1] = 2.0 * g * mu + 3.0 * mu * mu;
