@@ -33,7 +33,7 @@ struct FastSeq {
   __host__ __device__ static constexpr int radB(int p) { return p == 0 ? LAST : RC; }
   __host__ __device__ static constexpr int nsA(int p) { return p == 0 ? 1 : nsA(p - 1) * radA(p - 1); }
   __host__ __device__ static constexpr int nsB(int p) { return p == 0 ? 1 : nsB(p - 1) * radB(p - 1); }
-  // offset of pass p's twiddle table ([k][q-1], k < ns, q < R) within the sequence table
+  // offset of pass p's twiddle table ([q-1][k], q < R, k < ns) within the sequence table
   __host__ __device__ static constexpr int twA(int p) { return p <= 1 ? 0 : twA(p - 1) + nsA(p - 1) * (radA(p - 1) - 1); }
   __host__ __device__ static constexpr int twB(int p) { return p <= 1 ? 0 : twB(p - 1) + nsB(p - 1) * (radB(p - 1) - 1); }
   __host__ __device__ static constexpr int sizeA() { return twA(NPASS); }
@@ -101,10 +101,11 @@ struct FastPass {
       if constexpr (NS > 1) {
         const int j = t + b * TPF;
         const int k = j & (NS - 1);
-        const cplx<T>* w = tw + k * (R - 1);
+        // table [q-1][k]: consecutive lanes read consecutive entries
+        const cplx<T>* w = tw + k;
         cplx<T> wq[R];
 #pragma unroll
-        for (int q = 1; q < R; ++q) wq[q] = ldgc(w + q - 1);
+        for (int q = 1; q < R; ++q) wq[q] = ldgc(w + (q - 1) * NS);
 #pragma unroll
         for (int q = 1; q < R; ++q) {
           cplx<T> x = wq[q];
@@ -246,17 +247,24 @@ row_step_fast(FastRowArgs<T> a) {
   }
 
   // ---- transposing tile load: element (kx, y0 + r) -> sm[r * ld + pad(kx)], issued as
-  // asynchronous global->shared copies so that every load of the tile is in flight at once
-  for (int i = threadIdx.x; i < rows * M; i += blockDim.x) {
-    const int r = i & (rows - 1), kx = i >> rl2;
-    cplx<T>* dst = sm + r * ld + padi<P>(kx);
-    if (y0 + r < ny) {
-      const unsigned sdst = (unsigned)__cvta_generic_to_shared(dst);
-      const cplx<T>* src = gin + (size_t)kx * ny + (y0 + r);
-      asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sdst), "l"(src), "n"(sizeof(cplx<T>))
-                   : "memory");
-    } else {
-      *dst = mk(T(0), T(0));
+  // asynchronous global->shared copies so that every load of the tile is in flight at once.
+  // blockDim is a multiple of rows: each thread keeps one row and walks kx with a fixed
+  // stride, so the addresses advance by constants.
+  const int tr = threadIdx.x & (rows - 1), kx0 = threadIdx.x >> rl2, kstep = blockDim.x >> rl2;
+  const bool rvalid = y0 + tr < ny;
+  const size_t gstep = (size_t)kstep * ny;
+  {
+    cplx<T>* drow = sm + tr * ld;
+    const cplx<T>* src = gin + (size_t)kx0 * ny + (y0 + tr);
+    for (int kx = kx0; kx < M; kx += kstep, src += gstep) {
+      cplx<T>* dst = drow + padi<P>(kx);
+      if (rvalid) {
+        const unsigned sdst = (unsigned)__cvta_generic_to_shared(dst);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sdst), "l"(src), "n"(sizeof(cplx<T>))
+                     : "memory");
+      } else {
+        *dst = mk(T(0), T(0));
+      }
     }
   }
   // twiddle tables are read through the L1 cache
@@ -363,10 +371,11 @@ row_step_fast(FastRowArgs<T> a) {
     }
   }
   __syncthreads();
-  // ---- transposing tile store
-  for (int i = threadIdx.x; i < rows * M; i += blockDim.x) {
-    const int r = i & (rows - 1), kx = i >> rl2;
-    if (y0 + r < ny) gout[(size_t)kx * ny + (y0 + r)] = sm[r * ld + padi<P>(kx)];
+  // ---- transposing tile store, with the same thread-to-element map as the load
+  if (rvalid) {
+    const cplx<T>* srow = sm + tr * ld;
+    cplx<T>* dst = gout + (size_t)kx0 * ny + (y0 + tr);
+    for (int kx = kx0; kx < M; kx += kstep, dst += gstep) *dst = srow[padi<P>(kx)];
   }
 }
 

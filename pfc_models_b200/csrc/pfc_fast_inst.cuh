@@ -11,7 +11,8 @@ namespace pfc {
 namespace fast_detail {
 
 // Pass tables of sequences A and B for an N-point transform, laid out as FastSeq
-// expects: for p = 1 .. NPASS-1, ns(p) x (R(p) - 1) entries exp(-2 pi i q k / (ns R)).
+// expects: for p = 1 .. NPASS-1, (R(p) - 1) x ns(p) entries exp(-2 pi i q k / (ns R)),
+// [q-1][k], so that the lanes of a warp (consecutive k) read consecutive entries.
 template <class T, int N, int EE>
 void seq_tables(std::vector<long double>& tw, int& offA, int& offB) {
   using S = FastSeq<N, EE, RadixCap<T>::value>;
@@ -21,8 +22,8 @@ void seq_tables(std::vector<long double>& tw, int& offA, int& offB) {
     for (int p = 1; p < S::NPASS; ++p) {
       const int R = seq == 0 ? S::radA(p) : S::radB(p);
       const int ns = seq == 0 ? S::nsA(p) : S::nsB(p);
-      for (int k = 0; k < ns; ++k)
-        for (int q = 1; q < R; ++q) {
+      for (int q = 1; q < R; ++q)
+        for (int k = 0; k < ns; ++k) {
           const long double ang = -twopi * (long double)((long long)q * k) / (long double)(ns * R);
           tw.push_back(cosl(ang));
           tw.push_back(sinl(ang));
