@@ -1,8 +1,9 @@
 """ctypes binding of ``libpfc_b200.so`` (the C ABI of ``include/pfc_b200.h``).
 
 The shared library is built in-tree by :mod:`pfc_models_b200.build` and must
-sit next to this file. There is no fallback: if the library is missing or a
-CUDA device is absent, every entry point raises.
+sit next to this file ($PFC_B200_LIB may name another build of it, for A/B
+timing). There is no fallback: if the library is missing or a CUDA device is
+absent, every entry point raises.
 """
 from __future__ import annotations
 
@@ -81,7 +82,7 @@ def load(path: str | None = None):
     with _lock:
         if _lib is not None:
             return _lib
-        p = path or LIB_PATH
+        p = path or os.environ.get("PFC_B200_LIB") or LIB_PATH
         if not os.path.exists(p):
             raise ImportError(f"{p} is not built: run `python -m pfc_models_b200.build` "
                               "(there is no CPU fallback)")

@@ -347,35 +347,35 @@ row_step_fast(FastRowArgs<T> a) {
       group_sync<TPF>(g);
       QL::template compute<false>(v, t, twB_s + S::twB(NP - 1));
     }
-    // ---- forward-real post-twiddle: publish Z, then one (k, M - k) pair per step in place:
-    // Y[k] = E + r_k O, Y[M - k] = conj(E - r_k O), E = (Z[k] + conj Z[M-k]) / 2, O = -i (Z[k] - conj Z[M-k]) / 2
+    // ---- publish Z (the forward transform, natural order) for the fused post-twiddle store
     using QO = FastPass<T, M, EE, RL, M / RL, P>;
     constexpr int NBL = EE / RL;
 #pragma unroll
     for (int b = 0; b < NBL; ++b)
 #pragma unroll
       for (int q = 0; q < RL; ++q) row[padi<P>(QO::out_index(t, b, q))] = v[b * RL + q];
-    group_sync<TPF>(g);
-#pragma unroll 2
-    for (int k = t; k <= M / 2; k += TPF) {
-      if (k == 0) {
-        const cplx<T> z0 = row[0];
-        row[0] = mk(z0.x + z0.y, z0.x - z0.y);
-      } else {
-        const cplx<T> zk = row[padi<P>(k)], zm = row[padi<P>(M - k)];
-        const cplx<T> e = T(0.5) * (zk + conj(zm));
-        const cplx<T> o = cmul(ldgc(a.rtw + k), T(0.5) * rot4<false>(zk - conj(zm)));
-        row[padi<P>(k)] = e + o;
-        if (k != M / 2) row[padi<P>(M - k)] = conj(e - o);
-      }
-    }
   }
   __syncthreads();
-  // ---- transposing tile store, with the same thread-to-element map as the load
+  // ---- forward-real post-twiddle fused with the transposing tile store: one (k, M - k)
+  // pair per step, Y[k] = E + r_k O, Y[M - k] = conj(E - r_k O), with
+  // E = (Z[k] + conj Z[M-k]) / 2, O = -i (Z[k] - conj Z[M-k]) / 2, written to V[k][y]
+  // and V[M - k][y] (consecutive threads take consecutive y of one k: coalesced)
   if (rvalid) {
     const cplx<T>* srow = sm + tr * ld;
-    cplx<T>* dst = gout + (size_t)kx0 * ny + (y0 + tr);
-    for (int kx = kx0; kx < M; kx += kstep, dst += gstep) *dst = srow[padi<P>(kx)];
+    cplx<T>* col0 = gout + (y0 + tr);
+#pragma unroll 2
+    for (int k = kx0; k <= M / 2; k += kstep) {
+      if (k == 0) {
+        const cplx<T> z0 = srow[0];
+        col0[0] = mk(z0.x + z0.y, z0.x - z0.y);
+      } else {
+        const cplx<T> zk = srow[padi<P>(k)], zm = srow[padi<P>(M - k)];
+        const cplx<T> e = T(0.5) * (zk + conj(zm));
+        const cplx<T> o = cmul(ldgc(a.rtw + k), T(0.5) * rot4<false>(zk - conj(zm)));
+        col0[(size_t)k * ny] = e + o;
+        if (k != M / 2) col0[(size_t)(M - k) * ny] = conj(e - o);
+      }
+    }
   }
 }
 
@@ -463,7 +463,7 @@ col_step_fast(FastColArgs<T> a) {
   cplx<double>* nout = gnout + (size_t)kx * NY;
   if (kx != 0) {
     const cplx<double>* cf = gcoef + (size_t)kx * nyh;
-#pragma unroll 4
+#pragma unroll 8
     for (int ky = t; ky < NY; ky += TPF) {
       const int kh = ky <= NY / 2 ? ky : NY - ky;
       const cplx<double> c = cf[kh];
