@@ -179,12 +179,15 @@ struct pfc_plan {
 struct pfc_batch_class {
   std::vector<pfc_plan*> plans;
   pfc::BatchBufs* table[2] = {nullptr, nullptr};  // device tables, by parity of cur
+  cudaStream_t stream = nullptr;                  // classes run concurrently (fork/join)
+  cudaEvent_t done = nullptr;
 };
 
 struct pfc_batch {
   std::vector<pfc_batch_class> classes;
   bool fp32 = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaEvent_t fork = nullptr;
   long long launches = 0;
 };
 
@@ -521,20 +524,31 @@ int do_step(pfc_plan* h, long long nsteps, cudaStream_t s) {
 }
 
 // ---- batches
+// The classes are independent: each runs its nsteps on its own stream, forked from and
+// joined back to `s` (in a capture this makes parallel branches of the graph).
 template <class T>
 int batch_step_direct(pfc_batch* b, int parity, long long nsteps, cudaStream_t s) {
-  for (long long i = 0; i < nsteps; ++i) {
-    for (auto& c : b->classes) {
-      pfc_plan* h = c.plans[0];
-      const int n = (int)c.plans.size();
-      int rc = launch_step_row<T>(h, s, c.table[parity], n);
+  if (nsteps <= 0) return PFC_OK;
+  const bool fork = b->classes.size() > 1;
+  if (fork) PFC_CUDA(cudaEventRecord(b->fork, s));
+  for (auto& c : b->classes) {
+    cudaStream_t cs = fork ? c.stream : s;
+    if (fork) PFC_CUDA(cudaStreamWaitEvent(cs, b->fork, 0));
+    pfc_plan* h = c.plans[0];
+    const int n = (int)c.plans.size();
+    int p = parity;
+    for (long long i = 0; i < nsteps; ++i) {
+      int rc = launch_step_row<T>(h, cs, c.table[p], n);
       if (rc) return rc;
-      rc = launch_step_col<T>(h, s, c.table[parity], n);
+      rc = launch_step_col<T>(h, cs, c.table[p], n);
       if (rc) return rc;
       b->launches += 2;
+      p ^= 1;
     }
-    parity ^= 1;
+    if (fork) PFC_CUDA(cudaEventRecord(c.done, cs));
   }
+  if (fork)
+    for (auto& c : b->classes) PFC_CUDA(cudaStreamWaitEvent(s, c.done, 0));
   return PFC_OK;
 }
 
@@ -1041,6 +1055,15 @@ int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out) {
     }
     cls->plans.push_back(h);
   }
+  cudaError_t es = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  for (auto& c : b->classes) {
+    if (es == cudaSuccess) es = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking);
+    if (es == cudaSuccess) es = cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming);
+  }
+  if (es != cudaSuccess) {
+    pfc_batch_destroy(b);
+    return fail(PFC_E_CUDA, "pfc_batch_create: %s", cudaGetErrorString(es));
+  }
   for (auto& c : b->classes) {
     const size_t n = c.plans.size();
     std::vector<BatchBufs> host(n);
@@ -1078,9 +1101,13 @@ int pfc_batch_destroy(pfc_batch* b) {
   if (!b) return PFC_OK;
   for (auto& g : b->graph)
     if (g) cudaGraphExecDestroy(g);
-  for (auto& c : b->classes)
+  for (auto& c : b->classes) {
     for (auto& tb : c.table)
       if (tb) cudaFree(tb);
+    if (c.done) cudaEventDestroy(c.done);
+    if (c.stream) cudaStreamDestroy(c.stream);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
   delete b;
   return PFC_OK;
 }
