@@ -162,9 +162,12 @@ __device__ __forceinline__ void fast_mid(cplx<T>* buf, cplx<T>* v, int t, int g,
 struct BatchBufs {
   const void* w;        // W (row input, column output)
   void* v;              // V (row output, column input)
-  const void* nin;      // n_hat of the current state
+  const void* nin;      // n_hat of the current state (hi in the FP32 form)
   void* nout;           // n_hat of the next state
-  const void* coef;     // (A, Bg)
+  const void* nin_lo;   // FP32 form: the residual arrays of the two states
+  void* nout_lo;
+  const void* coef;     // (A - 1, Bg), working precision
+  const void* coef64;   // FP32 form: (A - 1, Bg) in FP64
   const double* scal;   // deviation-form scalars
 };
 
@@ -188,10 +191,14 @@ struct FastColArgs {
   int m, ny, nyh;
   const BatchBufs* batch;    // null: one plan, the pointers below
   const cplx<T>* in;         // V
-  const cplx<double>* nin;   // n_hat (FP64 in both precision forms)
-  cplx<double>* nout;        // n_hat'
+  const void* nin;           // n_hat: complex128, or hi (FP32 form; see ColArgs)
+  const cplx<float>* nin_lo;
+  void* nout;                // n_hat'
+  cplx<float>* nout_lo;
   cplx<T>* wout;             // W'
-  const cplx<double>* coef;  // (A - 1, Bg) [kx][ky <= ny/2], FP64
+  const cplx<T>* coef;       // (A - 1, Bg) [kx][ky <= ny/2], working precision
+  const cplx<double>* coef64;  // FP32 form: FP64 copy, read for the slow modes
+  float slow_tau;
   const cplx<T>* twA;        // column sequence A (forward)
   const cplx<T>* twB;        // column sequence B (inverse uses conjugates)
   T scale;
@@ -402,24 +409,31 @@ col_step_fast(FastColArgs<T> a) {
   cplx<T>* buf = sm + g * PADN;                   // exchange buffer of this column
   const int m = a.m, nyh = a.nyh;
   const cplx<T>* gin = a.in;
-  const cplx<double>* gnin = a.nin;
-  cplx<double>* gnout = a.nout;
+  const void* gnin = a.nin;
+  void* gnout = a.nout;
+  const cplx<float>* gnin_lo = a.nin_lo;
+  cplx<float>* gnout_lo = a.nout_lo;
   cplx<T>* gwout = a.wout;
-  const cplx<double>* gcoef = a.coef;
+  const cplx<T>* gcoef = a.coef;
+  const cplx<double>* gcoef64 = a.coef64;
   if (a.batch) {
     const BatchBufs& b = a.batch[blockIdx.y];
     gin = static_cast<const cplx<T>*>(b.v);
-    gnin = static_cast<const cplx<double>*>(b.nin);
-    gnout = static_cast<cplx<double>*>(b.nout);
+    gnin = b.nin;
+    gnout = b.nout;
+    gnin_lo = static_cast<const cplx<float>*>(b.nin_lo);
+    gnout_lo = static_cast<cplx<float>*>(b.nout_lo);
     gwout = static_cast<cplx<T>*>(const_cast<void*>(b.w));
-    gcoef = static_cast<const cplx<double>*>(b.coef);
+    gcoef = static_cast<const cplx<T>*>(b.coef);
+    gcoef64 = static_cast<const cplx<double>*>(b.coef64);
   }
   cplx<T> v[EE];
 
   // ---- start this column's n_hat and coefficients towards L2 while the forward
   // transform runs (the coefficient range is widened to 16-byte boundaries; it stays
   // inside the table, which has a row after every column a CTA handles)
-  l2_prefetch_range(gnin + (size_t)kx * NY, NY * (unsigned)sizeof(cplx<double>), t, TPF);
+  constexpr unsigned kStateElt = sizeof(T) == 8 ? sizeof(cplx<double>) : sizeof(cplx<float>);
+  l2_prefetch_range(static_cast<const char*>(gnin) + (size_t)kx * NY * kStateElt, NY * kStateElt, t, TPF);
   {
     const uintptr_t c0 = reinterpret_cast<uintptr_t>(gcoef + (size_t)kx * nyh) & ~(uintptr_t)15;
     const uintptr_t c1 = (reinterpret_cast<uintptr_t>(gcoef + (size_t)(kx + 1) * nyh) + 15) & ~(uintptr_t)15;
@@ -459,41 +473,45 @@ col_step_fast(FastColArgs<T> a) {
 #pragma unroll
     for (int q = 0; q < RL; ++q) buf[padi<P>(PO::out_index(t, b, q))] = v[b * RL + q];
   group_sync<TPF>(g);
-  const cplx<double>* nin = gnin + (size_t)kx * NY;
-  cplx<double>* nout = gnout + (size_t)kx * NY;
+  const size_t cb = (size_t)kx * NY;
+  const float tau = a.slow_tau;
   if (kx != 0) {
-    const cplx<double>* cf = gcoef + (size_t)kx * nyh;
+    const size_t ccb = (size_t)kx * nyh;
 #pragma unroll 8
     for (int ky = t; ky < NY; ky += TPF) {
       const int kh = ky <= NY / 2 ? ky : NY - ky;
-      const cplx<double> c = cf[kh];
-      const cplx<double> p = nin[ky];
+      bool slow;
+      const cplx<double> c = coef_ld<T>(gcoef, gcoef64, ccb + kh, tau, false, slow);
+      const cplx<double> p = state_ld<T>(gnin, gnin_lo, cb + ky, slow);
       const cplx<T> gv = buf[padi<P>(ky)];
       const cplx<double> o = p + c.x * p + c.y * mk((double)gv.x, (double)gv.y);
-      nout[ky] = o;
+      state_st<T>(gnout, gnout_lo, cb + ky, o, slow);
       buf[padi<P>(ky)] = mk((T)o.x, (T)o.y);
     }
   } else {
-    // packed DC/Nyquist column: one (ky, -ky) pair per step
-    const cplx<double>* c0 = gcoef;
-    const cplx<double>* cm = gcoef + (size_t)m * nyh;
+    // packed DC/Nyquist column (kx = 0 and kx = M): one (ky, -ky) pair per step, always
+    // at full precision
+    const size_t cmb = (size_t)m * nyh;
 #pragma unroll 2
     for (int ky = t; ky <= NY / 2; ky += TPF) {
       const int kyp = ky == 0 ? 0 : NY - ky;
       const cplx<T> qkt = buf[padi<P>(ky)], qkpt = buf[padi<P>(kyp)];
       const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
-      const cplx<double> pk = nin[ky], pkp = nin[kyp];
+      const cplx<double> pk = state_ld<T>(gnin, gnin_lo, cb + ky, true);
+      const cplx<double> pkp = state_ld<T>(gnin, gnin_lo, cb + kyp, true);
       cplx<double> h0, hm, g0, gm;
       unpack_pair(pk, pkp, h0, hm);
       unpack_pair(qk, qkp, g0, gm);
-      const cplx<double> a0 = c0[ky], am = cm[ky];
+      bool s0, sm;
+      const cplx<double> a0 = coef_ld<T>(gcoef, gcoef64, ky, tau, true, s0);
+      const cplx<double> am = coef_ld<T>(gcoef, gcoef64, cmb + ky, tau, true, sm);
       const cplx<double> h0n = h0 + a0.x * h0 + a0.y * g0;
       const cplx<double> hmn = hm + am.x * hm + am.y * gm;
       const cplx<double> ok = h0n + mul_i(hmn), okp = conj(h0n) + mul_i(conj(hmn));
-      nout[ky] = ok;
+      state_st<T>(gnout, gnout_lo, cb + ky, ok, true);
       buf[padi<P>(ky)] = mk((T)ok.x, (T)ok.y);
       if (kyp != ky) {
-        nout[kyp] = okp;
+        state_st<T>(gnout, gnout_lo, cb + kyp, okp, true);
         buf[padi<P>(kyp)] = mk((T)okp.x, (T)okp.y);
       }
     }

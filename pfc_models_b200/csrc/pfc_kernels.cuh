@@ -141,29 +141,83 @@ struct RowArgs {
   double g, min_phi, min_log, epsilon;
 };
 
-// The spectral state n_hat is FP64 in both precision forms and the update
-// n_hat' = n_hat + (A - 1) n_hat + Bg N_hat runs in FP64: slow modes (A near 1)
-// neither lose their increments to rounding of the state nor drift by a rounded A.
+// The spectral state and the update n_hat' = n_hat + (A - 1) n_hat + Bg N_hat.
+// FP64 form: n_hat is complex128 and (A - 1, Bg) FP64. FP32 form: n_hat is a complex64
+// "hi" array plus a complex64 "lo" array holding the rounding residual, and the update
+// runs in FP64; for the slow modes (|A - 1| < slow_tau, where rounding errors would
+// accumulate over many steps) it uses hi + lo and the FP64 coefficients, elsewhere hi and
+// the FP32 coefficients, whose rounding is damped within a few steps. lo stays 0 outside
+// the slow modes, so readers may always use hi + lo.
 template <class T>
 struct ColArgs {
   int nx, ny, m, cols, tpf, ld, nyh;
   FftDesc fft;
   const cplx<T>* tw;
-  const cplx<T>* in;        // V (step/init/combine)
-  const cplx<double>* sin;  // n_hat (parseval/export)
-  const cplx<double>* nin;  // n_hat (step/combine)
-  cplx<double>* nout;       // n_hat' (step/init)
-  cplx<T>* wout;            // W' (step/init/combine)
-  const cplx<double>* coef; // (A - 1, Bg) [kx][ky], kx <= m, ky <= ny/2, FP64
+  const cplx<T>* in;            // V (step/init/combine)
+  const void* sin;              // n_hat (parseval/export): complex128, or hi (FP32 form)
+  const cplx<float>* sin_lo;    //   its lo (FP32 form)
+  const void* nin;              // n_hat (step/combine)
+  const cplx<float>* nin_lo;
+  void* nout;                   // n_hat' (step/init)
+  cplx<float>* nout_lo;
+  cplx<T>* wout;                // W' (step/init/combine)
+  const cplx<T>* coef;          // (A - 1, Bg) [kx][ky], kx <= m, ky <= ny/2, working precision
+  const cplx<double>* coef64;   // FP32 form: the same in FP64, read for the slow modes
+  float slow_tau;
   double* partials;
-  double* out_c128;         // export: (ny, m+1) complex128
-  int dev_form;             // deviation form: keep the DC of column 0 at zero
-  int combine;              // kCombine*
-  double scale;             // 1 / (nx ny)
-  double fx, fy;            // 1/(nx dx), 1/(ny dy): k = 2 pi idx f
+  double* out_c128;             // export: (ny, m+1) complex128
+  int dev_form;                 // deviation form: keep the DC of column 0 at zero
+  int combine;                  // kCombine*
+  double scale;                 // 1 / (nx ny)
+  double fx, fy;                // 1/(nx dx), 1/(ny dy): k = 2 pi idx f
   double beta, q0, epsilon, w;  // L_mu, L_f, Gaussian width
-  const double* scal;       // device scalar block (export adds the deviation-form DC)
+  const double* scal;           // device scalar block (export adds the deviation-form DC)
 };
+
+// Element i of a spectral state (hi + lo in the FP32 form when with_lo).
+template <class T>
+__device__ __forceinline__ cplx<double> state_ld(const void* s, const cplx<float>* lo, size_t i, bool with_lo) {
+  if constexpr (sizeof(T) == 8) {
+    return static_cast<const cplx<double>*>(s)[i];
+  } else {
+    const cplx<float> h = static_cast<const cplx<float>*>(s)[i];
+    cplx<double> r = mk((double)h.x, (double)h.y);
+    if (with_lo) {
+      const cplx<float> l = lo[i];
+      r.x += (double)l.x;
+      r.y += (double)l.y;
+    }
+    return r;
+  }
+}
+
+// Stores element i of a spectral state (the FP32 form keeps the residual in lo when with_lo).
+template <class T>
+__device__ __forceinline__ void state_st(void* s, cplx<float>* lo, size_t i, cplx<double> v, bool with_lo) {
+  if constexpr (sizeof(T) == 8) {
+    static_cast<cplx<double>*>(s)[i] = v;
+  } else {
+    const cplx<float> h = mk((float)v.x, (float)v.y);
+    static_cast<cplx<float>*>(s)[i] = h;
+    if (with_lo) lo[i] = mk((float)(v.x - (double)h.x), (float)(v.y - (double)h.y));
+  }
+}
+
+// ETD coefficients (A - 1, Bg) of table entry ci in FP64; sets slow (always true in the
+// FP64 form, where the state carries no separate residual).
+template <class T>
+__device__ __forceinline__ cplx<double> coef_ld(const cplx<T>* c, const cplx<double>* c64, size_t ci, float tau,
+                                                bool force_slow, bool& slow) {
+  const cplx<T> v = c[ci];
+  if constexpr (sizeof(T) == 8) {
+    slow = true;
+    return v;
+  } else {
+    slow = force_slow || fabsf(v.x) < tau;
+    if (slow) return c64[ci];
+    return mk((double)v.x, (double)v.y);
+  }
+}
 
 // wavenumber^2 of packed-column entry (kx, ky), numpy rfftfreq/fftfreq convention
 __device__ __forceinline__ double ksq(int kx, int ky, int ny, double fx, double fy) {
@@ -345,12 +399,12 @@ __global__ void __launch_bounds__(LB) col_kernel(ColArgs<T> a) {
     // no transform: direct pass over n_hat
     KSum acc[1] = {{0.0, 0.0}};
     if (valid) {
-      const cplx<double>* col = a.sin + (size_t)kx * ny;
+      const size_t cb = (size_t)kx * ny;
       for (int ky = lt; ky < ny; ky += tpf) {
         const int kyp = ky == 0 ? 0 : ny - ky;
         if (kx == 0) {
           cplx<double> h0, hm;
-          unpack_pair(col[ky], col[kyp], h0, hm);
+          unpack_pair(state_ld<T>(a.sin, a.sin_lo, cb + ky, true), state_ld<T>(a.sin, a.sin_lo, cb + kyp, true), h0, hm);
           if (MODE == kColParseval) {
             const double k0 = ksq(0, ky, ny, a.fx, a.fy), kM = ksq(m, ky, ny, a.fx, a.fy);
             const double l0 = (a.beta / 2.0) * (a.q0 * a.q0 - k0) * (a.q0 * a.q0 - k0);
@@ -365,7 +419,7 @@ __global__ void __launch_bounds__(LB) col_kernel(ColArgs<T> a) {
             o[2 * m] = hm.x; o[2 * m + 1] = hm.y;
           }
         } else {
-          const cplx<double> v = col[ky];
+          const cplx<double> v = state_ld<T>(a.sin, a.sin_lo, cb + ky, true);
           if (MODE == kColParseval) {
             const double k2 = ksq(kx, ky, ny, a.fx, a.fy);
             const double l = (a.beta / 2.0) * (a.q0 * a.q0 - k2) * (a.q0 * a.q0 - k2);
@@ -396,26 +450,31 @@ __global__ void __launch_bounds__(LB) col_kernel(ColArgs<T> a) {
 
   if (MODE == kColInit) {
     if (valid) {
-      cplx<double>* out = a.nout + (size_t)kx * ny;
+      const size_t cb = (size_t)kx * ny;
       for (int ky = lt; ky < ny; ky += tpf) {
         cplx<T> v = buf[ky];
         if (a.dev_form && kx == 0 && ky == 0) { v.x = T(0); buf[0] = v; }
-        out[ky] = mk((double)v.x, (double)v.y);
+        state_st<T>(a.nout, a.nout_lo, cb + ky, mk((double)v.x, (double)v.y), true);   // lo = 0
       }
     }
     __syncthreads();
   } else if (MODE == kColStep) {
     if (valid) {
-      const cplx<double>* nin = a.nin + (size_t)kx * ny;
-      cplx<double>* nout = a.nout + (size_t)kx * ny;
+      const size_t cb = (size_t)kx * ny;
       for (int ky = lt; ky <= ny / 2; ky += tpf) {
         const int kyp = ky == 0 ? 0 : ny - ky;
         const cplx<T> qkt = buf[ky], qkpt = buf[kyp];
         const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
-        const cplx<double> pk = nin[ky], pkp = nin[kyp];
         cplx<double> ok, okp;
+        bool slow;
         if (kx == 0) {
-          const cplx<double> c0v = a.coef[ky], cMv = a.coef[(size_t)m * nyh + ky];
+          // the packed column holds kx = 0 (slow near ky = 0): always at full precision
+          bool s0, sM;
+          const cplx<double> c0v = coef_ld<T>(a.coef, a.coef64, ky, a.slow_tau, true, s0);
+          const cplx<double> cMv = coef_ld<T>(a.coef, a.coef64, (size_t)m * nyh + ky, a.slow_tau, true, sM);
+          slow = true;
+          const cplx<double> pk = state_ld<T>(a.nin, a.nin_lo, cb + ky, true);
+          const cplx<double> pkp = state_ld<T>(a.nin, a.nin_lo, cb + kyp, true);
           cplx<double> h0, hm, g0, gm;
           unpack_pair(pk, pkp, h0, hm);
           unpack_pair(qk, qkp, g0, gm);
@@ -424,20 +483,25 @@ __global__ void __launch_bounds__(LB) col_kernel(ColArgs<T> a) {
           ok = h0n + mul_i(hmn);
           okp = conj(h0n) + mul_i(conj(hmn));
         } else {
-          const cplx<double> c = a.coef[(size_t)kx * nyh + ky];
+          const cplx<double> c = coef_ld<T>(a.coef, a.coef64, (size_t)kx * nyh + ky, a.slow_tau, false, slow);
+          const cplx<double> pk = state_ld<T>(a.nin, a.nin_lo, cb + ky, slow);
+          const cplx<double> pkp = state_ld<T>(a.nin, a.nin_lo, cb + kyp, slow);
           ok = pk + c.x * pk + c.y * qk;
           okp = pkp + c.x * pkp + c.y * qkp;
         }
-        nout[ky] = ok;
+        state_st<T>(a.nout, a.nout_lo, cb + ky, ok, slow);
         buf[ky] = mk((T)ok.x, (T)ok.y);
-        if (kyp != ky) { nout[kyp] = okp; buf[kyp] = mk((T)okp.x, (T)okp.y); }
+        if (kyp != ky) {
+          state_st<T>(a.nout, a.nout_lo, cb + kyp, okp, slow);
+          buf[kyp] = mk((T)okp.x, (T)okp.y);
+        }
       }
     }
     __syncthreads();
   } else if (MODE == kColCombine) {
     // mu_hat = L_mu n_hat + N_hat (optionally Gaussian-filtered), or G n_hat, or N_hat
     if (valid) {
-      const cplx<double>* nin = a.nin + (size_t)kx * ny;
+      const size_t cb = (size_t)kx * ny;
       const double q2 = a.q0 * a.q0;
       for (int ky = lt; ky <= ny / 2; ky += tpf) {
         const int kyp = ky == 0 ? 0 : ny - ky;
@@ -456,7 +520,8 @@ __global__ void __launch_bounds__(LB) col_kernel(ColArgs<T> a) {
             default: mn[h] = 1.0; mq[h] = 0.0; break;
           }
         }
-        const cplx<double> pk = nin[ky], pkp = nin[kyp];
+        const cplx<double> pk = state_ld<T>(a.nin, a.nin_lo, cb + ky, true);
+        const cplx<double> pkp = state_ld<T>(a.nin, a.nin_lo, cb + kyp, true);
         cplx<double> qk = mk(0.0, 0.0), qkp = qk;
         if (need_v) {
           qk = mk((double)buf[ky].x, (double)buf[ky].y);

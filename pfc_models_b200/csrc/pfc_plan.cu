@@ -138,11 +138,13 @@ struct pfc_plan {
   size_t nspec = 0;     // m * ny complex elements per spectral array
   size_t elt = 0;       // bytes per complex element
   // device buffers
-  void* nhat[2] = {nullptr, nullptr};
+  void* nhat[2] = {nullptr, nullptr};     // complex128, or hi (complex64) in the FP32 form
+  void* nhat_lo[2] = {nullptr, nullptr};  // FP32 form: residuals of the slow modes
   void* W = nullptr;
   void* V = nullptr;
   void* W2 = nullptr;
-  void* coef = nullptr;
+  void* coef = nullptr;    // (A - 1, Bg), working precision
+  void* coef64 = nullptr;  // FP32 form: (A - 1, Bg) in FP64 for the slow modes
   void* tw = nullptr;
   double* partials = nullptr;
   size_t npartials = 0;
@@ -191,6 +193,11 @@ struct pfc_batch {
   long long launches = 0;
 };
 
+// FP32 form: modes with |A - 1| below this are "slow" and keep an FP64-accurate state
+// (hi + lo) and FP64 coefficients; the rounding of the others is damped by at least
+// this factor every step.
+constexpr float kSlowTau = 0.25f;
+
 namespace {
 
 template <class T>
@@ -216,7 +223,9 @@ ColArgs<T> col_args(const pfc_plan* h) {
   a.nyh = h->nyh;
   a.fft = h->colfft;
   a.tw = reinterpret_cast<const cplx<T>*>(h->tw);
-  a.coef = static_cast<const cplx<double>*>(h->coef);
+  a.coef = static_cast<const cplx<T>*>(h->coef);
+  a.coef64 = static_cast<const cplx<double>*>(h->coef64);
+  a.slow_tau = kSlowTau;
   a.dev_form = h->fp32 ? 1 : 0;
   a.scale = 1.0 / ((double)h->nx * (double)h->ny);
   const double dx = h->prob.lx / h->nx, dy = h->prob.ly / h->ny;
@@ -408,10 +417,14 @@ int launch_step_col(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
     a.batch = table;
     a.m = h->m; a.ny = h->ny; a.nyh = h->nyh;
     a.in = reinterpret_cast<const cplx<T>*>(h->V);
-    a.nin = reinterpret_cast<const cplx<double>*>(h->nhat[h->cur]);
-    a.nout = reinterpret_cast<cplx<double>*>(h->nhat[h->cur ^ 1]);
+    a.nin = h->nhat[h->cur];
+    a.nout = h->nhat[h->cur ^ 1];
+    a.nin_lo = static_cast<const cplx<float>*>(h->nhat_lo[h->cur]);
+    a.nout_lo = static_cast<cplx<float>*>(h->nhat_lo[h->cur ^ 1]);
+    a.coef64 = static_cast<const cplx<double>*>(h->coef64);
+    a.slow_tau = kSlowTau;
     a.wout = reinterpret_cast<cplx<T>*>(h->W);
-    a.coef = static_cast<const cplx<double>*>(h->coef);
+    a.coef = static_cast<const cplx<T>*>(h->coef);
     const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(h->tw);
     a.twA = tw + h->tw_ca; a.twB = tw + h->tw_cb;
     a.scale = (T)(1.0 / ((double)h->nx * (double)h->ny));
@@ -424,8 +437,10 @@ int launch_step_col(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
   ColArgs<T> ca = col_args<T>(h);
   ca.in = reinterpret_cast<const cplx<T>*>(h->V);
   ca.wout = reinterpret_cast<cplx<T>*>(h->W);
-  ca.nin = reinterpret_cast<const cplx<double>*>(h->nhat[h->cur]);
-  ca.nout = reinterpret_cast<cplx<double>*>(h->nhat[h->cur ^ 1]);
+  ca.nin = h->nhat[h->cur];
+  ca.nout = h->nhat[h->cur ^ 1];
+  ca.nin_lo = static_cast<const cplx<float>*>(h->nhat_lo[h->cur]);
+  ca.nout_lo = static_cast<cplx<float>*>(h->nhat_lo[h->cur ^ 1]);
   return launch_col<T, kColStep>(h, ca, s);
 }
 
@@ -449,7 +464,8 @@ int do_set_state(pfc_plan* h, const double* field, cudaStream_t s) {
   if (rc) return rc;
   ColArgs<T> ca = col_args<T>(h);
   ca.in = reinterpret_cast<const cplx<T>*>(h->V);
-  ca.nout = reinterpret_cast<cplx<double>*>(h->nhat[h->cur]);
+  ca.nout = h->nhat[h->cur];
+  ca.nout_lo = static_cast<cplx<float>*>(h->nhat_lo[h->cur]);
   ca.wout = reinterpret_cast<cplx<T>*>(h->W);
   rc = launch_col<T, kColInit>(h, ca, s);
   if (rc) return rc;
@@ -659,7 +675,8 @@ int do_reduce(pfc_plan* h, double* out3, cudaStream_t s) {
   int rc = launch_row<T, kRowReduce>(h, ra, s);
   if (rc) return rc;
   ColArgs<T> ca = col_args<T>(h);
-  ca.sin = reinterpret_cast<const cplx<double>*>(h->nhat[h->cur]);
+  ca.sin = h->nhat[h->cur];
+  ca.sin_lo = static_cast<const cplx<float>*>(h->nhat_lo[h->cur]);
   ca.partials = colp;
   rc = launch_col<T, kColParseval>(h, ca, s);
   if (rc) return rc;
@@ -671,11 +688,11 @@ int do_reduce(pfc_plan* h, double* out3, cudaStream_t s) {
   return PFC_OK;
 }
 
-// Nonlinear row spectra V of the "previous" state, and that state's n_hat.
+// Nonlinear row spectra V of the "previous" state, and the index of that state's n_hat.
 template <class T>
-int prepare_previous(pfc_plan* h, bool current, const void** nhat_old, cudaStream_t s) {
+int prepare_previous(pfc_plan* h, bool current, int* old_buf, cudaStream_t s) {
   if (h->steps_since_set > 0 && !current) {
-    *nhat_old = h->nhat[h->cur ^ 1];
+    *old_buf = h->cur ^ 1;
     return PFC_OK;
   }
   RowArgs<T> ra = row_args<T>(h);
@@ -683,7 +700,7 @@ int prepare_previous(pfc_plan* h, bool current, const void** nhat_old, cudaStrea
   ra.out = reinterpret_cast<cplx<T>*>(h->V);
   int rc = launch_row<T, kRowStep>(h, ra, s);
   if (rc) return rc;
-  *nhat_old = h->nhat[h->cur];
+  *old_buf = h->cur;
   return PFC_OK;
 }
 
@@ -695,12 +712,13 @@ int do_get_field(pfc_plan* h, int which, double w, double* out, cudaStream_t s) 
   if (!h->W2) {
     PFC_CUDA(cudaMalloc(&h->W2, h->nspec * h->elt));
   }
-  const void* nold = nullptr;
-  int rc = prepare_previous<T>(h, current, &nold, s);
+  int old_buf = 0;
+  int rc = prepare_previous<T>(h, current, &old_buf, s);
   if (rc) return rc;
   ColArgs<T> ca = col_args<T>(h);
   ca.in = reinterpret_cast<const cplx<T>*>(h->V);
-  ca.nin = reinterpret_cast<const cplx<double>*>(nold);
+  ca.nin = h->nhat[old_buf];
+  ca.nin_lo = static_cast<const cplx<float>*>(h->nhat_lo[old_buf]);
   ca.wout = reinterpret_cast<cplx<T>*>(h->W2);
   ca.w = w;
   int addslot = kScalZero;
@@ -718,10 +736,11 @@ int do_get_field(pfc_plan* h, int which, double w, double* out, cudaStream_t s) 
 
 template <class T>
 int do_get_spectrum(pfc_plan* h, int which, double* out, cudaStream_t s) {
-  const void* src = h->nhat[h->cur];
-  if (which == PFC_SPEC_N_HAT && h->steps_since_set > 0) src = h->nhat[h->cur ^ 1];
+  int buf = h->cur;
+  if (which == PFC_SPEC_N_HAT && h->steps_since_set > 0) buf = h->cur ^ 1;
   ColArgs<T> ca = col_args<T>(h);
-  ca.sin = reinterpret_cast<const cplx<double>*>(src);
+  ca.sin = h->nhat[buf];
+  ca.sin_lo = static_cast<const cplx<float>*>(h->nhat_lo[buf]);
   ca.out_c128 = out;
   int rc = launch_col<T, kColExport>(h, ca, s);
   if (rc) return rc;
@@ -868,13 +887,16 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
 
   // ---- device buffers
   const size_t specb = h->nspec * h->elt;
-  // the spectral state is FP64 in both forms
-  const size_t stateb = h->nspec * sizeof(double2);
+  // the spectral state: complex128 (FP64 form), or hi + lo complex64 arrays (FP32 form)
+  const size_t stateb = h->nspec * (h->fp32 ? sizeof(float2) : sizeof(double2));
+  const size_t ncoef = (size_t)(m + 1) * h->nyh;
   cudaError_t e = cudaSuccess;
   for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMalloc(&h->nhat[i], stateb);
+  for (int i = 0; i < 2 && e == cudaSuccess && h->fp32; ++i) e = cudaMalloc(&h->nhat_lo[i], stateb);
+  if (e == cudaSuccess && h->fp32) e = cudaMalloc(&h->coef64, ncoef * sizeof(double2));
   if (e == cudaSuccess) e = cudaMalloc(&h->W, specb);
   if (e == cudaSuccess) e = cudaMalloc(&h->V, specb);
-  if (e == cudaSuccess) e = cudaMalloc(&h->coef, (size_t)(m + 1) * h->nyh * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc(&h->coef, ncoef * h->elt);
   if (e == cudaSuccess) e = cudaMalloc(&h->tw, tw.size() / 2 * h->elt);
   h->npartials = 6 * (size_t)h->row_grid + 2 * (size_t)h->col_grid + 2 * 1024;
   if (e == cudaSuccess) e = cudaMalloc(&h->partials, h->npartials * sizeof(double));
@@ -894,14 +916,23 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
       else { double2 v = make_double2((double)tw[2 * i], (double)tw[2 * i + 1]); memcpy(&host[i * 16], &v, 16); }
     }
     e = cudaMemcpy(h->tw, host.data(), host.size(), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess)
+    if (h->fp32) {
+      std::vector<float2> c32(ncoef);
+      for (size_t i = 0; i < ncoef; ++i) c32[i] = make_float2((float)coefA[2 * i], (float)coefA[2 * i + 1]);
+      if (e == cudaSuccess) e = cudaMemcpy(h->coef, c32.data(), ncoef * sizeof(float2), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess)
+        e = cudaMemcpy(h->coef64, coefA.data(), coefA.size() * sizeof(double), cudaMemcpyHostToDevice);
+    } else if (e == cudaSuccess) {
       e = cudaMemcpy(h->coef, coefA.data(), coefA.size() * sizeof(double), cudaMemcpyHostToDevice);
+    }
     std::vector<double> sc(kScalCount, 0.0);
     if (e == cudaSuccess) e = cudaMemcpy(h->scal, sc.data(), sc.size() * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(h->status, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->W, 0, specb);
-    if (e == cudaSuccess) e = cudaMemset(h->nhat[0], 0, stateb);
-    if (e == cudaSuccess) e = cudaMemset(h->nhat[1], 0, stateb);
+    for (int i = 0; i < 2; ++i) {
+      if (e == cudaSuccess) e = cudaMemset(h->nhat[i], 0, stateb);
+      if (e == cudaSuccess && h->nhat_lo[i]) e = cudaMemset(h->nhat_lo[i], 0, stateb);
+    }
     if (e != cudaSuccess)
       return cleanup_fail(fail(PFC_E_CUDA, "pfc_plan_create: upload failed: %s", cudaGetErrorString(e)));
   }
@@ -915,7 +946,7 @@ int pfc_plan_destroy(pfc_plan* h) {
   if (!h) return PFC_OK;
   for (auto& g : h->graph)
     if (g) cudaGraphExecDestroy(g);
-  for (void* p : {h->nhat[0], h->nhat[1], h->W, h->V, h->W2, h->coef, h->tw})
+  for (void* p : {h->nhat[0], h->nhat[1], h->nhat_lo[0], h->nhat_lo[1], h->W, h->V, h->W2, h->coef, h->coef64, h->tw})
     if (p) cudaFree(p);
   if (h->partials) cudaFree(h->partials);
   if (h->scal) cudaFree(h->scal);
@@ -1074,7 +1105,10 @@ int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out) {
         host[i].v = h->V;
         host[i].nin = h->nhat[p];
         host[i].nout = h->nhat[p ^ 1];
+        host[i].nin_lo = h->nhat_lo[p];
+        host[i].nout_lo = h->nhat_lo[p ^ 1];
         host[i].coef = h->coef;
+        host[i].coef64 = h->coef64;
         host[i].scal = h->scal;
       }
       cudaError_t e = cudaMalloc(&c.table[p], n * sizeof(BatchBufs));
