@@ -142,7 +142,7 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
 #define PFC_FLAG_GENERIC_ONLY 1   /* do not use the power-of-two step kernels */
 #define PFC_FLAG_NO_GRAPHS 2      /* pfc_step launches every kernel directly */
 /* Variant of the power-of-two step kernels (0 in a field = the precision's default):
- * complex values per thread of the row and of the column kernel (FP32: 16 or 32,
+ * complex values per thread of the row and of the column kernel (FP32: 8, 16 or 32,
  * default 32; FP64: 8 or 16, default 16) and rows per CTA of the row kernel
  * (1, 2, 4, 8 or 16). Other values make pfc_plan_create return PFC_E_ARG. The
  * autotuner (pfc_models_b200/tune.py) measures these per grid and caches the best. */

@@ -299,11 +299,14 @@ int ilog2_exact(int n) {
 
 // Elements per thread of the step kernels built for each precision (the first is the default).
 template <class T> constexpr int fast_ee_default() { return sizeof(T) == 4 ? 32 : 16; }
-template <class T> bool fast_ee_valid(int ee) { return sizeof(T) == 4 ? (ee == 16 || ee == 32) : (ee == 8 || ee == 16); }
+template <class T> bool fast_ee_valid(int ee) {
+  return sizeof(T) == 4 ? (ee == 8 || ee == 16 || ee == 32) : (ee == 8 || ee == 16);
+}
 
 template <class T>
 bool fast_lookup(bool col, int lg, int ee, int model, FastKernel* k) {
   if (sizeof(T) == 4) {
+    if (ee == 8) return col ? FastInst<float, 8>::col(lg, k) : FastInst<float, 8>::row(lg, model, k);
     if (ee == 16) return col ? FastInst<float, 16>::col(lg, k) : FastInst<float, 16>::row(lg, model, k);
     return col ? FastInst<float, 32>::col(lg, k) : FastInst<float, 32>::row(lg, model, k);
   }
@@ -313,7 +316,10 @@ bool fast_lookup(bool col, int lg, int ee, int model, FastKernel* k) {
 
 template <class T>
 bool fast_seq_tables(int lg, int ee, std::vector<long double>& tw, int& a, int& b) {
-  if (sizeof(T) == 4) return ee == 16 ? FastInst<float, 16>::tables(lg, tw, a, b) : FastInst<float, 32>::tables(lg, tw, a, b);
+  if (sizeof(T) == 4) {
+    if (ee == 8) return FastInst<float, 8>::tables(lg, tw, a, b);
+    return ee == 16 ? FastInst<float, 16>::tables(lg, tw, a, b) : FastInst<float, 32>::tables(lg, tw, a, b);
+  }
   return ee == 8 ? FastInst<double, 8>::tables(lg, tw, a, b) : FastInst<double, 16>::tables(lg, tw, a, b);
 }
 
@@ -327,7 +333,7 @@ int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
   const int tile = PFC_FLAG_ROW_TILE_OF(flags);
   if (!fast_ee_valid<T>(ee_r) || !fast_ee_valid<T>(ee_c))
     return fail(PFC_E_ARG, "pfc_plan_create: elements per thread (%d, %d) not built for this precision "
-                "(FP32: 16 or 32, FP64: 8 or 16)", ee_r, ee_c);
+                "(FP32: 8, 16 or 32; FP64: 8 or 16)", ee_r, ee_c);
   if (tile && (tile > 16 || (tile & (tile - 1))))
     return fail(PFC_E_ARG, "pfc_plan_create: row tile %d is not a power of two <= 16", tile);
   const int lm = ilog2_exact(h->m), ly = ilog2_exact(h->ny);

@@ -24,7 +24,7 @@ from . import _lib
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PACKAGED = os.path.join(HERE, "tuned_b200.json")
-EE_CHOICES = {_lib.FP32_MIXED: (16, 32), _lib.FP64_PLAIN: (8, 16)}
+EE_CHOICES = {_lib.FP32_MIXED: (8, 16, 32), _lib.FP64_PLAIN: (8, 16)}
 TILE_CHOICES = (1, 2, 4, 8, 16)
 _lock = threading.Lock()
 _memo: dict = {}

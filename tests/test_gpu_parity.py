@@ -400,7 +400,7 @@ def test_kernel_variants_match_generic(nx, ny, precision):
     gen.State.n[...] = f0
     gen.TimeSteps(8)
     ref = gen.State.n.get()
-    ees = (16, 32) if precision == "fp32" else (8, 16)
+    ees = (8, 16, 32) if precision == "fp32" else (8, 16)
     tol = 1e-13 if precision == "fp64" else 1e-5
     for ee_r in ees:
         for ee_c in ees:
@@ -419,7 +419,7 @@ def test_kernel_variant_errors():
     from pfc_models_b200 import _lib
     prm = stdpfc.BuildStdPFCModelParameters(epsilon=-0.3, g=0.0, dt=0.5)
     geom = stdpfc.Build2DGeometry(128, 128, 32 * np.pi, 32 * np.pi)
-    for bad in ({"ee_row": 8}, {"ee_col": 64}, {"row_tile": 3}):
+    for bad in ({"ee_row": 4}, {"ee_col": 64}, {"row_tile": 3}):
         with pytest.raises(_lib.PfcError) as e:
             stdpfc.BuildB200_Simulation(prm, geom, precision="fp32", kernels=bad)
         assert e.value.code == _lib.PFC_E_ARG
