@@ -209,8 +209,9 @@ def coexistence(results, min_points=3, extend=0.5):
     """Per r: liquid-solid coexistence densities from the common tangent between the
     analytic liquid and the solid run (F and mu per site, cubic Hermite), or NaN.
     The solid branch may be continued `extend` density spacings below its lowest
-    point (crystals just below the coexistence density can melt within the run);
-    tangents further out are not reported."""
+    point (crystals just below the coexistence density can melt within the run) when
+    its first two points are neighbours on the density grid; tangents further out are
+    not reported."""
     from . import tangent
     out = []
     for r in sorted({d["r"] for d in results}):
@@ -220,11 +221,19 @@ def coexistence(results, min_points=3, extend=0.5):
                "mu": float("nan")}
         if len(sol) >= min_points:
             try:
-                h = sol[1]["mean"] - sol[0]["mean"]
+                # continue below the lowest point only on a first interval between neighbouring
+                # points of the density grid (the Hermite cubic there uses just those two)
+                gaps = np.diff([d["mean"] for d in sol])
+                h = float(np.min(gaps))
+                ext = extend * h if gaps[0] <= 1.5 * h else 0.0
                 br = tangent.tabulated_branch("solid", [d["mean"] for d in sol], [d["F"] for d in sol], min_points,
-                                              mu=[d["mu"] for d in sol], extend_lo=extend * h)
+                                              mu=[d["mu"] for d in sol], extend_lo=ext)
                 t = tangent.common_tangent(tangent.std_liquid_branch(r, -1.0, 0.5), br)
-                if t.ok:
+                # report it only where the solid branch at psi_s rests on two neighbouring
+                # grid points (a cubic across a gap is too loose a fit)
+                means = np.array([d["mean"] for d in sol])
+                j = int(np.clip(np.searchsorted(means, t.phi_b) - 1, 0, len(means) - 2)) if t.ok else 0
+                if t.ok and means[j + 1] - means[j] <= 1.5 * h:
                     row.update(psi_l=t.phi_a, psi_s=t.phi_b, mu=t.mu)
             except ValueError:
                 pass
