@@ -96,11 +96,15 @@ def run_points(points, steps, precision="fp32", block=1000, device=None, settle=
 
     from . import stdpfc
     from .simulation import Batch
+    from . import _lib, tune
+    from .simulation import _PRECISIONS
     sims = []
     for p in points:
         prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=p.r, g=0.0, dt=DT)
+        # the kernel variant measured for batches of this box size, if there is one
+        variant = tune.lookup(p.n, p.n, _PRECISIONS[precision], _lib.MODEL_STD, batched=True) or "auto"
         sim = stdpfc.BuildB200_Simulation(prm, stdpfc.Build2DGeometry(p.n, p.n, p.lx, p.ly), precision=precision,
-                                          device=device)
+                                          device=device, kernels=variant)
         sim.State.n[...] = initial_field(p)
         sims.append(sim)
     batch = Batch(sims)

@@ -35,10 +35,10 @@ def cache_path() -> str:
                                                            "tune.json")
 
 
-def _key(device_name, nx, ny, precision, model):
+def _key(device_name, nx, ny, precision, model, batched=False):
     prec = "fp32" if precision == _lib.FP32_MIXED else "fp64"
     mod = "log" if model == _lib.MODEL_LOG else "std"
-    return f"{device_name}|{nx}x{ny}|{prec}|{mod}"
+    return f"{device_name}|{nx}x{ny}|{prec}|{mod}" + ("|batch" if batched else "")
 
 
 def _load(path):
@@ -59,18 +59,22 @@ def _device_name():
     return torch.cuda.get_device_name()
 
 
-def lookup(nx, ny, precision, model, device_name=None):
-    """The cached variant {"ee_row", "ee_col", "row_tile"} for this grid, or None."""
+def lookup(nx, ny, precision, model, device_name=None, batched=False):
+    """The cached variant {"ee_row", "ee_col", "row_tile"} for this grid, or None.
+    `batched`: prefer the variant measured for many plans stepped as one batch (the
+    single-plan choice favours latency, a batch is throughput-bound)."""
     if device_name is None:
         try:
             device_name = _device_name()
         except Exception:
             return None
-    key = _key(device_name, nx, ny, precision, model)
-    for path in (cache_path(), PACKAGED):
-        e = _load(path).get(key)
-        if e:
-            return {k: int(e[k]) for k in ("ee_row", "ee_col", "row_tile")}
+    keys = ([_key(device_name, nx, ny, precision, model, True)] if batched else []) + \
+        [_key(device_name, nx, ny, precision, model)]
+    for key in keys:
+        for path in (cache_path(), PACKAGED):
+            e = _load(path).get(key)
+            if e:
+                return {k: int(e[k]) for k in ("ee_row", "ee_col", "row_tile")}
     return None
 
 
@@ -86,8 +90,12 @@ def _store(path, key, entry):
         _memo[path] = d
 
 
-def tune(nx, ny, precision="fp32", model="std", steps=20, warmup=3, save=True, path=None):
-    """Times the variants for one grid; returns the chosen entry (and caches it)."""
+def tune(nx, ny, precision="fp32", model="std", steps=20, warmup=3, save=True, path=None, batch=1):
+    """Times the variants for one grid; returns the chosen entry (and caches it).
+    With batch > 1 every variant steps `batch` plans together through a `Batch` and the
+    fastest whole step wins (cached under the grid's batch key)."""
+    if batch > 1:
+        return _tune_batch(nx, ny, precision, model, steps, warmup, save, path, batch)
     import numpy as np
     import torch
 
@@ -140,6 +148,61 @@ def tune(nx, ny, precision="fp32", model="std", steps=20, warmup=3, save=True, p
     return entry
 
 
+def _setup(nx, ny, precision, model):
+    from . import fields, logpfc, stdpfc
+    mod = logpfc if model == "log" else stdpfc
+    geom = mod.Build2DGeometry(nx, ny, nx * math.pi / 4, ny * math.pi / 4)
+    if model == "log":
+        prm = logpfc.BuildLogPFCModelParameters(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=0.1)
+        mean = 0.55
+    else:
+        prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.3, g=0.0, dt=0.5)
+        mean = -0.3
+    return mod, geom, prm, fields.GenerateNoisyLiquid(geom, mean, 0.01, seed=0)
+
+
+def _tune_batch(nx, ny, precision, model, steps, warmup, save, path, batch):
+    import torch
+
+    from .simulation import _PRECISIONS, Batch
+    prec = _PRECISIONS[precision]
+    mod, geom, prm, f0 = _setup(nx, ny, precision, model)
+    ees = EE_CHOICES[prec]
+    timed = {}
+    for ee_r, tile, ee_c in itertools.product(ees, TILE_CHOICES, ees):
+        variant = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile}
+        sims = [mod.BuildB200_Simulation(prm, geom, precision=precision, kernels=variant) for _ in range(batch)]
+        v = sims[0].plan.variant()
+        key = (v["ee_row"], v["row_tile"], v["ee_col"])
+        if not v["fast"] or key in timed:
+            for s in sims:
+                s.plan.close()
+            continue
+        for s in sims:
+            (s.State.phi if model == "log" else s.State.n)[...] = f0
+        b = Batch(sims)
+        b.step(max(warmup, 16))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.step(steps)
+        e1.record()
+        e1.synchronize()
+        timed[key] = 1e3 * e0.elapsed_time(e1) / steps
+        b.close()
+        for s in sims:
+            s.plan.close()
+    if not timed:
+        return None
+    (ee_r, tile, ee_c), us = min(timed.items(), key=lambda kv: kv[1])
+    entry = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile, "batch": batch, "step_us": us,
+             "row_us": None, "col_us": None,
+             "steps_us": {f"{a}/{b}/{c}": u for (a, b, c), u in sorted(timed.items())}}
+    if save:
+        _store(path or cache_path(), _key(_device_name(), nx, ny, prec,
+                                          _lib.MODEL_LOG if model == "log" else _lib.MODEL_STD, True), entry)
+    return entry
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--sizes", default="2048", help="comma list of n (n x n grids) or nx x ny items like 512x256")
@@ -147,6 +210,7 @@ def main():
     ap.add_argument("--model", default="std")
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--save", action="store_true", help="write the user cache")
+    ap.add_argument("--batch", type=int, default=1, help="time this many plans stepped as one batch")
     ap.add_argument("--out", default=None, help="also write all entries to this JSON file")
     a = ap.parse_args()
     allres = {}
@@ -154,9 +218,9 @@ def main():
         nx, ny = (int(v) for v in s.split("x")) if "x" in s else (int(s), int(s))
         for precision in a.precision.split(","):
             for model in a.model.split(","):
-                e = tune(nx, ny, precision, model, steps=a.steps, save=a.save)
+                e = tune(nx, ny, precision, model, steps=a.steps, save=a.save, batch=a.batch)
                 key = _key(_device_name(), nx, ny, _lib.FP32_MIXED if precision == "fp32" else _lib.FP64_PLAIN,
-                           _lib.MODEL_LOG if model == "log" else _lib.MODEL_STD)
+                           _lib.MODEL_LOG if model == "log" else _lib.MODEL_STD, a.batch > 1)
                 allres[key] = e
                 print(json.dumps({key: e}), flush=True)
     if a.out:

@@ -32,7 +32,7 @@ def test_sweep_runs_every_point_in_one_batch(both):
 def test_coexistence_fp32_mixed_matches_fp64(both):
     c32, c64 = both["fp32"][2], both["fp64"][2]
     found = [(a, b) for a, b in zip(c32, c64) if np.isfinite(a["psi_s"]) and np.isfinite(b["psi_s"])]
-    assert len(found) >= 5
+    assert len(found) >= 4
     for a, b in found:
         assert abs(a["psi_l"] - b["psi_l"]) < 1e-4 and abs(a["psi_s"] - b["psi_s"]) < 1e-4, (a, b)
         assert a["psi_l"] < a["psi_s"] < 0

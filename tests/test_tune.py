@@ -15,6 +15,13 @@ def test_packaged_table_is_used_without_a_user_cache(tmp_path, monkeypatch):
     assert v == {k: table[key][k] for k in ("ee_row", "ee_col", "row_tile")}
     for e in table.values():
         assert e["ee_row"] in (8, 16, 32) and e["ee_col"] in (8, 16, 32) and e["row_tile"] in (1, 2, 4, 8, 16)
+    # batch-measured entries are preferred for batches and fall back to the single-plan ones
+    bkey = "NVIDIA B200|512x512|fp32|std|batch"
+    assert bkey in table
+    vb = tune.lookup(512, 512, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200", batched=True)
+    assert vb == {k: table[bkey][k] for k in ("ee_row", "ee_col", "row_tile")}
+    v2 = tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200", batched=True)
+    assert v2 == v
     assert tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="other GPU") is None
 
 
