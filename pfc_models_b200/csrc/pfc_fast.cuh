@@ -480,6 +480,19 @@ col_step_fast(FastColArgs<T> a) {
 #pragma unroll 8
     for (int ky = t; ky < NY; ky += TPF) {
       const int kh = ky <= NY / 2 ? ky : NY - ky;
+      if constexpr (sizeof(T) == 4) {
+        // fast modes (|A - 1| >= tau): the update in FP32 on hi alone; their rounding
+        // errors are damped by at least tau every step
+        const cplx<T> cw = gcoef[ccb + kh];
+        if (fabsf(cw.x) >= tau) {
+          const cplx<float> p = static_cast<const cplx<float>*>(gnin)[cb + ky];
+          const cplx<float> gv = buf[padi<P>(ky)];
+          const cplx<float> o = mk(fmaf(cw.x, p.x, p.x) + cw.y * gv.x, fmaf(cw.x, p.y, p.y) + cw.y * gv.y);
+          static_cast<cplx<float>*>(gnout)[cb + ky] = o;
+          buf[padi<P>(ky)] = o;
+          continue;
+        }
+      }
       bool slow;
       const cplx<double> c = coef_ld<T>(gcoef, gcoef64, ccb + kh, tau, false, slow);
       const cplx<double> p = state_ld<T>(gnin, gnin_lo, cb + ky, slow);
