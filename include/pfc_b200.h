@@ -99,9 +99,9 @@ int pfc_get_state(pfc_plan* plan, double* dev_field, void* stream);
 
 /* Replaces `for _ in range(nsteps): sim.TimeStep()` (models/stdpfc/simulation.py:225-235,
  * models/logpfc/simulation.py:220-230). Stream-ordered, no host synchronisation.
- * Whole blocks of 16 steps are replayed from a CUDA graph that the plan records
- * the first time it needs one (once per starting ping-pong parity; not with
- * PFC_FLAG_NO_GRAPHS); the remaining steps are launched directly. */
+ * Whole blocks of 16 steps, and the remaining single steps, are replayed from CUDA
+ * graphs that the plan records the first time it needs each (once per starting
+ * ping-pong parity; with PFC_FLAG_NO_GRAPHS every kernel is launched directly). */
 int pfc_step(pfc_plan* plan, int64_t nsteps, void* stream);
 
 /* pfc_step with instrumentation: also returns the summed device time (ms) of

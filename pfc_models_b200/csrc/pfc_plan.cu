@@ -171,8 +171,9 @@ struct pfc_plan {
   size_t fr_smem = 0, fc_smem = 0;
   int tw_ra = 0, tw_rb = 0, tw_ca = 0, tw_cb = 0;  // table offsets (complex elements)
   double lmu0 = 0, lf0 = 0;
-  // CUDA graphs of kGraphBlock steps, one per starting ping-pong parity
+  // CUDA graphs of kGraphBlock steps and of one step, one per starting ping-pong parity
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t graph1[2] = {nullptr, nullptr};
 };
 
 // A batch of plans stepped in lockstep: plans with the same step kernels, sizes and
@@ -519,30 +520,45 @@ int step_direct(pfc_plan* h, long long nsteps, cudaStream_t s) {
   return PFC_OK;
 }
 
-// Whole blocks of kGraphBlock steps replay a graph captured once per starting
-// parity; the remainder is launched directly.
+// Replays `count` times a graph of `len` steps that starts at the current parity
+// (captured on first use) and updates cur and the counters as direct stepping would.
+// A graph of odd length flips the parity, so it is replayed once per call (count = 1).
+template <class T>
+int replay_steps(pfc_plan* h, cudaGraphExec_t* slot, int len, long long count, cudaStream_t s) {
+  const int p = h->cur;
+  if (!slot[p]) {
+    const long long launches = h->launches, since = h->steps_since_set;
+    int rc = capture_graph([&](cudaStream_t cs) { return step_direct<T>(h, len, cs); }, &slot[p]);
+    h->launches = launches;
+    h->steps_since_set = since;
+    h->cur = p;
+    if (rc) return rc;
+  }
+  for (long long b = 0; b < count; ++b) {
+    cudaError_t e = cudaGraphLaunch(slot[p], s);
+    if (e != cudaSuccess) return fail(PFC_E_CUDA, "cudaGraphLaunch failed: %s", cudaGetErrorString(e));
+  }
+  h->launches += 2LL * len * count;
+  h->steps_since_set += (long long)len * count;
+  if ((len * count) & 1) h->cur ^= 1;
+  return PFC_OK;
+}
+
+// Whole blocks of kGraphBlock steps and the remaining single steps replay graphs captured
+// once per starting parity (smaller gaps between the kernels than direct launches).
 template <class T>
 int do_step(pfc_plan* h, long long nsteps, cudaStream_t s) {
-  const bool graphs = !(h->prob.flags & PFC_FLAG_NO_GRAPHS);
-  const long long blocks = graphs ? nsteps / kGraphBlock : 0;
+  if (h->prob.flags & PFC_FLAG_NO_GRAPHS) return step_direct<T>(h, nsteps, s);
+  const long long blocks = nsteps / kGraphBlock;
   if (blocks > 0) {
-    const int p = h->cur;
-    if (!h->graph[p]) {
-      const long long launches = h->launches, since = h->steps_since_set;
-      int rc = capture_graph([&](cudaStream_t cs) { return step_direct<T>(h, kGraphBlock, cs); }, &h->graph[p]);
-      h->launches = launches;
-      h->steps_since_set = since;
-      h->cur = p;
-      if (rc) return rc;
-    }
-    for (long long b = 0; b < blocks; ++b) {
-      cudaError_t e = cudaGraphLaunch(h->graph[p], s);
-      if (e != cudaSuccess) return fail(PFC_E_CUDA, "cudaGraphLaunch failed: %s", cudaGetErrorString(e));
-    }
-    h->launches += 2 * kGraphBlock * blocks;
-    h->steps_since_set += kGraphBlock * blocks;
+    int rc = replay_steps<T>(h, h->graph, kGraphBlock, blocks, s);
+    if (rc) return rc;
   }
-  return step_direct<T>(h, nsteps - blocks * kGraphBlock, s);
+  for (long long i = blocks * kGraphBlock; i < nsteps; ++i) {
+    int rc = replay_steps<T>(h, h->graph1, 1, 1, s);
+    if (rc) return rc;
+  }
+  return PFC_OK;
 }
 
 // ---- batches
@@ -951,6 +967,8 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
 int pfc_plan_destroy(pfc_plan* h) {
   if (!h) return PFC_OK;
   for (auto& g : h->graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto& g : h->graph1)
     if (g) cudaGraphExecDestroy(g);
   for (void* p : {h->nhat[0], h->nhat[1], h->nhat_lo[0], h->nhat_lo[1], h->W, h->V, h->W2, h->coef, h->coef64, h->tw})
     if (p) cudaFree(p);
