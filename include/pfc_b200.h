@@ -141,6 +141,9 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
 /* problem.flags bits */
 #define PFC_FLAG_GENERIC_ONLY 1   /* do not use the power-of-two step kernels */
 #define PFC_FLAG_NO_GRAPHS 2      /* pfc_step launches every kernel directly */
+#define PFC_FLAG_PDL 4            /* launch the power-of-two step kernels with programmatic
+                                     dependent launch: each may start (and send its column's
+                                     state towards L2) while the kernel before it drains */
 /* Variant of the power-of-two step kernels (0 in a field = the precision's default):
  * complex values per thread of the row and of the column kernel (FP32: 8, 16 or 32,
  * default 32; FP64: 8 or 16, default 16) and rows per CTA of the row kernel
@@ -149,9 +152,13 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
 #define PFC_FLAG_ROW_EE(e) ((int32_t)(e) << 8)
 #define PFC_FLAG_COL_EE(e) ((int32_t)(e) << 16)
 #define PFC_FLAG_ROW_TILE(r) ((int32_t)(r) << 24)
+/* columns per CTA of the column kernel: 1, 2 or 4, at most as many as fill 256 threads
+ * (0 = that many) */
+#define PFC_FLAG_COL_CTA(c) ((int32_t)((c) == 4 ? 3 : (c) == 2 ? 2 : (c) == 1 ? 1 : 0) << 29)
 #define PFC_FLAG_ROW_EE_OF(f) (((f) >> 8) & 0xff)
 #define PFC_FLAG_COL_EE_OF(f) (((f) >> 16) & 0xff)
 #define PFC_FLAG_ROW_TILE_OF(f) (((f) >> 24) & 0x1f)
+#define PFC_FLAG_COL_CTA_OF(f) ((((f) >> 29) & 3) ? 1 << ((((f) >> 29) & 3) - 1) : 0)
 
 /* The variant a plan uses: out4 = {row values per thread, column values per thread,
  * row tile rows, 1 if the power-of-two step kernels are used} (zeros when not). */

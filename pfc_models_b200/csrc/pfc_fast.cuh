@@ -215,6 +215,16 @@ __device__ __forceinline__ void l2_prefetch_range(const void* p, unsigned bytes,
   }
 }
 
+// Programmatic dependent launch. A step kernel launched with programmatic stream
+// serialisation may start while the kernel before it in the stream is still running:
+// pdl_wait() returns once that kernel has completed and its writes are visible (at
+// once for a kernel launched without the attribute). Each step kernel calls
+// pdl_trigger() right after pdl_wait(), so the code a kernel runs before its own
+// pdl_wait() starts only after the kernel two launches back has completed; that code
+// reads only buffers written two or more launches back and writes nothing.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 template <int TPF> struct FastBound { static constexpr int value = TPF > 256 ? TPF : 256; };
 // minimum resident CTAs per SM requested from the register allocator (256-thread CTAs)
 // from the registers the values held take (2 per real): with up to 32 of them the
@@ -252,6 +262,10 @@ row_step_fast(FastRowArgs<T> a) {
     gout = static_cast<cplx<T>*>(b.v);
     scal = b.scal;
   }
+
+  // W is the previous column pass's output
+  pdl_wait();
+  pdl_trigger();
 
   // ---- transposing tile load: element (kx, y0 + r) -> sm[r * ld + pad(kx)], issued as
   // asynchronous global->shared copies so that every load of the tile is in flight at once.
@@ -439,6 +453,11 @@ col_step_fast(FastColArgs<T> a) {
     const uintptr_t c1 = (reinterpret_cast<uintptr_t>(gcoef + (size_t)(kx + 1) * nyh) + 15) & ~(uintptr_t)15;
     l2_prefetch_range(reinterpret_cast<const void*>(c0), (unsigned)(c1 - c0), t, TPF);
   }
+
+  // V is the row pass's output (n_hat and the coefficients above were written two or
+  // more launches back)
+  pdl_wait();
+  pdl_trigger();
 
   // ---- forward sequence A; pass 0 reads the column of V from HBM
   {

@@ -363,7 +363,9 @@ int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
   while (ld % slots != want) ++ld;
   // column kernel: one group of tpc threads per column
   const int tpc = kc.tpf;
-  const int ngc = std::min(std::max(1, 256 / tpc), h->m);
+  // (the kernels are built for at most 256 threads per CTA, or one group if larger)
+  const int col_cta = PFC_FLAG_COL_CTA_OF(flags), ngc_max = std::max(1, 256 / tpc);
+  const int ngc = std::min(col_cta ? std::min(col_cta, ngc_max) : ngc_max, h->m);
   const size_t fr_smem = (size_t)rows * ld * elt;
   const size_t fc_smem = (size_t)ngc * (h->ny + (h->ny >> P) + 2) * elt;   // one exchange buffer per column
   if (ngr * tpr > 1024 || ngc * tpc > 1024 || fr_smem > 200 * 1024 || fc_smem > 200 * 1024 ||
@@ -390,6 +392,24 @@ int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
 }
 
 // One row pass of a step: W -> V (of every plan in `table` when batched).
+// Launches a power-of-two step kernel, with PFC_FLAG_PDL as a programmatic dependent
+// launch (the kernel may start while the previous kernel of the stream drains; it waits
+// for it with griddepcontrol.wait before reading its outputs).
+inline cudaError_t launch_step_kernel(const pfc_plan* h, const void* fn, dim3 grid, dim3 block, void** args,
+                                      size_t smem, cudaStream_t s) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = (h->prob.flags & PFC_FLAG_PDL) ? 1 : 0;
+  return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
 template <class T>
 int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullptr, int count = 1) {
   if (h->fast) {
@@ -405,7 +425,8 @@ int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
     a.g = h->prob.g; a.min_phi = h->prob.min_phi;
     a.min_log = (h->prob.min_phi > 0) ? std::log(h->prob.min_phi) : -INFINITY;
     void* args[] = {(void*)&a};
-    cudaError_t e = cudaLaunchKernel(h->fast_row_fn, dim3(h->fr_grid, count), dim3(h->fr_threads), args, h->fr_smem, s);
+    cudaError_t e = launch_step_kernel(h, h->fast_row_fn, dim3(h->fr_grid, count), dim3(h->fr_threads), args,
+                                       h->fr_smem, s);
     ++h->launches;
     if (e != cudaSuccess) return fail(PFC_E_CUDA, "row step launch failed: %s", cudaGetErrorString(e));
     return PFC_OK;
@@ -436,7 +457,8 @@ int launch_step_col(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
     a.twA = tw + h->tw_ca; a.twB = tw + h->tw_cb;
     a.scale = (T)(1.0 / ((double)h->nx * (double)h->ny));
     void* args[] = {(void*)&a};
-    cudaError_t e = cudaLaunchKernel(h->fast_col_fn, dim3(h->fc_grid, count), dim3(h->fc_threads), args, h->fc_smem, s);
+    cudaError_t e = launch_step_kernel(h, h->fast_col_fn, dim3(h->fc_grid, count), dim3(h->fc_threads), args,
+                                       h->fc_smem, s);
     ++h->launches;
     if (e != cudaSuccess) return fail(PFC_E_CUDA, "column step launch failed: %s", cudaGetErrorString(e));
     return PFC_OK;

@@ -41,9 +41,9 @@ def GetLinearKernel_phi(modelParameters, DerivativeKernels):
 
 class Simulation(_Simulation):
     def __init__(self, modelParameters, geometry, precision="fp64", clamp_log=False, device=None, kernels="auto",
-                 graphs=True):
+                 graphs=True, pdl=None):
         super().__init__("log", modelParameters, geometry, precision=precision, clamp_log=clamp_log, device=device,
-                         kernels=kernels, graphs=graphs)
+                         kernels=kernels, graphs=graphs, pdl=pdl)
 
     def Get_local_phi(self):
         """Gaussian-coarsened phi (models/logpfc/simulation.py:232-242)."""
@@ -51,9 +51,9 @@ class Simulation(_Simulation):
 
 
 def BuildB200_Simulation(modelParameters, geometry, precision="fp64", clamp_log=False, device=None, kernels="auto",
-                         graphs=True):
+                         graphs=True, pdl=None):
     return Simulation(modelParameters, geometry, precision=precision, clamp_log=clamp_log, device=device,
-                      kernels=kernels, graphs=graphs)
+                      kernels=kernels, graphs=graphs, pdl=pdl)
 
 
 def BuildCupyGPU_Simulation(modelParameters, geometry, *_, precision="fp64", **__):

@@ -356,9 +356,11 @@ class _SimulationState:
 def _kernel_flags(kernels, prob):
     """problem.flags bits for the `kernels` choice of a Simulation: "auto" (the variant
     the autotuner cached for this grid, else the defaults), "default", "generic" (the
-    mixed-radix kernels everywhere), or a dict {"ee_row", "ee_col", "row_tile"}."""
+    mixed-radix kernels everywhere), or a dict with any of "ee_row", "ee_col",
+    "row_tile", "col_cta" (columns per CTA of the column kernel) and "pdl"."""
     if isinstance(kernels, dict):
-        return _lib.flag_variant(kernels.get("ee_row", 0), kernels.get("ee_col", 0), kernels.get("row_tile", 0))
+        return _lib.flag_variant(**{k: kernels.get(k, 0) for k in ("ee_row", "ee_col", "row_tile", "col_cta",
+                                                                    "pdl")})
     if kernels == "generic":
         return _lib.FLAG_GENERIC_ONLY
     if kernels == "default":
@@ -374,7 +376,7 @@ class Simulation:
     """The reference's Simulation (models/stdpfc/simulation.py:166-268) backed by a plan."""
 
     def __init__(self, model: str, modelParameters, geometry, precision="fp64", clamp_log=False, device=None,
-                 kernels="auto", graphs=True):
+                 kernels="auto", graphs=True, pdl=None):
         if model not in ("std", "log"):
             raise ValueError(f"model must be 'std' or 'log', got {model!r}")
         if precision not in _PRECISIONS:
@@ -395,6 +397,8 @@ class Simulation:
         prob.min_phi = float(getattr(m, "minPhi", 0.0) or 0.0)
         prob.clamp_log = 1 if clamp_log else 0
         prob.flags = _kernel_flags(kernels, prob) | (0 if graphs else _lib.FLAG_NO_GRAPHS)
+        if pdl is not None:   # None: as the variant says
+            prob.flags = (prob.flags & ~_lib.FLAG_PDL) | (_lib.FLAG_PDL if pdl else 0)
         self._plan = Plan(prob, device)
         self._version = 0
         self._mu_current = False

@@ -44,9 +44,10 @@ def GetLinearKernel_n(modelParameters, DerivativeKernels):
 
 
 class Simulation(_Simulation):
-    def __init__(self, modelParameters, geometry, precision="fp64", device=None, kernels="auto", graphs=True):
+    def __init__(self, modelParameters, geometry, precision="fp64", device=None, kernels="auto", graphs=True,
+                 pdl=None):
         super().__init__("std", modelParameters, geometry, precision=precision, device=device, kernels=kernels,
-                         graphs=graphs)
+                         graphs=graphs, pdl=pdl)
 
     def Get_local_n(self):
         """Gaussian-coarsened n of the state at the start of the last step, on the host
@@ -54,11 +55,15 @@ class Simulation(_Simulation):
         return self._get_local()
 
 
-def BuildB200_Simulation(modelParameters, geometry, precision="fp64", device=None, kernels="auto", graphs=True):
+def BuildB200_Simulation(modelParameters, geometry, precision="fp64", device=None, kernels="auto", graphs=True,
+                         pdl=None):
     """precision: "fp64" (plain) or "fp32" (mixed); kernels: "auto" (power-of-two step
     kernels where the grid allows) or "generic" (mixed-radix kernels everywhere);
-    graphs: replay blocks of 16 steps from a recorded CUDA graph."""
-    return Simulation(modelParameters, geometry, precision=precision, device=device, kernels=kernels, graphs=graphs)
+    graphs: replay steps from recorded CUDA graphs (blocks of 16 and single steps);
+    pdl: let each power-of-two step kernel start while the one before it drains (None:
+    as the tuned variant says)."""
+    return Simulation(modelParameters, geometry, precision=precision, device=device, kernels=kernels, graphs=graphs,
+                      pdl=pdl)
 
 
 def BuildCupyGPU_Simulation(modelParameters, geometry, *_, precision="fp64", **__):

@@ -5,7 +5,11 @@
 For one grid, precision and model it times every built variant of the two step
 kernels (complex values per thread of the row and the column kernel, rows per
 CTA of the row kernel) with CUDA events on a seeded noisy-liquid state, and keeps
-the fastest row and the fastest column variant. Results are cached as JSON, keyed
+the fastest row and the fastest column variant. A second stage times that choice
+with 1, 2 and 4 columns per CTA of the column kernel, with and without programmatic
+dependent launch, over whole steps replayed from CUDA graphs, and keeps a change only
+where it is at least 1 % faster (`--refine` runs this stage alone on the entries the
+package or the cache already holds). Results are cached as JSON, keyed
 by GPU name, grid, precision and model, in the file named by $PFC_TUNE_CACHE
 (default ~/.cache/pfc_models_b200/tune.json). `Simulation(kernels="auto")` looks
 a grid up there first, then in the table measured on B200 that ships with the
@@ -26,6 +30,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PACKAGED = os.path.join(HERE, "tuned_b200.json")
 EE_CHOICES = {_lib.FP32_MIXED: (8, 16, 32), _lib.FP64_PLAIN: (8, 16)}
 TILE_CHOICES = (1, 2, 4, 8, 16)
+COL_CTA_CHOICES = (1, 2, 4)
+VARIANT_KEYS = ("ee_row", "ee_col", "row_tile", "col_cta", "pdl")
 _lock = threading.Lock()
 _memo: dict = {}
 
@@ -60,7 +66,8 @@ def _device_name():
 
 
 def lookup(nx, ny, precision, model, device_name=None, batched=False):
-    """The cached variant {"ee_row", "ee_col", "row_tile"} for this grid, or None.
+    """The cached variant {"ee_row", "ee_col", "row_tile", "col_cta", "pdl"} for this
+    grid, or None.
     `batched`: prefer the variant measured for many plans stepped as one batch (the
     single-plan choice favours latency, a batch is throughput-bound)."""
     if device_name is None:
@@ -74,7 +81,7 @@ def lookup(nx, ny, precision, model, device_name=None, batched=False):
         for path in (cache_path(), PACKAGED):
             e = _load(path).get(key)
             if e:
-                return {k: int(e[k]) for k in ("ee_row", "ee_col", "row_tile")}
+                return {k: int(e.get(k) or 0) for k in VARIANT_KEYS}
     return None
 
 
@@ -142,6 +149,7 @@ def tune(nx, ny, precision="fp32", model="std", steps=20, warmup=3, save=True, p
     entry = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile, "row_us": row_us, "col_us": col_us,
              "rows_us": {f"{a}/{b}": u for (a, b), u in sorted(rows.items())},
              "cols_us": {str(k): u for k, u in sorted(col_avg.items())}}
+    entry.update(refine(nx, ny, precision, model, entry))
     if save:
         _store(path or cache_path(), _key(_device_name(), nx, ny, prec,
                                           _lib.MODEL_LOG if model == "log" else _lib.MODEL_STD), entry)
@@ -197,10 +205,84 @@ def _tune_batch(nx, ny, precision, model, steps, warmup, save, path, batch):
     entry = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile, "batch": batch, "step_us": us,
              "row_us": None, "col_us": None,
              "steps_us": {f"{a}/{b}/{c}": u for (a, b, c), u in sorted(timed.items())}}
+    entry.update(refine(nx, ny, precision, model, entry, batch=batch))
     if save:
         _store(path or cache_path(), _key(_device_name(), nx, ny, prec,
                                           _lib.MODEL_LOG if model == "log" else _lib.MODEL_STD, True), entry)
     return entry
+
+
+def _time_blocks(nx, ny, precision, model, variant, batch, steps=320):
+    """us per whole step of `batch` plans (1: one plan) with this variant, replayed from
+    16-step graphs after a warm-up that records them; None if the fast kernels do not
+    apply. Also returns the column kernel's threads per CTA, to merge equal launches."""
+    import torch
+
+    from .simulation import Batch
+    mod, geom, prm, f0 = _setup(nx, ny, precision, model)
+    sims = [mod.BuildB200_Simulation(prm, geom, precision=precision, kernels=variant) for _ in range(batch)]
+    b = None
+    try:
+        if not sims[0].plan.variant()["fast"]:
+            return None, None
+        threads = sims[0].plan.info()["fast_col_threads"]
+        for s in sims:
+            (s.State.phi if model == "log" else s.State.n)[...] = f0
+        b = Batch(sims) if batch > 1 else None
+        stepper = b if b is not None else sims[0].plan
+        stepper.step(32)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        stepper.step(steps)
+        e1.record()
+        e1.synchronize()
+        return 1e3 * e0.elapsed_time(e1) / steps, threads
+    finally:
+        if b is not None:
+            b.close()
+        for s in sims:
+            s.plan.close()
+
+
+def refine(nx, ny, precision, model, base, batch=1, min_gain=0.01):
+    """Second stage: columns per CTA of the column kernel and programmatic dependent
+    launch for the row/column variant in `base`, timed over whole steps. Returns
+    {"col_cta", "pdl", "refine_us"}; keeps the defaults (0, 0) unless a choice is at
+    least `min_gain` faster than they are."""
+    v0 = {k: int(base.get(k) or 0) for k in ("ee_row", "ee_col", "row_tile")}
+    timed, seen = {}, {}
+    for cc in (0,) + COL_CTA_CHOICES:
+        for pdl in (0, 1):
+            us, threads = _time_blocks(nx, ny, precision, model, dict(v0, col_cta=cc, pdl=pdl), batch)
+            if us is None:
+                return {"col_cta": 0, "pdl": 0}
+            if cc and seen.get((threads, pdl)) is not None:
+                continue     # the same launch as a choice timed already
+            seen.setdefault((threads, pdl), cc)
+            timed[(cc, pdl)] = us
+    best = min(timed.items(), key=lambda kv: kv[1])
+    if best[1] > (1 - min_gain) * timed[(0, 0)]:
+        best = ((0, 0), timed[(0, 0)])
+    (cc, pdl), _ = best
+    return {"col_cta": cc, "pdl": pdl, "refine_us": {f"{a}/{b}": u for (a, b), u in sorted(timed.items())}}
+
+
+def refine_table(path_in, device_name, steps=320):
+    """Runs the second stage on every entry of `path_in` for this GPU; returns the
+    updated table."""
+    d = dict(_load(path_in))
+    for key, e in sorted(d.items()):
+        parts = key.split("|")
+        if parts[0] != device_name:
+            continue
+        nx, ny = (int(v) for v in parts[1].split("x"))
+        batch = int(e.get("batch") or 1) if len(parts) > 4 and parts[4] == "batch" else 1
+        e = dict(e)
+        e.update(refine(nx, ny, parts[2], parts[3], e, batch=batch))
+        d[key] = e
+        print(json.dumps({key: {k: e.get(k) for k in VARIANT_KEYS + ("refine_us",)}}), flush=True)
+    return d
 
 
 def main():
@@ -212,7 +294,16 @@ def main():
     ap.add_argument("--save", action="store_true", help="write the user cache")
     ap.add_argument("--batch", type=int, default=1, help="time this many plans stepped as one batch")
     ap.add_argument("--out", default=None, help="also write all entries to this JSON file")
+    ap.add_argument("--refine", default=None, metavar="TABLE",
+                    help="run only the second stage on every entry of TABLE ('packaged' for the shipped "
+                         "table) and write the result to --out")
     a = ap.parse_args()
+    if a.refine:
+        d = refine_table(PACKAGED if a.refine == "packaged" else a.refine, _device_name())
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(d, f, indent=1, sort_keys=True)
+        return
     allres = {}
     for s in a.sizes.split(","):
         nx, ny = (int(v) for v in s.split("x")) if "x" in s else (int(s), int(s))

@@ -1,8 +1,9 @@
-"""Batched stepping (pfc_batch_*) and CUDA-graph replay of step blocks.
+"""Batched stepping (pfc_batch_*), CUDA-graph replay of steps and programmatic
+dependent launch of the step kernels.
 
-Both only change how the step kernels are launched, never what they compute, so
+These only change how the step kernels are launched, never what they compute, so
 the results must be bit-identical to stepping each plan on its own with every
-kernel launched directly.
+kernel launched directly and serialised.
 """
 import numpy as np
 import pytest
@@ -13,32 +14,32 @@ from pfc_models_b200.simulation import Batch
 pytestmark = pytest.mark.gpu
 
 
-def _std_sim(nx, ny, eps, mean, precision, seed, graphs=True):
+def _std_sim(nx, ny, eps, mean, precision, seed, graphs=True, pdl=None, kernels="auto"):
     prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=eps, g=0.0, dt=0.5)
     geom = stdpfc.Build2DGeometry(nx, ny, nx * np.pi / 4, ny * np.pi / 4)
-    sim = stdpfc.BuildB200_Simulation(prm, geom, precision=precision, graphs=graphs)
+    sim = stdpfc.BuildB200_Simulation(prm, geom, precision=precision, graphs=graphs, pdl=pdl, kernels=kernels)
     sim.State.n[...] = mean + 0.05 * np.random.default_rng(seed).uniform(-1, 1, (ny, nx))
     return sim
 
 
-def _log_sim(nx, ny, precision, seed, graphs=True):
+def _log_sim(nx, ny, precision, seed, graphs=True, pdl=None, kernels="auto"):
     prm = logpfc.BuildLogPFCModelParameters(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=0.05)
     geom = logpfc.Build2DGeometry(nx, ny, nx * np.pi / 4, ny * np.pi / 4)
-    sim = logpfc.BuildB200_Simulation(prm, geom, precision=precision, graphs=graphs)
+    sim = logpfc.BuildB200_Simulation(prm, geom, precision=precision, graphs=graphs, pdl=pdl, kernels=kernels)
     sim.State.phi[...] = 0.55 + 0.05 * np.random.default_rng(seed).uniform(-1, 1, (ny, nx))
     return sim
 
 
-def _mixed(precision, graphs):
+def _mixed(precision, graphs, pdl=None):
     """Six plans in four classes: 64^2 std (x2), 128^2 std (x2), 64^2 log, 128x64 std."""
     specs = [("std", 64, 64, -0.3, -0.3), ("std", 128, 128, -0.25, -0.2), ("std", 64, 64, -0.6, -0.45),
              ("log", 64, 64, None, None), ("std", 128, 64, -0.1, -0.05), ("std", 128, 128, -0.5, -0.4)]
     sims = []
     for i, (m, nx, ny, eps, mean) in enumerate(specs):
         if m == "std":
-            sims.append(_std_sim(nx, ny, eps, mean, precision, seed=i, graphs=graphs))
+            sims.append(_std_sim(nx, ny, eps, mean, precision, seed=i, graphs=graphs, pdl=pdl))
         else:
-            sims.append(_log_sim(nx, ny, precision, seed=i, graphs=graphs))
+            sims.append(_log_sim(nx, ny, precision, seed=i, graphs=graphs, pdl=pdl))
     return sims
 
 
@@ -49,11 +50,12 @@ def _field(sim):
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_batch_matches_individual_plans(precision):
     """37 steps (two replayed 16-step blocks and 5 direct steps) of a batch equal the
-    same plans stepped one by one; a second call continues from the other parity."""
-    ref = _mixed(precision, graphs=False)
+    same plans stepped one by one with serialised launches; a second call continues
+    from the other parity."""
+    ref = _mixed(precision, graphs=False, pdl=False)
     for s in ref:
         s.TimeSteps(37)
-    sims = _mixed(precision, graphs=True)
+    sims = _mixed(precision, graphs=True, pdl=True)
     b = Batch(sims)
     assert b.classes == 4
     b.step(37)
@@ -81,6 +83,32 @@ def test_graph_replay_matches_direct_launches(precision):
         assert np.array_equal(a.State.n.get(), d.State.n.get())
     # the count includes the launches that materialise the fields read above
     assert a.plan.launches() == d.plan.launches() >= 2 * 90
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("model", ["std", "log"])
+def test_launch_modes_match_serialised_launches(precision, model):
+    """A step kernel that starts while the previous one drains (griddepcontrol), and
+    column kernels of 1, 2 or 4 columns per CTA, give the same bits as serialised
+    launches of the default shape, replayed from graphs or launched directly."""
+    def make(graphs, pdl, col_cta=0):
+        kernels = "auto"
+        if col_cta:
+            v = make(False, False).plan.variant()
+            kernels = {"ee_row": v["ee_row"], "ee_col": v["ee_col"], "row_tile": v["row_tile"], "col_cta": col_cta}
+        if model == "std":
+            return _std_sim(512, 256, -0.25, -0.25, precision, seed=5, graphs=graphs, pdl=pdl, kernels=kernels)
+        return _log_sim(256, 256, precision, seed=5, graphs=graphs, pdl=pdl, kernels=kernels)
+    ref = make(False, False)
+    sims = [make(True, True), make(False, True), make(True, False, 1), make(True, True, 4)]
+    assert sims[2].plan.info()["fast_col_ctas"] == sims[2].Geometry.Nx // 2    # one column per CTA
+    for n in (17, 1, 32, 3):
+        ref.TimeSteps(n)
+        want = _field(ref)
+        for s in sims:
+            s.TimeSteps(n)
+            assert np.array_equal(_field(s), want)
+    assert all(s.Reduce() == ref.Reduce() for s in sims)
 
 
 def test_batch_rejects_mixed_parity_and_unsupported_plans():
@@ -136,6 +164,6 @@ def test_auto_kernels_use_the_packaged_table():
     sim = _std_sim(256, 256, -0.25, -0.25, "fp32", seed=0)
     v = sim.plan.variant()
     if key in table and tune.lookup(256, 256, _lib.FP32_MIXED, _lib.MODEL_STD) == \
-            {k: table[key][k] for k in ("ee_row", "ee_col", "row_tile")}:
+            {k: int(table[key].get(k) or 0) for k in tune.VARIANT_KEYS}:
         assert (v["ee_row"], v["ee_col"]) == (table[key]["ee_row"], table[key]["ee_col"])
     assert v["fast"] == 1

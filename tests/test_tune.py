@@ -12,14 +12,15 @@ def test_packaged_table_is_used_without_a_user_cache(tmp_path, monkeypatch):
     key = "NVIDIA B200|2048x2048|fp32|std"
     assert key in table
     v = tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200")
-    assert v == {k: table[key][k] for k in ("ee_row", "ee_col", "row_tile")}
+    assert v == {k: int(table[key].get(k) or 0) for k in tune.VARIANT_KEYS}
     for e in table.values():
         assert e["ee_row"] in (8, 16, 32) and e["ee_col"] in (8, 16, 32) and e["row_tile"] in (1, 2, 4, 8, 16)
+        assert e.get("col_cta", 0) in (0, 1, 2, 4) and e.get("pdl", 0) in (0, 1)
     # batch-measured entries are preferred for batches and fall back to the single-plan ones
     bkey = "NVIDIA B200|512x512|fp32|std|batch"
     assert bkey in table
     vb = tune.lookup(512, 512, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200", batched=True)
-    assert vb == {k: table[bkey][k] for k in ("ee_row", "ee_col", "row_tile")}
+    assert vb == {k: int(table[bkey].get(k) or 0) for k in tune.VARIANT_KEYS}
     v2 = tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200", batched=True)
     assert v2 == v
     assert tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="other GPU") is None
@@ -33,7 +34,12 @@ def test_user_cache_overrides_and_round_trips(tmp_path, monkeypatch):
     tune._memo.clear()
     assert json.load(open(path))[key]["ee_col"] == 32
     assert tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200") == \
-        {"ee_row": 16, "ee_col": 32, "row_tile": 2}
+        {"ee_row": 16, "ee_col": 32, "row_tile": 2, "col_cta": 0, "pdl": 0}
+    # entries of the second stage carry the column CTA width and the launch mode
+    tune._store(str(path), key, {"ee_row": 16, "ee_col": 16, "row_tile": 4, "col_cta": 1, "pdl": 1})
+    tune._memo.clear()
+    assert tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200") == \
+        {"ee_row": 16, "ee_col": 16, "row_tile": 4, "col_cta": 1, "pdl": 1}
     tune._memo.clear()
 
 
@@ -45,3 +51,8 @@ def test_flag_encoding_matches_header():
     shifts = dict(re.findall(r"#define PFC_FLAG_(ROW_EE|COL_EE|ROW_TILE)\(\w\) \(\(int32_t\)\(\w\) << (\d+)\)", src))
     assert shifts == {"ROW_EE": "8", "COL_EE": "16", "ROW_TILE": "24"}
     assert _lib.flag_variant(16, 32, 4) == (16 << 8) | (32 << 16) | (4 << 24)
+    assert re.search(r"#define PFC_FLAG_PDL 4\b", src)
+    assert re.search(r"#define PFC_FLAG_COL_CTA\(c\) .*<< 29\)", src)
+    # columns per CTA 1, 2, 4 -> field values 1, 2, 3 in bits 29-30
+    assert [_lib.flag_variant(col_cta=c) >> 29 for c in (0, 1, 2, 4)] == [0, 1, 2, 3]
+    assert _lib.flag_variant(pdl=1) == _lib.FLAG_PDL
