@@ -500,17 +500,29 @@ col_step_fast(FastColArgs<T> a) {
     for (int ky = t; ky < NY; ky += TPF) {
       const int kh = ky <= NY / 2 ? ky : NY - ky;
       if constexpr (sizeof(T) == 4) {
-        // fast modes (|A - 1| >= tau): the update in FP32 on hi alone; their rounding
-        // errors are damped by at least tau every step
+        // the coefficient and the state's hi part are loaded together (both paths read
+        // them), so the loads of the unrolled iterations are all in flight at once
         const cplx<T> cw = gcoef[ccb + kh];
+        const cplx<float> p = static_cast<const cplx<float>*>(gnin)[cb + ky];
+        const cplx<float> gv = buf[padi<P>(ky)];
         if (fabsf(cw.x) >= tau) {
-          const cplx<float> p = static_cast<const cplx<float>*>(gnin)[cb + ky];
-          const cplx<float> gv = buf[padi<P>(ky)];
+          // fast modes (|A - 1| >= tau): the update in FP32 on hi alone; their rounding
+          // errors are damped by at least tau every step
           const cplx<float> o = mk(fmaf(cw.x, p.x, p.x) + cw.y * gv.x, fmaf(cw.x, p.y, p.y) + cw.y * gv.y);
           static_cast<cplx<float>*>(gnout)[cb + ky] = o;
           buf[padi<P>(ky)] = o;
-          continue;
+        } else {
+          // slow modes: FP64 coefficients and the state with its residual
+          const cplx<double> c = gcoef64[ccb + kh];
+          const cplx<float> l = gnin_lo[cb + ky];
+          cplx<double> pd = mk((double)p.x, (double)p.y);
+          pd.x += (double)l.x;
+          pd.y += (double)l.y;
+          const cplx<double> o = pd + c.x * pd + c.y * mk((double)gv.x, (double)gv.y);
+          state_st<T>(gnout, gnout_lo, cb + ky, o, true);
+          buf[padi<P>(ky)] = mk((T)o.x, (T)o.y);
         }
+        continue;
       }
       bool slow;
       const cplx<double> c = coef_ld<T>(gcoef, gcoef64, ccb + kh, tau, false, slow);
