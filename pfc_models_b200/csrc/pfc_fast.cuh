@@ -496,67 +496,94 @@ col_step_fast(FastColArgs<T> a) {
   const float tau = a.slow_tau;
   if (kx != 0) {
     const size_t ccb = (size_t)kx * nyh;
-#pragma unroll 8
-    for (int ky = t; ky < NY; ky += TPF) {
-      const int kh = ky <= NY / 2 ? ky : NY - ky;
-      if constexpr (sizeof(T) == 4) {
-        // the coefficient and the state's hi part are loaded together (both paths read
-        // them), so the loads of the unrolled iterations are all in flight at once
-        const cplx<T> cw = gcoef[ccb + kh];
-        const cplx<float> p = static_cast<const cplx<float>*>(gnin)[cb + ky];
-        const cplx<float> gv = buf[padi<P>(ky)];
-        if (fabsf(cw.x) >= tau) {
-          // fast modes (|A - 1| >= tau): the update in FP32 on hi alone; their rounding
-          // errors are damped by at least tau every step
-          const cplx<float> o = mk(fmaf(cw.x, p.x, p.x) + cw.y * gv.x, fmaf(cw.x, p.y, p.y) + cw.y * gv.y);
-          static_cast<cplx<float>*>(gnout)[cb + ky] = o;
-          buf[padi<P>(ky)] = o;
+    // Each thread updates modes ky = t + j TPF, j < EE, in chunks: the coefficients and
+    // states of a whole chunk are loaded before any of its results is stored (the
+    // compiler may not move a load above an earlier store to memory it cannot tell
+    // apart), so the chunk's loads are in flight together.
+    constexpr int CH = (sizeof(T) == 4 && EE >= 16) ? 8 : 4;   // within the 64-register budget
+    static_assert(EE % CH == 0, "chunks tile the modes of a thread");
+#pragma unroll 1
+    for (int j0 = 0; j0 < EE; j0 += CH) {
+      cplx<T> cw[CH], p[CH];
+#pragma unroll
+      for (int j = 0; j < CH; ++j) {
+        const int ky = t + (j0 + j) * TPF;
+        const int kh = ky <= NY / 2 ? ky : NY - ky;
+        cw[j] = gcoef[ccb + kh];
+        p[j] = static_cast<const cplx<T>*>(gnin)[cb + ky];
+      }
+#pragma unroll
+      for (int j = 0; j < CH; ++j) {
+        const int ky = t + (j0 + j) * TPF;
+        const int kh = ky <= NY / 2 ? ky : NY - ky;
+        const cplx<T> gv = buf[padi<P>(ky)];
+        if constexpr (sizeof(T) == 4) {
+          if (fabsf(cw[j].x) >= tau) {
+            // fast modes (|A - 1| >= tau): the update in FP32 on hi alone; their
+            // rounding errors are damped by at least tau every step
+            const cplx<float> o = mk(fmaf(cw[j].x, p[j].x, p[j].x) + cw[j].y * gv.x,
+                                     fmaf(cw[j].x, p[j].y, p[j].y) + cw[j].y * gv.y);
+            static_cast<cplx<float>*>(gnout)[cb + ky] = o;
+            buf[padi<P>(ky)] = o;
+          } else {
+            // slow modes: FP64 coefficients and the state with its residual
+            const cplx<double> c = gcoef64[ccb + kh];
+            const cplx<float> l = gnin_lo[cb + ky];
+            cplx<double> pd = mk((double)p[j].x, (double)p[j].y);
+            pd.x += (double)l.x;
+            pd.y += (double)l.y;
+            const cplx<double> o = pd + c.x * pd + c.y * mk((double)gv.x, (double)gv.y);
+            state_st<T>(gnout, gnout_lo, cb + ky, o, true);
+            buf[padi<P>(ky)] = mk((T)o.x, (T)o.y);
+          }
         } else {
-          // slow modes: FP64 coefficients and the state with its residual
-          const cplx<double> c = gcoef64[ccb + kh];
-          const cplx<float> l = gnin_lo[cb + ky];
-          cplx<double> pd = mk((double)p.x, (double)p.y);
-          pd.x += (double)l.x;
-          pd.y += (double)l.y;
+          const cplx<double> c = cw[j], pd = p[j];
           const cplx<double> o = pd + c.x * pd + c.y * mk((double)gv.x, (double)gv.y);
           state_st<T>(gnout, gnout_lo, cb + ky, o, true);
           buf[padi<P>(ky)] = mk((T)o.x, (T)o.y);
         }
-        continue;
       }
-      bool slow;
-      const cplx<double> c = coef_ld<T>(gcoef, gcoef64, ccb + kh, tau, false, slow);
-      const cplx<double> p = state_ld<T>(gnin, gnin_lo, cb + ky, slow);
-      const cplx<T> gv = buf[padi<P>(ky)];
-      const cplx<double> o = p + c.x * p + c.y * mk((double)gv.x, (double)gv.y);
-      state_st<T>(gnout, gnout_lo, cb + ky, o, slow);
-      buf[padi<P>(ky)] = mk((T)o.x, (T)o.y);
     }
   } else {
     // packed DC/Nyquist column (kx = 0 and kx = M): one (ky, -ky) pair per step, always
     // at full precision
     const size_t cmb = (size_t)m * nyh;
-#pragma unroll 2
-    for (int ky = t; ky <= NY / 2; ky += TPF) {
-      const int kyp = ky == 0 ? 0 : NY - ky;
-      const cplx<T> qkt = buf[padi<P>(ky)], qkpt = buf[padi<P>(kyp)];
-      const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
-      const cplx<double> pk = state_ld<T>(gnin, gnin_lo, cb + ky, true);
-      const cplx<double> pkp = state_ld<T>(gnin, gnin_lo, cb + kyp, true);
-      cplx<double> h0, hm, g0, gm;
-      unpack_pair(pk, pkp, h0, hm);
-      unpack_pair(qk, qkp, g0, gm);
-      bool s0, sm;
-      const cplx<double> a0 = coef_ld<T>(gcoef, gcoef64, ky, tau, true, s0);
-      const cplx<double> am = coef_ld<T>(gcoef, gcoef64, cmb + ky, tau, true, sm);
-      const cplx<double> h0n = h0 + a0.x * h0 + a0.y * g0;
-      const cplx<double> hmn = hm + am.x * hm + am.y * gm;
-      const cplx<double> ok = h0n + mul_i(hmn), okp = conj(h0n) + mul_i(conj(hmn));
-      state_st<T>(gnout, gnout_lo, cb + ky, ok, true);
-      buf[padi<P>(ky)] = mk((T)ok.x, (T)ok.y);
-      if (kyp != ky) {
-        state_st<T>(gnout, gnout_lo, cb + kyp, okp, true);
-        buf[padi<P>(kyp)] = mk((T)okp.x, (T)okp.y);
+    // two pairs per chunk, both loaded before either is stored (as above)
+    constexpr int CP = 2;
+#pragma unroll 1
+    for (int i0 = 0; t + i0 * TPF <= NY / 2; i0 += CP) {
+      cplx<double> pk[CP], pkp[CP], a0[CP], am[CP];
+#pragma unroll
+      for (int j = 0; j < CP; ++j) {
+        const int ky = t + (i0 + j) * TPF;
+        if (ky <= NY / 2) {
+          const int kyp = ky == 0 ? 0 : NY - ky;
+          bool s0, sm;
+          pk[j] = state_ld<T>(gnin, gnin_lo, cb + ky, true);
+          pkp[j] = state_ld<T>(gnin, gnin_lo, cb + kyp, true);
+          a0[j] = coef_ld<T>(gcoef, gcoef64, ky, tau, true, s0);
+          am[j] = coef_ld<T>(gcoef, gcoef64, cmb + ky, tau, true, sm);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < CP; ++j) {
+        const int ky = t + (i0 + j) * TPF;
+        if (ky > NY / 2) break;
+        const int kyp = ky == 0 ? 0 : NY - ky;
+        const cplx<T> qkt = buf[padi<P>(ky)], qkpt = buf[padi<P>(kyp)];
+        const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
+        cplx<double> h0, hm, g0, gm;
+        unpack_pair(pk[j], pkp[j], h0, hm);
+        unpack_pair(qk, qkp, g0, gm);
+        const cplx<double> h0n = h0 + a0[j].x * h0 + a0[j].y * g0;
+        const cplx<double> hmn = hm + am[j].x * hm + am[j].y * gm;
+        const cplx<double> ok = h0n + mul_i(hmn), okp = conj(h0n) + mul_i(conj(hmn));
+        state_st<T>(gnout, gnout_lo, cb + ky, ok, true);
+        buf[padi<P>(ky)] = mk((T)ok.x, (T)ok.y);
+        if (kyp != ky) {
+          state_st<T>(gnout, gnout_lo, cb + kyp, okp, true);
+          buf[padi<P>(kyp)] = mk((T)okp.x, (T)okp.y);
+        }
       }
     }
   }
