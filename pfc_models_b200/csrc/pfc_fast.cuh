@@ -7,9 +7,13 @@
 // nonlinearity between them (inverse A, forward B) and the column kernel applies the
 // ETD1 update between them (forward A, inverse B) without a shared-memory round trip.
 //
-// Shared-memory exchanges between passes use the padded index i + (i >> P) with
-// 2^P = elements per 128 bytes (16 complex floats, 8 complex doubles), which makes
-// the stride-R writes of every Stockham pass with R <= 2^P bank-conflict free.
+// Shared-memory exchanges between passes use the padded index i + (i >> P), one pad
+// element per 2^P. Shared memory serves 8-byte accesses per half-warp (16 lanes, bank
+// pair = index mod 16) and 16-byte accesses per quarter-warp (8 lanes, index mod 8);
+// P is chosen per element size and values per thread so that the Stockham loads and
+// stores of every pass need the fewest wavefronts under that rule (fast_pad_shift).
+// Every radix R of a sequence satisfies R <= 2^P, so the R consecutive outputs of an
+// NS = 1 pass never straddle a pad.
 // A transform group synchronises with __syncwarp when it fits in a warp, otherwise
 // with its own named barrier, so groups never wait for each other.
 #pragma once
@@ -40,13 +44,20 @@ struct FastSeq {
   __host__ __device__ static constexpr int sizeB() { return twB(NPASS); }
 };
 
-// pad one element per 2^P: P = 5 for complex float (radix-32 passes), 4 for complex double
-template <class T> struct PadShift { static constexpr int value = 5; };
-template <> struct PadShift<double> { static constexpr int value = 4; };
+// Pad shift of the exchange buffers for EE values per thread (the effective EE of the
+// transform). Complex float: radix-32 passes (EE = 32) need a pad per 32 elements,
+// radix-16 and radix-8 passes one per 16; complex double: one per 16 for radix 16,
+// one per 8 for radix 8. (With one pad per 32 the radix-16 FP32 column transform
+// stored 1.5 wavefronts per 128 bytes in three of its four exchanges.)
+__host__ __device__ constexpr int fast_pad_shift(bool fp64, int ee) {
+  return fp64 ? (ee >= 16 ? 4 : 3) : (ee >= 32 ? 5 : 4);
+}
+template <class T, int EE> struct FastPad { static constexpr int value = fast_pad_shift(sizeof(T) == 8, EE); };
 
 template <int P> __device__ __forceinline__ int padi(int i) { return i + (i >> P); }
 
-template <class T> struct RadixCap { static constexpr int value = 1 << PadShift<T>::value; };
+// largest radix of a pass: 32 complex floats or 16 complex doubles per thread
+template <class T> struct RadixCap { static constexpr int value = sizeof(T) == 4 ? 32 : 16; };
 
 __device__ __forceinline__ float2 ldg2(const float2* p) { return __ldg(p); }
 __device__ __forceinline__ double2 ldg2(const double2* p) { return __ldg(p); }
@@ -74,6 +85,7 @@ __device__ __forceinline__ void group_sync(int g) {
 // TPF threads holding EE = R * NB values each (v[b * R + q], butterfly j = t + b * TPF).
 template <class T, int N, int EE, int R, int NS, int P>
 struct FastPass {
+  static_assert(R <= (1 << P), "a butterfly's consecutive outputs must not straddle a pad");
   static constexpr int TPF = N / EE, NB = EE / R, NR = N / R;
   // padi(x + q * S) = padi(x) + q * (S + S / 2^P) whenever 2^P divides S
   static constexpr int NRP = NR + (NR >> P);
@@ -143,7 +155,7 @@ template <class T, int N, int EE_REQ, bool SEQB, bool INV, int PA, int PB>
 __device__ __forceinline__ void fast_mid(cplx<T>* buf, cplx<T>* v, int t, int g, const cplx<T>* __restrict__ tw) {
   if constexpr (PA < PB) {
     using S = FastSeq<N, EE_REQ, RadixCap<T>::value>;
-    constexpr int P = PadShift<T>::value;
+    constexpr int P = FastPad<T, S::EE>::value;
     constexpr int R = SEQB ? S::radB(PA) : S::radA(PA);
     constexpr int NS = SEQB ? S::nsB(PA) : S::nsA(PA);
     constexpr int OFF = SEQB ? S::twB(PA) : S::twA(PA);
@@ -244,7 +256,7 @@ __global__ void __launch_bounds__(FastBound<FastSeq<M, EE_REQ, RadixCap<T>::valu
                                 FastSeq<M, EE_REQ, RadixCap<T>::value>::TPF>::value)
 row_step_fast(FastRowArgs<T> a) {
   using S = FastSeq<M, EE_REQ, RadixCap<T>::value>;
-  constexpr int P = PadShift<T>::value;
+  constexpr int P = FastPad<T, S::EE>::value;
   constexpr int EE = S::EE, TPF = S::TPF, NP = S::NPASS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
@@ -410,7 +422,7 @@ __global__ void __launch_bounds__(FastBound<FastSeq<NY, EE_REQ, RadixCap<T>::val
                                                 FastSeq<NY, EE_REQ, RadixCap<T>::value>::TPF>::value)
 col_step_fast(FastColArgs<T> a) {
   using S = FastSeq<NY, EE_REQ, RadixCap<T>::value>;
-  constexpr int P = PadShift<T>::value;
+  constexpr int P = FastPad<T, S::EE>::value;
   constexpr int EE = S::EE, TPF = S::TPF, NP = S::NPASS;
   constexpr int PADN = NY + (NY >> P) + 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];

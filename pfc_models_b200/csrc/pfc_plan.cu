@@ -344,7 +344,10 @@ int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
   FastKernel kr, kc;
   if (!fast_lookup<T>(false, lm, ee_r, h->prob.model, &kr) || !fast_lookup<T>(true, ly, ee_c, h->prob.model, &kc))
     return PFC_OK;
-  constexpr int P = PadShift<T>::value;
+  // pad shifts of the row tile and the column exchange buffers, as the kernels use them
+  // (for the effective values per thread, length / threads per transform)
+  const int P = fast_pad_shift(sizeof(T) == 8, h->m / kr.tpf);
+  const int Pc = fast_pad_shift(sizeof(T) == 8, h->ny / kc.tpf);
   const int elt = (int)sizeof(cplx<T>);
   // row kernel: tile of fr_rows rows (>= 64 B per kx run by default), groups of tpf threads
   const int tpr = kr.tpf;
@@ -367,7 +370,7 @@ int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
   const int col_cta = PFC_FLAG_COL_CTA_OF(flags), ngc_max = std::max(1, 256 / tpc);
   const int ngc = std::min(col_cta ? std::min(col_cta, ngc_max) : ngc_max, h->m);
   const size_t fr_smem = (size_t)rows * ld * elt;
-  const size_t fc_smem = (size_t)ngc * (h->ny + (h->ny >> P) + 2) * elt;   // one exchange buffer per column
+  const size_t fc_smem = (size_t)ngc * (h->ny + (h->ny >> Pc) + 2) * elt;   // one exchange buffer per column
   if (ngr * tpr > 1024 || ngc * tpc > 1024 || fr_smem > 200 * 1024 || fc_smem > 200 * 1024 ||
       ilog2_exact(rows) < 0)
     return PFC_OK;  // generic path
