@@ -212,10 +212,11 @@ def _tune_batch(nx, ny, precision, model, steps, warmup, save, path, batch):
     return entry
 
 
-def _time_blocks(nx, ny, precision, model, variant, batch, steps=320):
-    """us per whole step of `batch` plans (1: one plan) with this variant, replayed from
-    16-step graphs after a warm-up that records them; None if the fast kernels do not
-    apply. Also returns the column kernel's threads per CTA, to merge equal launches."""
+def _time_blocks(nx, ny, precision, model, variant, batch, steps=320, skip=None):
+    """(us per whole step, column-kernel threads per CTA) of `batch` plans (1: one plan)
+    with this variant, replayed from 16-step graphs after a warm-up that records them.
+    (None, None) if the fast kernels do not apply; (None, threads) without timing when
+    skip(threads) is true (a launch equal to one timed already)."""
     import torch
 
     from .simulation import Batch
@@ -226,6 +227,8 @@ def _time_blocks(nx, ny, precision, model, variant, batch, steps=320):
         if not sims[0].plan.variant()["fast"]:
             return None, None
         threads = sims[0].plan.info()["fast_col_threads"]
+        if skip is not None and skip(threads):
+            return None, threads
         for s in sims:
             (s.State.phi if model == "log" else s.State.n)[...] = f0
         b = Batch(sims) if batch > 1 else None
@@ -251,15 +254,16 @@ def refine(nx, ny, precision, model, base, batch=1, min_gain=0.01):
     {"col_cta", "pdl", "refine_us"}; keeps the defaults (0, 0) unless a choice is at
     least `min_gain` faster than they are."""
     v0 = {k: int(base.get(k) or 0) for k in ("ee_row", "ee_col", "row_tile")}
-    timed, seen = {}, {}
+    timed, seen = {}, set()
     for cc in (0,) + COL_CTA_CHOICES:
         for pdl in (0, 1):
-            us, threads = _time_blocks(nx, ny, precision, model, dict(v0, col_cta=cc, pdl=pdl), batch)
-            if us is None:
+            us, threads = _time_blocks(nx, ny, precision, model, dict(v0, col_cta=cc, pdl=pdl), batch,
+                                       skip=lambda th: (th, pdl) in seen)
+            if threads is None:
                 return {"col_cta": 0, "pdl": 0}
-            if cc and seen.get((threads, pdl)) is not None:
+            if us is None:
                 continue     # the same launch as a choice timed already
-            seen.setdefault((threads, pdl), cc)
+            seen.add((threads, pdl))
             timed[(cc, pdl)] = us
     best = min(timed.items(), key=lambda kv: kv[1])
     if best[1] > (1 - min_gain) * timed[(0, 0)]:

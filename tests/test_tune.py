@@ -56,3 +56,40 @@ def test_flag_encoding_matches_header():
     # columns per CTA 1, 2, 4 -> field values 1, 2, 3 in bits 29-30
     assert [_lib.flag_variant(col_cta=c) >> 29 for c in (0, 1, 2, 4)] == [0, 1, 2, 3]
     assert _lib.flag_variant(pdl=1) == _lib.FLAG_PDL
+
+
+def test_refine_keeps_defaults_unless_clearly_faster(monkeypatch):
+    """Second stage: (columns per CTA, programmatic launch) is taken from whole-step
+    timings only when at least 1 % faster than the defaults; choices whose launch equals
+    one timed already (same column-kernel threads) are not timed again. The timings are
+    faked, so this runs without a GPU."""
+    calls = []
+
+    def fake(times, threads):
+        def _time_blocks(nx, ny, precision, model, variant, batch, steps=320, skip=None):
+            key = (variant["col_cta"], variant["pdl"])
+            th = threads[variant["col_cta"]]
+            if skip is not None and skip(th):
+                return None, th
+            calls.append(key)
+            return times[key], th
+        return _time_blocks
+
+    base = {"ee_row": 32, "ee_col": 16, "row_tile": 8}
+    # 256 threads by default (2 columns of 128); 4 columns clamp to the same launch
+    threads = {0: 256, 1: 128, 2: 256, 4: 256}
+    times = {(0, 0): 40.0, (0, 1): 39.8, (1, 0): 45.0, (1, 1): 47.0}
+    monkeypatch.setattr(tune, "_time_blocks", fake(times, threads))
+    r = tune.refine(2048, 2048, "fp32", "std", base)
+    assert (r["col_cta"], r["pdl"]) == (0, 0)            # 0.5 % faster is not enough
+    # 2 and 4 columns per CTA launch like the default here: skipped, not timed
+    assert calls == [(0, 0), (0, 1), (1, 0), (1, 1)]
+    assert set(r["refine_us"]) == {"0/0", "0/1", "1/0", "1/1"}
+    calls.clear()
+    times = {(0, 0): 12.0, (0, 1): 11.5, (1, 0): 9.4, (1, 1): 8.6}
+    monkeypatch.setattr(tune, "_time_blocks", fake(times, {0: 256, 1: 128, 2: 256, 4: 256}))
+    r = tune.refine(128, 128, "fp32", "std", base)
+    assert (r["col_cta"], r["pdl"]) == (1, 1)
+    # a grid the fast kernels do not cover keeps the defaults
+    monkeypatch.setattr(tune, "_time_blocks", lambda *a, **k: (None, None))
+    assert tune.refine(96, 96, "fp32", "std", base) == {"col_cta": 0, "pdl": 0}
