@@ -211,6 +211,20 @@ int pfc_batch_classes(pfc_batch* batch);
  * plan. Stream-ordered. */
 int pfc_field_mean_noalloc(const double* dev_field, int64_t count, double* dev_mean, void* stream);
 
+/* Vacancy tracking on the device: for each of `count` vacancies, the position that
+ * _VacancyTracker.LocateVacancy (src/pfc_models/analysis/vacancy_tracker.py:22-60)
+ * computes from a local (coarse-grained) density field, so that a tracker needs no
+ * copy of the field to the host. dev_field: ny x nx FP64, row-major, the layout
+ * pfc_get_field writes (e.g. PFC_FIELD_LOCAL_N). dev_xy: 2*count doubles (x, y) in
+ * length units (pixel * dx, pixel * dy), read as the previous positions and
+ * overwritten with the new ones. dev_status: count int32, 0 = located; where the
+ * reference raises, the position is left as it was and the status is 1 for its
+ * ValueError (a non-finite position, a 3 x 3 neighbourhood that NumPy slicing leaves
+ * empty) or 2 for its IndexError (a cross neighbour past the last row or column). Bit-identical to the reference's FP64 arithmetic. Needs no plan,
+ * allocates nothing, stream-ordered. */
+int pfc_locate_vacancies(const double* dev_field, int32_t nx, int32_t ny, double dx, double dy, double* dev_xy,
+                         int32_t count, int32_t* dev_status, void* stream);
+
 /* Copies the last error message of this thread into buf (NUL-terminated). */
 int pfc_last_error(char* buf, size_t len);
 

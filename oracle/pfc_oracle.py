@@ -198,3 +198,54 @@ def run(model, params: Params, geom: Geometry, field0, steps, record_every=None)
         if s < steps:
             sim.step()
     return sim.n, rec
+
+
+# ---------------------------------------------------------------- vacancy tracking
+def _np_index(i: int, n: int) -> int:
+    """An integer index on an axis of length n as NumPy reads it: negative counts from
+    the end, out of range raises IndexError."""
+    j = i + n if i < 0 else i
+    if j < 0 or j >= n:
+        raise IndexError(f"index {i} is out of bounds for axis with size {n}")
+    return j
+
+
+def _np_slice(start: int, stop: int, n: int) -> range:
+    """range(*slice(start, stop).indices(n)) for a unit step, as NumPy slices an axis."""
+    return range(*slice(start, stop).indices(n))
+
+
+def locate_vacancy(local: np.ndarray, x0: float, y0: float, dx: float, dy: float):
+    """analysis/vacancy_tracker.py:22-60 (_VacancyTracker.LocateVacancy), restated with
+    the index rules spelled out: the nearest pixel of (x0, y0) by round-half-to-even,
+    the first minimum (row-major) of the 3 x 3 neighbourhood as a NumPy slice cuts it
+    (negative starts wrap, stops clip; an empty slice raises ValueError), the parabolic
+    sub-pixel step along each axis from the 5-point cross (zero denominator: no step;
+    index -1 wraps, one past the end raises IndexError). Returns (x, y)."""
+    if not (np.isfinite(x0) and np.isfinite(y0)):
+        raise ValueError("cannot convert a non-finite position to a pixel")
+    ny_, nx_ = local.shape
+    px = int(np.round(x0 / dx))
+    py = int(np.round(y0 / dy))
+    rows = _np_slice(py - 1, py + 2, ny_)
+    cols = _np_slice(px - 1, px + 2, nx_)
+    if len(rows) == 0 or len(cols) == 0:
+        raise ValueError("attempt to get argmin of an empty sequence")
+    best, bi, bj = None, 0, 0
+    for i, r in enumerate(rows):
+        for j, c in enumerate(cols):
+            v = local[r, c]
+            if best is None or (np.isnan(v) and not np.isnan(best)) or (not np.isnan(best) and v < best):
+                best, bi, bj = v, i, j
+    py += bi - 1
+    px += bj - 1
+    f_mid = local[_np_index(py, ny_), _np_index(px, nx_)]
+    f_left = local[_np_index(py, ny_), _np_index(px - 1, nx_)]
+    f_right = local[_np_index(py, ny_), _np_index(px + 1, nx_)]
+    f_up = local[_np_index(py - 1, ny_), _np_index(px, nx_)]
+    f_down = local[_np_index(py + 1, ny_), _np_index(px, nx_)]
+    denom_x = 2.0 * (f_left - 2.0 * f_mid + f_right)
+    delta_x = (f_left - f_right) / denom_x if denom_x != 0 else 0.0
+    denom_y = 2.0 * (f_up - 2.0 * f_mid + f_down)
+    delta_y = (f_up - f_down) / denom_y if denom_y != 0 else 0.0
+    return (float(px + delta_x) * dx, float(py + delta_y) * dy)

@@ -54,6 +54,7 @@ SIGNATURES = {
     "pfc_batch_destroy": (ctypes.c_int, [_vp]),
     "pfc_batch_launch_count": (_i64, [_vp]),
     "pfc_batch_classes": (ctypes.c_int, [_vp]),
+    "pfc_locate_vacancies": (ctypes.c_int, [_vp, _i32, _i32, _dbl, _dbl, _vp, _i32, _vp, _vp]),
 }
 
 

@@ -1288,3 +1288,17 @@ extern "C" int pfc_field_mean_noalloc(const double* dev_field, int64_t count, do
   PFC_LAUNCHED();
   return PFC_OK;
 }
+
+extern "C" int pfc_locate_vacancies(const double* dev_field, int32_t nx, int32_t ny, double dx, double dy,
+                                    double* dev_xy, int32_t count, int32_t* dev_status, void* stream) {
+  if (count < 0) return fail(PFC_E_ARG, "pfc_locate_vacancies: count %d < 0", count);
+  if (nx < 1 || ny < 1) return fail(PFC_E_ARG, "pfc_locate_vacancies: grid %d x %d", nx, ny);
+  if (!(dx > 0.0) || !(dy > 0.0) || !std::isfinite(dx) || !std::isfinite(dy))
+    return fail(PFC_E_ARG, "pfc_locate_vacancies: spacings dx = %g, dy = %g must be finite and > 0", dx, dy);
+  if (count == 0) return PFC_OK;
+  if (!dev_field || !dev_xy || !dev_status) return fail(PFC_E_ARG, "pfc_locate_vacancies: null pointer");
+  cudaError_t e = launch_locate_vacancies(dev_field, nx, ny, dx, dy, dev_xy, count, dev_status,
+                                          static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return fail(PFC_E_CUDA, "pfc_locate_vacancies: launch failed: %s", cudaGetErrorString(e));
+  return PFC_OK;
+}

@@ -2,7 +2,10 @@
 // several .cu files (one per precision and variant) that compile in parallel; the
 // plan code finds them through these functions.
 #pragma once
+#include <cstdint>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 namespace pfc {
 
@@ -35,5 +38,9 @@ struct GenericInst {
   static void* row(int mode, int model, int rset);
   static void* col(int mode, int rset);
 };
+
+// Vacancy location on a local density field (pfc_track.cu), count > 0.
+cudaError_t launch_locate_vacancies(const double* field, int nx, int ny, double dx, double dy, double* xy,
+                                    int count, int32_t* status, cudaStream_t stream);
 
 }  // namespace pfc
