@@ -211,6 +211,24 @@ int pfc_batch_classes(pfc_batch* batch);
  * plan. Stream-ordered. */
 int pfc_field_mean_noalloc(const double* dev_field, int64_t count, double* dev_mean, void* stream);
 
+/* 3-mode fitness diagnostics of a crystal, on the device: what the phase-diagram
+ * adapters' `diagnose` computes (src/pfc_models/models/stdpfc_cpu/phase_diagram.py:178-215;
+ * logpfc_cpu/phase_diagram.py has the same code). dev_field: the plan's n (ny x nx FP64,
+ * as pfc_get_state writes it); dev_spectrum: its rfft2 (as pfc_get_spectrum writes
+ * PFC_SPEC_N_HAT_NOW). mode_rc: host, n_modes (row, col) index pairs into the half
+ * spectrum, already scaled to the box (NumPy indexing: negative values count from the
+ * end), mode_set: host, n_modes set numbers 0, 1, 2 (the 1-, 2- and 3-mode sets);
+ * amplitude_sign: the structure's amplitudeSign. Writes 6 doubles to dev_out6:
+ * fitness = 1 - |mean((n - n3)^2)| with n3 the field rebuilt from the mean and the set
+ * amplitudes, |A|, |B|, |C| (NaN-skipping mean of |n_hat| over each set, per site),
+ * the mean, and the number of strict local maxima over the 8 periodic neighbours.
+ * n_modes <= 64; a pair outside the half spectrum returns PFC_E_ARG (the reference
+ * raises IndexError). Uses the plan's reduction scratch: one call at a time per plan.
+ * Allocates nothing, stream-ordered. */
+int pfc_diagnose_modes(pfc_plan* plan, const double* dev_field, const double* dev_spectrum, const int32_t* mode_rc,
+                       const int32_t* mode_set, int32_t n_modes, double amplitude_sign, double* dev_out6,
+                       void* stream);
+
 /* Vacancy tracking on the device: for each of `count` vacancies, the position that
  * _VacancyTracker.LocateVacancy (src/pfc_models/analysis/vacancy_tracker.py:22-60)
  * computes from a local (coarse-grained) density field, so that a tracker needs no

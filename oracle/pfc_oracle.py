@@ -249,3 +249,34 @@ def locate_vacancy(local: np.ndarray, x0: float, y0: float, dx: float, dy: float
     denom_y = 2.0 * (f_up - 2.0 * f_mid + f_down)
     delta_y = (f_up - f_down) / denom_y if denom_y != 0 else 0.0
     return (float(px + delta_x) * dx, float(py + delta_y) * dy)
+
+
+# ---------------------------------------------------------------- 3-mode diagnostics
+def diagnose_modes(n: np.ndarray, mode_sets, amplitude_sign: float, cells: int):
+    """models/stdpfc_cpu/phase_diagram.py:178-215 (`_build3Mode`, `_calcFitness`,
+    `_maxima_per_cell`; logpfc_cpu/phase_diagram.py has the same code): amplitudes A, B, C
+    = sign * NaN-skipping mean of |rfft2(n)| over each set of (row, col) half-spectrum
+    indices, per site; fitness = 1 - |mean((n - n3)^2)| with n3 the inverse rfft of the
+    spectrum holding n_hat(0, 0) at DC and the set amplitudes times the site count at the
+    set indices (later sets overwrite earlier ones); maxima per cell = the strict
+    8-neighbour periodic maxima over `cells` cells. Returns
+    (fitness, |A|, |B|, |C|, maxima per cell); raises IndexError for an index outside the
+    half spectrum, as the reference does."""
+    ny, nx = n.shape
+    size = n.size
+    n_hat = np.fft.rfft2(n)
+    amps = []
+    for rows, cols in mode_sets:
+        amps.append(amplitude_sign * np.nanmean(np.abs(n_hat[rows, cols])) / size)
+    rebuilt = np.zeros_like(n_hat)
+    rebuilt[0, 0] = n_hat.flat[0] / size * size
+    for (rows, cols), a in zip(mode_sets, amps):
+        rebuilt[rows, cols] = a * size
+    n3 = np.fft.irfftn(rebuilt, s=(ny, nx), axes=(0, 1)).real
+    fitness = 1 - float(np.abs(np.power(n - n3, 2).mean()))
+    is_max = np.ones(n.shape, dtype=bool)
+    for dy in (-1, 0, 1):
+        for dx in (-1, 0, 1):
+            if dy or dx:
+                is_max &= n > np.roll(n, (dy, dx), axis=(0, 1))
+    return fitness, abs(amps[0]), abs(amps[1]), abs(amps[2]), int(is_max.sum()) / cells

@@ -55,6 +55,7 @@ SIGNATURES = {
     "pfc_batch_launch_count": (_i64, [_vp]),
     "pfc_batch_classes": (ctypes.c_int, [_vp]),
     "pfc_locate_vacancies": (ctypes.c_int, [_vp, _i32, _i32, _dbl, _dbl, _vp, _i32, _vp, _vp]),
+    "pfc_diagnose_modes": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _dbl, _vp, _vp]),
 }
 
 

@@ -1,0 +1,139 @@
+// 3-mode fitness diagnostics of a crystal field on the device: the quantities the
+// reference's phase-diagram adapters compute in `diagnose`
+// (src/pfc_models/models/stdpfc_cpu/phase_diagram.py:178-215, the same code in
+// logpfc_cpu/phase_diagram.py:182-240): the mean |n_hat| over each of three sets of mode
+// indices (the amplitudes A, B, C), the mean squared deviation of n from the field those
+// amplitudes and the mean rebuild (`_build3Mode`), and the count of strict local maxima
+// over the 8 periodic neighbours (`_maxima_per_cell`).
+//
+// The reference rebuilds the 3-mode field with an inverse FFT and subtracts it in real
+// space. Here the deviation comes from Parseval instead: the rebuilt field's spectrum is
+// non-zero only at the DC entry and the mode entries, so
+//   mean((n - n3)^2) = mean(n^2) - sum_e w_e (|n_hat_e|^2 - |n_hat_e - V_e|^2) / N^2
+// over those entries e (w_e = 1 in the DC and Nyquist columns of the half spectrum, 2
+// elsewhere; V_e the rebuilt value there). One pass over the field gives mean(n^2)
+// (compensated) and the maxima count; a one-warp kernel gathers the entries.
+#include <cmath>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "pfc_kernels.cuh"
+#include "pfc_registry.h"
+
+namespace pfc {
+namespace {
+
+constexpr int kDiagBlocks = 256, kDiagThreads = 256;
+
+// Compensated merge of n (s, c) pairs at p[stride * b] by one warp; lane 0 holds the total.
+__device__ KSum diag_warp_merge(const double* p, int n, int stride) {
+  const int lane = threadIdx.x & 31;
+  KSum acc = {0.0, 0.0};
+  for (int b = lane; b < n; b += 32) acc = ksum_merge(acc, KSum{p[(size_t)stride * b], p[(size_t)stride * b + 1]});
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    KSum o;
+    o.s = __shfl_down_sync(0xffffffffu, acc.s, off);
+    o.c = __shfl_down_sync(0xffffffffu, acc.c, off);
+    acc = ksum_merge(acc, o);
+  }
+  return acc;
+}
+
+// Per CTA: compensated sum of n^2 (2 doubles) and the count of strict periodic
+// 8-neighbour maxima (as a double, exact below 2^53), at partials[4 * blockIdx.x].
+__global__ void __launch_bounds__(kDiagThreads) diag_field_kernel(const double* __restrict__ f, int nx, int ny,
+                                                                   double* __restrict__ partials) {
+  KSum acc[1] = {{0.0, 0.0}};
+  unsigned long long count = 0;
+  const size_t n = (size_t)nx * ny;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double v = f[i];
+    ksum_add(acc[0], v * v);
+    const int x = (int)(i % nx), y = (int)(i / nx);
+    const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+    const double* rm = f + (size_t)ym * nx;
+    const double* r0 = f + (size_t)y * nx;
+    const double* rp = f + (size_t)yp * nx;
+    const bool is_max = v > rm[xm] && v > rm[x] && v > rm[xp] && v > r0[xm] && v > r0[xp] && v > rp[xm] &&
+                        v > rp[x] && v > rp[xp];
+    count += is_max ? 1 : 0;
+  }
+  // integer counts: any summation order is exact
+  __shared__ unsigned long long red[kDiagThreads / 32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) count += __shfl_down_sync(0xffffffffu, count, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = count;
+  block_reduce_store<1>(acc, partials + 4 * blockIdx.x);   // synchronises the CTA
+  if (threadIdx.x == 0) {
+    unsigned long long c = 0;
+    for (int w = 0; w < kDiagThreads / 32; ++w) c += red[w];
+    partials[4 * blockIdx.x + 2] = (double)c;
+  }
+}
+
+// out6 = {fitness, |A|, |B|, |C|, mean, maxima count}
+__global__ void diag_finalize_kernel(const double* __restrict__ partials, int nb, const double* __restrict__ spec,
+                                     DiagModes m, double n_sites, double* __restrict__ out6) {
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  const KSum sq = diag_warp_merge(partials, nb, 4);
+  if (threadIdx.x != 0) return;
+  double count = 0.0;
+  for (int b = 0; b < nb; ++b) count += partials[4 * b + 2];
+  const double mean_sq = (sq.s + sq.c) / n_sites;
+  // amplitudes: NaN-skipping mean of |n_hat| over each set's entries (duplicates count),
+  // signed, per site
+  double amp[3];
+  for (int s = 0; s < 3; ++s) {
+    double sum = 0.0;
+    int cnt = 0;
+    for (int e = 0; e < m.n_list; ++e) {
+      if (m.list_set[e] != s) continue;
+      const double re = spec[2 * (size_t)m.list_flat[e]], im = spec[2 * (size_t)m.list_flat[e] + 1];
+      const double a = hypot(re, im);
+      if (isnan(a)) continue;
+      sum += a;
+      ++cnt;
+    }
+    amp[s] = cnt ? (m.sign * (sum / cnt)) / n_sites : NAN;
+  }
+  // the rebuilt spectrum V at the distinct entries; the DC entry carries n_hat(0, 0)
+  double corr = 0.0;
+  for (int e = 0; e < m.n_uniq; ++e) {
+    const double re = spec[2 * (size_t)m.uniq_flat[e]], im = spec[2 * (size_t)m.uniq_flat[e] + 1];
+    double vr, vi;
+    if (m.uniq_set[e] < 0) {
+      vr = spec[0];
+      vi = spec[1];
+    } else {
+      vr = amp[m.uniq_set[e]] * n_sites;
+      vi = 0.0;
+    }
+    const double dr = re - vr, di = im - vi;
+    corr += m.uniq_w[e] * ((re * re + im * im) - (dr * dr + di * di));
+  }
+  const double dev = mean_sq - corr / (n_sites * n_sites);
+  out6[0] = 1.0 - fabs(dev);
+  out6[1] = fabs(amp[0]);
+  out6[2] = fabs(amp[1]);
+  out6[3] = fabs(amp[2]);
+  out6[4] = spec[0] / n_sites;
+  out6[5] = count;
+}
+
+}  // namespace
+
+cudaError_t launch_diagnose_modes(const double* field, const double* spec, int nx, int ny, const DiagModes& m,
+                                  double* partials, double* out6, cudaStream_t stream) {
+  diag_field_kernel<<<kDiagBlocks, kDiagThreads, 0, stream>>>(field, nx, ny, partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  diag_finalize_kernel<<<1, 32, 0, stream>>>(partials, kDiagBlocks, spec, m, (double)nx * (double)ny, out6);
+  return cudaGetLastError();
+}
+
+int diagnose_partials_needed() { return 4 * kDiagBlocks; }
+
+}  // namespace pfc

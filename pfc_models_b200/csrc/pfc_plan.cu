@@ -1302,3 +1302,55 @@ extern "C" int pfc_locate_vacancies(const double* dev_field, int32_t nx, int32_t
   if (e != cudaSuccess) return fail(PFC_E_CUDA, "pfc_locate_vacancies: launch failed: %s", cudaGetErrorString(e));
   return PFC_OK;
 }
+
+extern "C" int pfc_diagnose_modes(pfc_plan* h, const double* dev_field, const double* dev_spectrum,
+                                  const int32_t* mode_rc, const int32_t* mode_set, int32_t n_modes,
+                                  double amplitude_sign, double* dev_out6, void* stream) {
+  if (!h) return fail(PFC_E_ARG, "pfc_diagnose_modes: null plan");
+  if (!dev_field || !dev_spectrum || !dev_out6) return fail(PFC_E_ARG, "pfc_diagnose_modes: null device pointer");
+  if (n_modes < 0 || n_modes > kDiagMaxModes)
+    return fail(PFC_E_ARG, "pfc_diagnose_modes: %d modes (0 .. %d)", n_modes, kDiagMaxModes);
+  if (n_modes > 0 && (!mode_rc || !mode_set)) return fail(PFC_E_ARG, "pfc_diagnose_modes: null mode table");
+  if (h->npartials < (size_t)diagnose_partials_needed())
+    return fail(PFC_E_STATE, "pfc_diagnose_modes: plan scratch too small");
+  const int nx = h->nx, ny = h->ny, nxh = nx / 2 + 1;
+  DiagModes m{};
+  m.sign = amplitude_sign;
+  // the rebuilt spectrum as _build3Mode assigns it: the DC entry, then the 1-, 2- and
+  // 3-mode sets in turn, a later assignment to an entry replacing an earlier one
+  m.uniq_flat[0] = 0;
+  m.uniq_set[0] = -1;
+  m.uniq_w[0] = 1.0;
+  m.n_uniq = 1;
+  for (int s = 0; s < 3; ++s)
+    for (int i = 0; i < n_modes; ++i) {
+      if (mode_set[i] < 0 || mode_set[i] > 2)
+        return fail(PFC_E_ARG, "pfc_diagnose_modes: mode %d has set %d (0, 1 or 2)", i, mode_set[i]);
+      if (mode_set[i] != s) continue;
+      const int r = mode_rc[2 * i], c = mode_rc[2 * i + 1];
+      const int rw = r < 0 ? r + ny : r, cw = c < 0 ? c + nxh : c;
+      if (rw < 0 || rw >= ny || cw < 0 || cw >= nxh)
+        return fail(PFC_E_ARG, "pfc_diagnose_modes: mode (%d, %d) lies outside the %d x %d half spectrum", r, c, ny,
+                    nxh);
+      const int flat = rw * nxh + cw;
+      int e = 0;
+      while (e < m.n_uniq && m.uniq_flat[e] != flat) ++e;
+      if (e == m.n_uniq) {
+        m.uniq_flat[e] = flat;
+        m.uniq_w[e] = (cw == 0 || (nx % 2 == 0 && cw == nx / 2)) ? 1.0 : 2.0;
+        ++m.n_uniq;
+      }
+      m.uniq_set[e] = s;
+    }
+  // the entries each set's amplitude averages, repeats included, in the given order
+  for (int i = 0; i < n_modes; ++i) {
+    const int r = mode_rc[2 * i], c = mode_rc[2 * i + 1];
+    m.list_flat[i] = (r < 0 ? r + ny : r) * nxh + (c < 0 ? c + nxh : c);
+    m.list_set[i] = mode_set[i];
+  }
+  m.n_list = n_modes;
+  cudaError_t e = launch_diagnose_modes(dev_field, dev_spectrum, nx, ny, m, h->partials, dev_out6,
+                                        static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return fail(PFC_E_CUDA, "pfc_diagnose_modes: launch failed: %s", cudaGetErrorString(e));
+  return PFC_OK;
+}

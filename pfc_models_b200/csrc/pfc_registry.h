@@ -39,6 +39,23 @@ struct GenericInst {
   static void* col(int mode, int rset);
 };
 
+// Mode entries of the 3-mode diagnostics (pfc_diag.cu), built on the host from the
+// reference's k-vector sets: the list (with repeats) whose |n_hat| each set averages,
+// and the distinct entries of the rebuilt spectrum with their half-spectrum weights
+// (set -1: the DC entry, which keeps n_hat(0, 0)). Indices are flat in the
+// (ny, nx / 2 + 1) half spectrum.
+constexpr int kDiagMaxModes = 64;
+struct DiagModes {
+  double sign;
+  int n_list, n_uniq;
+  int list_flat[kDiagMaxModes], list_set[kDiagMaxModes];
+  int uniq_flat[kDiagMaxModes + 1], uniq_set[kDiagMaxModes + 1];
+  double uniq_w[kDiagMaxModes + 1];
+};
+cudaError_t launch_diagnose_modes(const double* field, const double* spec, int nx, int ny, const DiagModes& m,
+                                  double* partials, double* out6, cudaStream_t stream);
+int diagnose_partials_needed();
+
 // Vacancy location on a local density field (pfc_track.cu), count > 0.
 cudaError_t launch_locate_vacancies(const double* field, int nx, int ny, double dx, double dy, double* xy,
                                     int count, int32_t* status, cudaStream_t stream);

@@ -1,0 +1,104 @@
+"""3-mode crystal diagnostics on the device, for the phase-diagram adapters.
+
+`diagnose(sim, structure, cell)` returns what the reference adapters' `diagnose`
+returns (src/pfc_models/models/stdpfc_cpu/phase_diagram.py:204-215, the same in
+logpfc_cpu/phase_diagram.py): `fitness` = 1 - |mean((n - n3)^2)| with n3 the field
+rebuilt from the mean and the 1-, 2- and 3-mode amplitudes, `amplitudes` = (|A|, |B|,
+|C|) (mean |n_hat| over each mode set, per site) and `details['maxima_per_cell']` (strict
+8-neighbour periodic maxima per rectangular cell). The reference copies the field to
+the host, runs an FFT, rebuilds n3 with an inverse FFT and compares in real space; here
+`pfc_diagnose_modes` works on the plan's device field and spectrum (one pass over the
+field, the deviation by Parseval over the few rebuilt entries) and 48 bytes come back.
+
+`STRUCTURES` holds the reference's mode tables (phase_diagram.py:57-92): the lattice's
+1-, 2- and 3-mode k-vectors as (row, col) indices of one rectangular cell's half
+spectrum, the sign of the amplitudes and the ansatz scale; the values are those of the
+lattices, kept identical so that the same `structure` names select the same modes.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+
+@dataclass(frozen=True)
+class Structure:
+    name: str
+    kvectors: tuple
+    amplitudeSign: int
+    amplitudeScale: float
+    maxima_per_cell: int | None
+
+
+_TRI_MODES = (((1, 1), (2, 0), (-2, 0), (-1, 1)), ((0, 2), (3, 1), (-3, 1)), ((2, 2), (4, 0), (-4, 0), (-2, 2)))
+STRUCTURES = {
+    "triangle": Structure("triangle", _TRI_MODES, +1, 1.0 / 3, 2),
+    "honeycomb": Structure("honeycomb", _TRI_MODES, -1, 1.0 / 3, 4),
+    "stripe": Structure("stripe", (((2, 0), (-2, 0)), ((4, 0), (-4, 0)), ((6, 0), (-6, 0))), +1, 1.0 / 2, None),
+}
+_CELL_KEYS = ("uNx", "uNy", "Mx", "My")
+
+
+@dataclass
+class Diagnostics:
+    """Fields of the reference's phase_diagram.q0star.Diagnostics."""
+    fitness: float
+    amplitudes: tuple
+    details: dict = field(default_factory=dict)
+
+
+def _structure(structure):
+    return STRUCTURES[structure] if isinstance(structure, str) else structure
+
+
+def _cell(cell):
+    c = dict(cell)
+    if sorted(c) != sorted(_CELL_KEYS):
+        raise ValueError(f"cell needs exactly {list(_CELL_KEYS)}, got {sorted(c)}")
+    out = {}
+    for k in _CELL_KEYS:
+        v = c[k]
+        if int(v) != v or int(v) < 1:
+            raise ValueError(f"cell {k}={v!r} must be a positive integer")
+        out[k] = int(v)
+    return out
+
+
+def mode_table(structure, cell):
+    """(rows, cols, sets) int32 arrays of the structure's mode indices scaled to the box
+    (row * My, col * Mx), in set order."""
+    st, c = _structure(structure), _cell(cell)
+    rows, cols, sets = [], [], []
+    for s, pos in enumerate(st.kvectors):
+        for r, q in pos:
+            rows.append(r * c["My"])
+            cols.append(q * c["Mx"])
+            sets.append(s)
+    return (np.array(rows, dtype=np.int32), np.array(cols, dtype=np.int32), np.array(sets, dtype=np.int32))
+
+
+def diagnose(sim, structure, cell):
+    """The adapters' `diagnose` on the device (see the module docstring)."""
+    import torch
+    st, c = _structure(structure), _cell(cell)
+    plan = sim.plan
+    rows, cols, sets = mode_table(st, c)
+    rc = np.ascontiguousarray(np.stack([rows, cols], axis=1).ravel(), dtype=np.int32)
+    f = plan.get_state()
+    spec = plan.get_spectrum(_lib.SPEC_N_HAT_NOW)
+    out = torch.empty(6, dtype=torch.float64, device=f.device)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(f.device).cuda_stream)
+    rc_err = plan.lib.pfc_diagnose_modes(plan.handle, ctypes.c_void_p(f.data_ptr()),
+                                         ctypes.c_void_p(spec.data_ptr()), rc.ctypes.data_as(ctypes.c_void_p),
+                                         sets.ctypes.data_as(ctypes.c_void_p), int(len(sets)),
+                                         float(st.amplitudeSign), ctypes.c_void_p(out.data_ptr()), stream)
+    if rc_err == _lib.PFC_E_ARG and "outside" in _lib.last_error():
+        raise IndexError(_lib.last_error())
+    _lib.check(rc_err)
+    v = out.cpu().tolist()
+    return Diagnostics(fitness=v[0], amplitudes=(v[1], v[2], v[3]),
+                       details={"maxima_per_cell": v[5] / (c["Mx"] * c["My"]), "mean": v[4]})
