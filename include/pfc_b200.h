@@ -229,6 +229,16 @@ int pfc_diagnose_modes(pfc_plan* plan, const double* dev_field, const double* de
                        const int32_t* mode_set, int32_t n_modes, double amplitude_sign, double* dev_out6,
                        void* stream);
 
+/* Frozen-field moments of a logPFC field, on the device: what FrozenField
+ * (src/pfc_models/models/logpfc_cpu/phase_diagram.py:465-505) computes for frozen_q.
+ * dev_field / dev_spectrum as for pfc_diagnose_modes; lx_ref, ly_ref: the q00 = 1 box of the
+ * cell (Mx 4 pi / sqrt 3, My 4 pi). Writes 4 doubles to dev_out4: A_n = sum over the full
+ * fft2 grid of |phi_hat_k / N|^2 |k_ref|^(2n), n = 0, 1, 2, and the local term
+ * mean(phi ln phi + temp/2 phi^2 + g/3 phi^3 + v0/4 phi^4). Uses the plan's reduction
+ * scratch: one call at a time per plan. Allocates nothing, stream-ordered. */
+int pfc_frozen_moments(pfc_plan* plan, const double* dev_field, const double* dev_spectrum, double lx_ref,
+                       double ly_ref, double temp, double g, double v0, double* dev_out4, void* stream);
+
 /* Vacancy tracking on the device: for each of `count` vacancies, the position that
  * _VacancyTracker.LocateVacancy (src/pfc_models/analysis/vacancy_tracker.py:22-60)
  * computes from a local (coarse-grained) density field, so that a tracker needs no

@@ -280,3 +280,24 @@ def diagnose_modes(n: np.ndarray, mode_sets, amplitude_sign: float, cells: int):
             if dy or dx:
                 is_max &= n > np.roll(n, (dy, dx), axis=(0, 1))
     return fitness, abs(amps[0]), abs(amps[1]), abs(amps[2]), int(is_max.sum()) / cells
+
+
+# ---------------------------------------------------------------- frozen field (frozen_q)
+def frozen_moments(phi: np.ndarray, temp: float, g: float, v0: float, cell: dict):
+    """models/logpfc_cpu/phase_diagram.py:465-505 (`_k2_ref`, `FrozenField.__init__`):
+    A_n = sum_k |fft2(phi)_k / N|^2 |k_ref|^(2n), n = 0, 1, 2, on the full FFT grid of the
+    q00 = 1 box (Lx = Mx 4 pi / sqrt 3, Ly = My 4 pi), and the local term
+    mean(phi ln phi + temp/2 phi^2 + g/3 phi^3 + v0/4 phi^4). Returns (A, local)."""
+    phi = np.asarray(phi, dtype=float)
+    ny, nx = phi.shape
+    N = phi.size
+    P = np.abs(np.fft.fft2(phi)) ** 2 / N ** 2
+    Lx = cell['Mx'] * 4 * np.pi / np.sqrt(3.0)
+    Ly = cell['My'] * 4 * np.pi
+    kx = 2 * np.pi * np.fft.fftfreq(nx, d=Lx / nx)
+    ky = 2 * np.pi * np.fft.fftfreq(ny, d=Ly / ny)
+    KX, KY = np.meshgrid(kx, ky)
+    K = KX ** 2 + KY ** 2
+    A = np.array([P.sum(), (P * K).sum(), (P * K * K).sum()])
+    local = float(np.mean(phi * np.log(phi) + temp / 2 * phi ** 2 + g / 3 * phi ** 3 + v0 / 4 * phi ** 4))
+    return A, local

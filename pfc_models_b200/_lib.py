@@ -56,6 +56,7 @@ SIGNATURES = {
     "pfc_batch_classes": (ctypes.c_int, [_vp]),
     "pfc_locate_vacancies": (ctypes.c_int, [_vp, _i32, _i32, _dbl, _dbl, _vp, _i32, _vp, _vp]),
     "pfc_diagnose_modes": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _dbl, _vp, _vp]),
+    "pfc_frozen_moments": (ctypes.c_int, [_vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _dbl, _vp, _vp]),
 }
 
 

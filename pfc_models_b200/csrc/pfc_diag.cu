@@ -123,7 +123,77 @@ __global__ void diag_finalize_kernel(const double* __restrict__ partials, int nb
   out6[5] = count;
 }
 
+// ---- frozen-field moments (logpfc_cpu/phase_diagram.py:465-505): per CTA, compensated
+// sums of w |X_k|^2 K^n, n = 0, 1, 2, over the half spectrum (w = 1 in the DC and Nyquist
+// columns, 2 elsewhere, so the sums equal those over the full fft2 grid), with
+// K = |k_ref|^2 from NumPy's fftfreq ordering; at partials[6 * blockIdx.x].
+constexpr int kFrozenBlocks = 128;
+
+__global__ void __launch_bounds__(kDiagThreads) frozen_spectral_kernel(const double* __restrict__ spec, int nx,
+                                                                        int ny, double fx, double fy,
+                                                                        double* __restrict__ partials) {
+  KSum acc[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+  const int nxh = nx / 2 + 1;
+  const size_t n = (size_t)ny * nxh;
+  const double two_pi = 6.283185307179586;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i / nxh), c = (int)(i % nxh);
+    const double re = spec[2 * i], im = spec[2 * i + 1];
+    const int ky_i = r <= (ny - 1) / 2 ? r : r - ny;
+    const double kx = two_pi * ((double)c * fx), ky = two_pi * ((double)ky_i * fy);
+    const double K = kx * kx + ky * ky;
+    const double w = (c == 0 || (nx % 2 == 0 && c == nx / 2)) ? 1.0 : 2.0;
+    const double wp = w * (re * re + im * im);
+    ksum_add(acc[0], wp);
+    ksum_add(acc[1], wp * K);
+    ksum_add(acc[2], wp * K * K);
+  }
+  block_reduce_store<3>(acc, partials + 6 * blockIdx.x);
+}
+
+// The local term phi ln phi + temp/2 phi^2 + g/3 phi^3 + v0/4 phi^4 summed over the field
+// (compensated), at partials[2 * blockIdx.x].
+__global__ void __launch_bounds__(kDiagThreads) frozen_local_kernel(const double* __restrict__ f, size_t n,
+                                                                     double temp, double g, double v0,
+                                                                     double* __restrict__ partials) {
+  KSum acc[1] = {{0.0, 0.0}};
+  const double ct = temp / 2, cg = g / 3, cv = v0 / 4;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double p = f[i], p2 = p * p;
+    ksum_add(acc[0], p * log(p) + ct * p2 + cg * (p2 * p) + cv * (p2 * p2));
+  }
+  block_reduce_store<1>(acc, partials + 2 * blockIdx.x);
+}
+
+// out4 = {A0, A1, A2, local}
+__global__ void frozen_finalize_kernel(const double* __restrict__ sp, const double* __restrict__ lp, int nb,
+                                       double n_sites, double* __restrict__ out4) {
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  KSum s[3];
+  for (int q = 0; q < 3; ++q) s[q] = diag_warp_merge(sp + 2 * q, nb, 6);
+  const KSum l = diag_warp_merge(lp, nb, 2);
+  if (threadIdx.x != 0) return;
+  const double n2 = n_sites * n_sites;
+  for (int q = 0; q < 3; ++q) out4[q] = (s[q].s + s[q].c) / n2;
+  out4[3] = (l.s + l.c) / n_sites;
+}
+
 }  // namespace
+
+cudaError_t launch_frozen_moments(const double* field, const double* spec, int nx, int ny, double fx, double fy,
+                                  double temp, double g, double v0, double* partials, double* out4,
+                                  cudaStream_t stream) {
+  double* sp = partials;
+  double* lp = partials + 6 * kFrozenBlocks;
+  frozen_spectral_kernel<<<kFrozenBlocks, kDiagThreads, 0, stream>>>(spec, nx, ny, fx, fy, sp);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  frozen_local_kernel<<<kFrozenBlocks, kDiagThreads, 0, stream>>>(field, (size_t)nx * ny, temp, g, v0, lp);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  frozen_finalize_kernel<<<1, 32, 0, stream>>>(sp, lp, kFrozenBlocks, (double)nx * (double)ny, out4);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_diagnose_modes(const double* field, const double* spec, int nx, int ny, const DiagModes& m,
                                   double* partials, double* out6, cudaStream_t stream) {
@@ -134,6 +204,6 @@ cudaError_t launch_diagnose_modes(const double* field, const double* spec, int n
   return cudaGetLastError();
 }
 
-int diagnose_partials_needed() { return 4 * kDiagBlocks; }
+int diagnose_partials_needed() { return 4 * kDiagBlocks > 8 * kFrozenBlocks ? 4 * kDiagBlocks : 8 * kFrozenBlocks; }
 
 }  // namespace pfc

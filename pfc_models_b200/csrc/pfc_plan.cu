@@ -1354,3 +1354,19 @@ extern "C" int pfc_diagnose_modes(pfc_plan* h, const double* dev_field, const do
   if (e != cudaSuccess) return fail(PFC_E_CUDA, "pfc_diagnose_modes: launch failed: %s", cudaGetErrorString(e));
   return PFC_OK;
 }
+
+extern "C" int pfc_frozen_moments(pfc_plan* h, const double* dev_field, const double* dev_spectrum, double lx_ref,
+                                  double ly_ref, double temp, double g, double v0, double* dev_out4, void* stream) {
+  if (!h) return fail(PFC_E_ARG, "pfc_frozen_moments: null plan");
+  if (!dev_field || !dev_spectrum || !dev_out4) return fail(PFC_E_ARG, "pfc_frozen_moments: null device pointer");
+  if (!(lx_ref > 0.0) || !(ly_ref > 0.0) || !std::isfinite(lx_ref) || !std::isfinite(ly_ref))
+    return fail(PFC_E_ARG, "pfc_frozen_moments: box %g x %g must be finite and > 0", lx_ref, ly_ref);
+  if (h->npartials < (size_t)diagnose_partials_needed())
+    return fail(PFC_E_STATE, "pfc_frozen_moments: plan scratch too small");
+  // NumPy's fftfreq(n, d = L / n) spacing: 1 / (n * d)
+  const double fx = 1.0 / (h->nx * (lx_ref / h->nx)), fy = 1.0 / (h->ny * (ly_ref / h->ny));
+  cudaError_t e = launch_frozen_moments(dev_field, dev_spectrum, h->nx, h->ny, fx, fy, temp, g, v0, h->partials,
+                                        dev_out4, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return fail(PFC_E_CUDA, "pfc_frozen_moments: launch failed: %s", cudaGetErrorString(e));
+  return PFC_OK;
+}

@@ -54,6 +54,9 @@ struct DiagModes {
 };
 cudaError_t launch_diagnose_modes(const double* field, const double* spec, int nx, int ny, const DiagModes& m,
                                   double* partials, double* out6, cudaStream_t stream);
+cudaError_t launch_frozen_moments(const double* field, const double* spec, int nx, int ny, double fx, double fy,
+                                  double temp, double g, double v0, double* partials, double* out4,
+                                  cudaStream_t stream);
 int diagnose_partials_needed();
 
 // Vacancy location on a local density field (pfc_track.cu), count > 0.

@@ -10,6 +10,10 @@ the host, runs an FFT, rebuilds n3 with an inverse FFT and compares in real spac
 `pfc_diagnose_modes` works on the plan's device field and spectrum (one pass over the
 field, the deviation by Parseval over the few rebuilt entries) and 48 bytes come back.
 
+`frozen_field(state, params, temp, cell)` returns the logPFC adapter's `FrozenField`
+(logpfc_cpu/phase_diagram.py:465-505) with its moments A_n = sum |phi_hat / N|^2 |k_ref|^2n
+and local term computed on the device (`pfc_frozen_moments`).
+
 `STRUCTURES` holds the reference's mode tables (phase_diagram.py:57-92): the lattice's
 1-, 2- and 3-mode k-vectors as (row, col) indices of one rectangular cell's half
 spectrum, the sign of the amplitudes and the ansatz scale; the values are those of the
@@ -102,3 +106,67 @@ def diagnose(sim, structure, cell):
     v = out.cpu().tolist()
     return Diagnostics(fitness=v[0], amplitudes=(v[1], v[2], v[3]),
                        details={"maxima_per_cell": v[5] / (c["Mx"] * c["My"]), "mean": v[4]})
+
+
+class FrozenField:
+    """f(q) of one field frozen on the grid while the box scale q00 = q changes
+    (models/logpfc_cpu/phase_diagram.py:476-500): f(q) = local + beta/2 (q0^4 A0 -
+    2 q0^2 q^2 A1 + q^4 A2), q_opt = q0 sqrt(A1 / A2). A and local come from the device."""
+
+    def __init__(self, A, local, beta, q0):
+        self.A = np.asarray(A, dtype=float)
+        self.local = float(local)
+        self.beta, self.q0 = float(beta), float(q0)
+
+    def f(self, q):
+        s, q0 = np.asarray(q, dtype=float) ** 2, self.q0
+        A0, A1, A2 = self.A
+        return self.local + self.beta / 2 * (q0 ** 4 * A0 - 2 * q0 ** 2 * s * A1 + s ** 2 * A2)
+
+    def q_opt(self):
+        return self.q0 * np.sqrt(self.A[1] / self.A[2])
+
+
+def _log_params(params):
+    p = dict(params)
+    unknown = sorted(set(p) - {"beta", "g", "v0", "Gamma", "q0"})
+    if unknown:
+        raise ValueError(f"unknown model parameters {unknown}")
+    missing = [k for k in ("beta", "g") if k not in p]
+    if missing:
+        raise ValueError(f"missing model parameters {missing}")
+    if float(p.get("v0", 1.0)) != 1.0:
+        raise ValueError("v0 must be 1.0 (the quartic coefficient of the models is 1)")
+    return float(p["beta"]), float(p["g"]), 1.0, float(p.get("q0", 1.0))
+
+
+def frozen_field(state, params, temp, cell):
+    """FrozenField of a logPFC field (the adapter's `frozen_field`, logpfc_cpu/
+    phase_diagram.py:503-505). `state` is a Simulation of this package (its field and
+    spectrum stay on the device) or an array of the cell's grid (copied to the device
+    into a plan of the cell's q00 = 1 box)."""
+    import torch
+    beta, g, v0, q0 = _log_params(params)
+    c = _cell(cell)
+    lx = c["Mx"] * 4 * np.pi / np.sqrt(3.0)
+    ly = c["My"] * 4 * np.pi
+    plan = getattr(state, "plan", None)
+    if plan is None:
+        from . import stdpfc
+        phi = np.asarray(state, dtype=float)
+        nx, ny = c["uNx"] * c["Mx"], c["uNy"] * c["My"]
+        if phi.shape != (ny, nx):
+            raise ValueError(f"state has shape {phi.shape}, the cell's grid is {(ny, nx)}")
+        prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=beta, q0=q0, epsilon=float(temp), g=g, dt=0.01)
+        holder = stdpfc.BuildB200_Simulation(prm, stdpfc.Build2DGeometry(nx, ny, lx, ly), precision="fp64")
+        holder.State.n[...] = phi
+        plan = holder.plan
+    f = plan.get_state()
+    spec = plan.get_spectrum(_lib.SPEC_N_HAT_NOW)
+    out = torch.empty(4, dtype=torch.float64, device=f.device)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(f.device).cuda_stream)
+    _lib.check(plan.lib.pfc_frozen_moments(plan.handle, ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(spec.data_ptr()),
+                                           float(lx), float(ly), float(temp), g, v0, ctypes.c_void_p(out.data_ptr()),
+                                           stream))
+    v = out.cpu().tolist()
+    return FrozenField(v[:3], v[3], beta, q0)

@@ -9,6 +9,12 @@ Parseval instead of an inverse FFT and a real-space difference: FP64 plan, fitne
 within 1e-12 absolute and amplitudes within 1e-11 relative; FP32-mixed plan (state
 held as an FP32 deviation), fitness within 1e-7 and amplitudes within 1e-5. The maxima
 count is an integer and must match exactly.
+
+Frozen-field moments (logpfc_cpu/phase_diagram.py:465-505) likewise: the oracle equal to
+the reference's FrozenField (tests/golden/frozen.npz, make_frozen_golden.py), the device
+moments within 1e-12 relative, and the reference test's property that f(q) equals the
+free energy of the field in the box scaled by q, here within 1e-11 through this
+package's own logPFC reduction.
 """
 import ctypes
 import math
@@ -126,3 +132,57 @@ def test_device_diagnose_raises_where_the_reference_does():
     sim = _sim(cell, (16 * 0.8, 32 * 0.8), "fp64", field)
     with pytest.raises(IndexError):
         diagnostics.diagnose(sim, "triangle", cell)
+
+
+# ---------------------------------------------------------------- frozen field
+FROZEN_CELL = dict(uNx=14, uNy=24, Mx=2, My=1)
+
+
+def test_oracle_frozen_moments_match_reference(golden):
+    d = golden("frozen")
+    for k, (beta, g, temp) in enumerate(d["params"]):
+        A, local = orc.frozen_moments(d[f"phi_{k}"], temp, g, 1.0, FROZEN_CELL)
+        assert np.array_equal(A, d[f"A_{k}"])
+        assert local == d[f"local_{k}"][0]
+
+
+def test_frozen_field_formulas_match_reference(golden):
+    d = golden("frozen")
+    for k, (beta, g, temp) in enumerate(d["params"]):
+        ff = diagnostics.FrozenField(d[f"A_{k}"], d[f"local_{k}"][0], beta, 1.0)
+        assert [float(ff.f(q)) for q in d["qs"]] == list(d[f"f_{k}"])
+        assert ff.q_opt() == d[f"qopt_{k}"][0]
+
+
+@pytest.mark.gpu
+def test_device_frozen_field_matches_reference(golden):
+    d = golden("frozen")
+    for k, (beta, g, temp) in enumerate(d["params"]):
+        ff = diagnostics.frozen_field(d[f"phi_{k}"], {"beta": beta, "g": g, "v0": 1.0}, temp, FROZEN_CELL)
+        assert ff.A == pytest.approx(d[f"A_{k}"], rel=1e-12)
+        assert ff.local == pytest.approx(d[f"local_{k}"][0], rel=1e-13)
+        assert ff.q_opt() == pytest.approx(d[f"qopt_{k}"][0], rel=1e-12)
+        assert [float(ff.f(q)) for q in d["qs"]] == pytest.approx(list(d[f"f_{k}"]), rel=1e-12)
+
+
+@pytest.mark.gpu
+def test_frozen_f_equals_free_energy_in_the_rescaled_box(golden):
+    """The reference test's property (tests/test_phase_diagram_frozen_q.py:22-34): f(q) of
+    the frozen field equals the free energy of the same field in the box scaled by q; here
+    F comes from this package's logPFC plan (its own reduction) and from the reference's
+    adapter (the fixture)."""
+    from pfc_models_b200 import logpfc
+    d = golden("frozen")
+    a, h = 4 * math.pi / math.sqrt(3), 4 * math.pi
+    for k, (beta, g, temp) in enumerate(d["params"]):
+        phi = d[f"phi_{k}"]
+        ny, nx = phi.shape
+        ff = diagnostics.frozen_field(phi, {"beta": beta, "g": g, "v0": 1.0}, temp, FROZEN_CELL)
+        for q, f_ref in zip(d["qs"], d[f"f_adapter_{k}"]):
+            prm = logpfc.BuildLogPFCModelParameters(Gamma=1.0, beta=beta, q0=1.0, epsilon=temp, g=g, dt=0.01)
+            geom = logpfc.Build2DGeometry(nx, ny, FROZEN_CELL["Mx"] * a / q, FROZEN_CELL["My"] * h / q)
+            sim = logpfc.BuildB200_Simulation(prm, geom, precision="fp64")
+            sim.State.phi[...] = phi
+            F = float(sim.CalculateFreeEnergy())
+            assert float(ff.f(q)) == pytest.approx(F, rel=1e-11, abs=1e-12)
+            assert F == pytest.approx(f_ref, rel=1e-11, abs=1e-12)
