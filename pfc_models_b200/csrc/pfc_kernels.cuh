@@ -459,41 +459,77 @@ __global__ void __launch_bounds__(LB) col_kernel(ColArgs<T> a) {
     }
     __syncthreads();
   } else if (MODE == kColStep) {
-    if (valid) {
-      const size_t cb = (size_t)kx * ny;
+    if (valid && kx == 0) {
+      const size_t cb = 0;
       for (int ky = lt; ky <= ny / 2; ky += tpf) {
         const int kyp = ky == 0 ? 0 : ny - ky;
         const cplx<T> qkt = buf[ky], qkpt = buf[kyp];
         const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
-        cplx<double> ok, okp;
-        bool slow;
-        if (kx == 0) {
-          // the packed column holds kx = 0 (slow near ky = 0): always at full precision
-          bool s0, sM;
-          const cplx<double> c0v = coef_ld<T>(a.coef, a.coef64, ky, a.slow_tau, true, s0);
-          const cplx<double> cMv = coef_ld<T>(a.coef, a.coef64, (size_t)m * nyh + ky, a.slow_tau, true, sM);
-          slow = true;
-          const cplx<double> pk = state_ld<T>(a.nin, a.nin_lo, cb + ky, true);
-          const cplx<double> pkp = state_ld<T>(a.nin, a.nin_lo, cb + kyp, true);
-          cplx<double> h0, hm, g0, gm;
-          unpack_pair(pk, pkp, h0, hm);
-          unpack_pair(qk, qkp, g0, gm);
-          const cplx<double> h0n = h0 + c0v.x * h0 + c0v.y * g0;
-          const cplx<double> hmn = hm + cMv.x * hm + cMv.y * gm;
-          ok = h0n + mul_i(hmn);
-          okp = conj(h0n) + mul_i(conj(hmn));
-        } else {
-          const cplx<double> c = coef_ld<T>(a.coef, a.coef64, (size_t)kx * nyh + ky, a.slow_tau, false, slow);
-          const cplx<double> pk = state_ld<T>(a.nin, a.nin_lo, cb + ky, slow);
-          const cplx<double> pkp = state_ld<T>(a.nin, a.nin_lo, cb + kyp, slow);
-          ok = pk + c.x * pk + c.y * qk;
-          okp = pkp + c.x * pkp + c.y * qkp;
-        }
-        state_st<T>(a.nout, a.nout_lo, cb + ky, ok, slow);
+        // the packed column holds kx = 0 (slow near ky = 0): always at full precision
+        bool s0, sM;
+        const cplx<double> c0v = coef_ld<T>(a.coef, a.coef64, ky, a.slow_tau, true, s0);
+        const cplx<double> cMv = coef_ld<T>(a.coef, a.coef64, (size_t)m * nyh + ky, a.slow_tau, true, sM);
+        const cplx<double> pk = state_ld<T>(a.nin, a.nin_lo, cb + ky, true);
+        const cplx<double> pkp = state_ld<T>(a.nin, a.nin_lo, cb + kyp, true);
+        cplx<double> h0, hm, g0, gm;
+        unpack_pair(pk, pkp, h0, hm);
+        unpack_pair(qk, qkp, g0, gm);
+        const cplx<double> h0n = h0 + c0v.x * h0 + c0v.y * g0;
+        const cplx<double> hmn = hm + cMv.x * hm + cMv.y * gm;
+        const cplx<double> ok = h0n + mul_i(hmn);
+        const cplx<double> okp = conj(h0n) + mul_i(conj(hmn));
+        state_st<T>(a.nout, a.nout_lo, cb + ky, ok, true);
         buf[ky] = mk((T)ok.x, (T)ok.y);
         if (kyp != ky) {
-          state_st<T>(a.nout, a.nout_lo, cb + kyp, okp, slow);
+          state_st<T>(a.nout, a.nout_lo, cb + kyp, okp, true);
           buf[kyp] = mk((T)okp.x, (T)okp.y);
+        }
+      }
+    } else if (valid) {
+      // (ky, -ky) pairs in chunks of two, the coefficients and states of a chunk loaded
+      // before any of its results is stored (the compiler keeps a later pair's loads
+      // behind an earlier pair's stores); arithmetic as coef_ld / state_ld / state_st
+      constexpr int CH = 2;
+      const size_t cb = (size_t)kx * ny;
+      const cplx<T>* nin = static_cast<const cplx<T>*>(a.nin);
+      for (int ky0 = lt; ky0 <= ny / 2; ky0 += CH * tpf) {
+        cplx<T> cw[CH], ph[CH], pph[CH];
+#pragma unroll
+        for (int j = 0; j < CH; ++j) {
+          const int ky = ky0 + j * tpf;
+          if (ky <= ny / 2) {
+            const int kyp = ky == 0 ? 0 : ny - ky;
+            cw[j] = a.coef[(size_t)kx * nyh + ky];
+            ph[j] = nin[cb + ky];
+            pph[j] = nin[cb + kyp];
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < CH; ++j) {
+          const int ky = ky0 + j * tpf;
+          if (ky > ny / 2) break;
+          const int kyp = ky == 0 ? 0 : ny - ky;
+          const cplx<T> qkt = buf[ky], qkpt = buf[kyp];
+          const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
+          const bool slow = sizeof(T) == 8 || fabs((double)cw[j].x) < (double)a.slow_tau;
+          const cplx<double> c = (sizeof(T) == 4 && slow) ? a.coef64[(size_t)kx * nyh + ky]
+                                                           : mk((double)cw[j].x, (double)cw[j].y);
+          cplx<double> pk = mk((double)ph[j].x, (double)ph[j].y), pkp = mk((double)pph[j].x, (double)pph[j].y);
+          if (sizeof(T) == 4 && slow) {
+            const cplx<float> l = a.nin_lo[cb + ky], lp = a.nin_lo[cb + kyp];
+            pk.x += (double)l.x;
+            pk.y += (double)l.y;
+            pkp.x += (double)lp.x;
+            pkp.y += (double)lp.y;
+          }
+          const cplx<double> ok = pk + c.x * pk + c.y * qk;
+          const cplx<double> okp = pkp + c.x * pkp + c.y * qkp;
+          state_st<T>(a.nout, a.nout_lo, cb + ky, ok, slow);
+          buf[ky] = mk((T)ok.x, (T)ok.y);
+          if (kyp != ky) {
+            state_st<T>(a.nout, a.nout_lo, cb + kyp, okp, slow);
+            buf[kyp] = mk((T)okp.x, (T)okp.y);
+          }
         }
       }
     }

@@ -862,6 +862,11 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   cudaDeviceGetAttribute(&smem_opt, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   if (smem_opt <= 0) smem_opt = 227 * 1024;
   const int budget = std::min(smem_opt - 8 * 1024, 200 * 1024);
+  // at least two CTAs per SM where the grid allows it: larger tiles coalesce better, but
+  // on small and medium grids they left most SMs idle
+  int n_sm = 0;
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, h->device);
+  const int min_ctas = 2 * std::max(n_sm, 1);
   {
     h->row_tpf = threads_per_fft(rrow, m, h->fp32);
     h->row_ld = m + 1;
@@ -876,6 +881,7 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
     while (2 * rows <= rows_cap && (size_t)(2 * rows) * h->row_ld * cbytes <= (size_t)budget / 2 && rows < p->ny)
       rows *= 2;
     while ((size_t)rows * h->row_ld * cbytes > (size_t)budget && rows > std::max(1, 32 / h->row_tpf)) rows /= 2;
+    while (rows > rows_min && (p->ny + rows - 1) / rows < min_ctas) rows /= 2;
     if ((size_t)rows * h->row_ld * cbytes > (size_t)budget || rows * h->row_tpf > kBlockMax)
       return cleanup_fail(fail(PFC_E_ARG, "pfc_plan_create: row transform of %d points does not fit", m));
     h->rows = rows;
@@ -892,6 +898,7 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
     int cols = std::max(1, 32 / h->col_tpf);
     while (2 * cols * h->col_tpf <= kBlockMax && (size_t)(2 * cols) * h->col_ld * cbytes <= (size_t)budget / 2 && cols < m)
       cols *= 2;
+    while (cols > std::max(1, 32 / h->col_tpf) && (m + cols - 1) / cols < min_ctas) cols /= 2;
     if ((size_t)cols * h->col_ld * cbytes > (size_t)budget || cols * h->col_tpf > kBlockMax)
       return cleanup_fail(fail(PFC_E_ARG, "pfc_plan_create: column transform of %d points does not fit", p->ny));
     h->cols = cols;
