@@ -13,6 +13,12 @@ template <int MODE> constexpr bool row_uses_model() { return MODE == kRowStep ||
 template <class T, int MODE>
 void* pick_row(int model, int rset) {
   const bool log = row_uses_model<MODE>() && model == kModelLog;
+  if (rset == kRadixAllDense) {
+    if constexpr (sizeof(T) == 4 && MODE == kRowStep)
+      return log ? (void*)row_kernel<T, MODE, kModelLog, kRadixAll, 256, 2>
+                 : (void*)row_kernel<T, MODE, kModelStd, kRadixAll, 256, 2>;
+    rset = kRadixAll;
+  }
   if (rset == kRadixPow2Big)
     return log ? (void*)row_kernel<T, MODE, kModelLog, kRadixPow2, 1024>
                : (void*)row_kernel<T, MODE, kModelStd, kRadixPow2, 1024>;
@@ -25,6 +31,10 @@ void* pick_row(int model, int rset) {
 
 template <class T, int MODE>
 void* pick_col(int rset) {
+  if (rset == kRadixAllDense) {
+    if constexpr (sizeof(T) == 4 && MODE == kColStep) return (void*)col_kernel<T, MODE, kRadixAll, 256, 2>;
+    rset = kRadixAll;
+  }
   if (rset == kRadixPow2Big) return (void*)col_kernel<T, MODE, kRadixPow2, 1024>;
   if (MODE == kColParseval || MODE == kColExport || rset == kRadixPow2) return (void*)col_kernel<T, MODE, kRadixPow2, 256>;
   return (void*)col_kernel<T, MODE, kRadixAll, 256>;

@@ -230,8 +230,8 @@ __device__ __forceinline__ double ksq(int kx, int ky, int ny, double fx, double 
 
 // ---------------------------------------------------------------- row kernel
 // rows transforms of length m per CTA, tpf threads each; smem = rows * ld complex.
-template <class T, int MODE, int MODEL, int RSET, int LB = 256>
-__global__ void __launch_bounds__(LB) row_kernel(RowArgs<T> a) {
+template <class T, int MODE, int MODEL, int RSET, int LB = 256, int MINB = 1>
+__global__ void __launch_bounds__(LB, MINB) row_kernel(RowArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
   const int m = a.m, ny = a.ny, rows = a.rows, tpf = a.tpf, ld = a.ld;
@@ -384,8 +384,8 @@ __device__ __forceinline__ void unpack_pair(cplx<T> pk, cplx<T> pkp, cplx<T>& h0
 }
 
 // cols transforms of length ny per CTA, tpf threads each; smem = cols * ld complex.
-template <class T, int MODE, int RSET, int LB = 256>
-__global__ void __launch_bounds__(LB) col_kernel(ColArgs<T> a) {
+template <class T, int MODE, int RSET, int LB = 256, int MINB = 1>
+__global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
   const int ny = a.ny, m = a.m, cols = a.cols, tpf = a.tpf, ld = a.ld, nyh = a.nyh;

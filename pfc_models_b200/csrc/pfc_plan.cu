@@ -833,6 +833,10 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   h->nspec = (size_t)m * p->ny;
   h->row_rset = all_pow2(rrow) ? kRadixPow2 : kRadixAll;
   h->col_rset = all_pow2(rcol) ? kRadixPow2 : kRadixAll;
+  if (h->fp32 && (long long)p->nx * p->ny >= kDenseMinSites) {
+    if (h->row_rset == kRadixAll) h->row_rset = kRadixAllDense;
+    if (h->col_rset == kRadixAll) h->col_rset = kRadixAllDense;
+  }
   h->elt = h->fp32 ? sizeof(float2) : sizeof(double2);
   cudaGetDevice(&h->device);
 

@@ -13,6 +13,11 @@ namespace pfc {
 // transform needs more than 256 threads (>= 8192 points in FP32); kRadixPow2 and
 // kRadixAll (pfc_fft.cuh) select the 256-thread kernels.
 constexpr int kRadixPow2Big = 2;
+// The all-radix step kernels (row and column) built for two CTAs per SM (at most 128
+// registers, with some spills) instead of one: faster for large FP32 grids, slower for
+// small grids and in FP64 (measured on B200). Modes other than the step use kRadixAll.
+constexpr int kRadixAllDense = 3;
+constexpr long long kDenseMinSites = 1LL << 20;
 
 // log2 sizes of the power-of-two step kernels: row transforms of M = nx/2 points,
 // column transforms of ny points

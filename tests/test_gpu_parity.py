@@ -267,6 +267,31 @@ def test_sizes_against_oracle(nx, ny, model):
         assert rel_l2(field.get() - mean, ref - mean) < tol, precision
 
 
+@pytest.mark.parametrize("model", ["std", "log"])
+def test_large_mixed_radix_fp32_against_oracle(model):
+    """A grid of at least 2^20 sites with radices 3, 5 and 7 in FP32-mixed form runs the
+    mixed-radix step kernels built for two CTAs per SM (128 registers); 20 steps within
+    2e-5 relative L2 of the oracle, as the other sizes."""
+    nx, ny = 1120, 1008
+    geom_o = orc.build_geometry(nx, ny, nx * 0.9, ny * 0.8)
+    if model == "std":
+        prm = dict(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.25, g=0.3, dt=0.2)
+        mean = -0.2
+    else:
+        prm = dict(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=0.05)
+        mean = 0.55
+    f0 = mean + 0.05 * np.random.default_rng(11).uniform(-1, 1, (ny, nx))
+    ref, _ = orc.run(model, orc.Params(**prm), geom_o, f0, 20)
+    mod = stdpfc if model == "std" else logpfc
+    builder = mod.BuildStdPFCModelParameters if model == "std" else mod.BuildLogPFCModelParameters
+    sim = mod.BuildB200_Simulation(builder(**prm), mod.Build2DGeometry(nx, ny, nx * 0.9, ny * 0.8), precision="fp32")
+    assert sim.plan.variant()["fast"] == 0
+    field = sim.State.n if model == "std" else sim.State.phi
+    field[...] = f0
+    sim.TimeSteps(20)
+    assert rel_l2(field.get() - mean, ref - mean) < 2e-5
+
+
 # ------------------------------------------------------------------ observables and views
 def test_views_and_reductions():
     """n_hat, mu, local fields and the reductions against the oracle's definitions."""
