@@ -448,3 +448,21 @@ def test_kernel_variant_errors():
         with pytest.raises(_lib.PfcError) as e:
             stdpfc.BuildB200_Simulation(prm, geom, precision="fp32", kernels=bad)
         assert e.value.code == _lib.PFC_E_ARG
+
+
+@pytest.mark.parametrize("nx,ny", [(256, 384), (448, 448), (224, 392), (1120, 1008)])
+def test_mixed_radix_tiles_leave_no_sm_idle(nx, ny):
+    """The mixed-radix kernels' row and column tiles give at least two CTAs per SM, or are
+    already at their smallest (whole warps of rows, or the starting column count)."""
+    import torch
+    n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.25, g=0.0, dt=0.5)
+    for precision in ("fp32", "fp64"):
+        sim = stdpfc.BuildB200_Simulation(prm, stdpfc.Build2DGeometry(nx, ny, nx * 0.8, ny * 0.8), precision=precision)
+        info = sim.plan.info()
+        assert info["fast"] == 0
+        rows_min = max(1, 32 // info["row_threads_per_fft"])
+        cols_min = max(1, 32 // info["col_threads_per_fft"])
+        assert info["row_ctas"] >= 2 * n_sm or info["rows_per_cta"] == rows_min, info
+        assert info["col_ctas"] >= 2 * n_sm or info["cols_per_cta"] == cols_min, info
+        sim.plan.close()
