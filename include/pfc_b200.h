@@ -239,6 +239,18 @@ int pfc_diagnose_modes(pfc_plan* plan, const double* dev_field, const double* de
 int pfc_frozen_moments(pfc_plan* plan, const double* dev_field, const double* dev_spectrum, double lx_ref,
                        double ly_ref, double temp, double g, double v0, double* dev_out4, void* stream);
 
+/* Defect screen of a logPFC field, on the device: what defect_diagnostics
+ * (src/pfc_models/models/logpfc_cpu/phase_diagram.py:512-528) computes for frozen_q.
+ * dev_field / dev_spectrum as for pfc_diagnose_modes; lx_ref, ly_ref as for
+ * pfc_frozen_moments. Writes 4 doubles to dev_out4: the peak spread (max - min) / mean
+ * of the heights above the mean of the sites >= their 8 periodic neighbours and above
+ * the mean, the sub-q ratio (largest |phi_hat|^2 at 0 < |k_ref| < 0.95 over the largest
+ * at k != 0), the peak count, and 0; NaN where there is no peak or no power. Uses the
+ * plan's reduction scratch: one call at a time per plan. Allocates nothing,
+ * stream-ordered. */
+int pfc_defect_screen(pfc_plan* plan, const double* dev_field, const double* dev_spectrum, double lx_ref,
+                      double ly_ref, double* dev_out4, void* stream);
+
 /* Vacancy tracking on the device: for each of `count` vacancies, the position that
  * _VacancyTracker.LocateVacancy (src/pfc_models/analysis/vacancy_tracker.py:22-60)
  * computes from a local (coarse-grained) density field, so that a tracker needs no

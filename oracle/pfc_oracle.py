@@ -301,3 +301,28 @@ def frozen_moments(phi: np.ndarray, temp: float, g: float, v0: float, cell: dict
     A = np.array([P.sum(), (P * K).sum(), (P * K * K).sum()])
     local = float(np.mean(phi * np.log(phi) + temp / 2 * phi ** 2 + g / 3 * phi ** 3 + v0 / 4 * phi ** 4))
     return A, local
+
+
+def defect_screen(phi: np.ndarray, cell: dict):
+    """models/logpfc_cpu/phase_diagram.py:512-528 (`defect_diagnostics`): peak spread =
+    (max - min) / mean of the heights above the mean of the sites >= their 8 periodic
+    neighbours and above the mean; sub-q ratio = the largest |fft2(phi - mean)|^2 at
+    0 < |k_ref| < 0.95 over the largest |fft2(phi - mean)|^2; the peak count.
+    Returns (peak_spread, subq_ratio, n_peaks)."""
+    phi = np.asarray(phi, dtype=float)
+    m = phi.mean()
+    nb = [np.roll(np.roll(phi, a, 0), b, 1) for a in (-1, 0, 1) for b in (-1, 0, 1) if (a, b) != (0, 0)]
+    mask = np.all([phi >= x for x in nb], axis=0) & (phi > m)
+    h = phi[mask] - m
+    spread = float((h.max() - h.min()) / h.mean()) if h.size else float('nan')
+    P = np.abs(np.fft.fft2(phi - m)) ** 2
+    ny, nx = phi.shape
+    Lx = cell['Mx'] * 4 * np.pi / np.sqrt(3.0)
+    Ly = cell['My'] * 4 * np.pi
+    kx = 2 * np.pi * np.fft.fftfreq(nx, d=Lx / nx)
+    ky = 2 * np.pi * np.fft.fftfreq(ny, d=Ly / ny)
+    KX, KY = np.meshgrid(kx, ky)
+    kr = np.sqrt(KX ** 2 + KY ** 2)
+    sub = (kr > 1e-9) & (kr < 0.95)
+    ratio = float(P[sub].max() / P.max()) if P.max() > 0 else float('nan')
+    return spread, ratio, int(mask.sum())

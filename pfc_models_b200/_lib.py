@@ -57,6 +57,7 @@ SIGNATURES = {
     "pfc_locate_vacancies": (ctypes.c_int, [_vp, _i32, _i32, _dbl, _dbl, _vp, _i32, _vp, _vp]),
     "pfc_diagnose_modes": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _dbl, _vp, _vp]),
     "pfc_frozen_moments": (ctypes.c_int, [_vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _dbl, _vp, _vp]),
+    "pfc_defect_screen": (ctypes.c_int, [_vp, _vp, _vp, _dbl, _dbl, _vp, _vp]),
 }
 
 

@@ -178,7 +178,149 @@ __global__ void frozen_finalize_kernel(const double* __restrict__ sp, const doub
   out4[3] = (l.s + l.c) / n_sites;
 }
 
+// ---- defect screen (logpfc_cpu/phase_diagram.py:512-528). Field pass, per CTA at
+// partials[5 * b]: the count of sites >= their 8 periodic neighbours and above the mean,
+// the compensated sum of their heights above the mean (2 doubles), the largest and the
+// smallest height. The mean is the spectrum's DC entry over the site count.
+constexpr int kDefectBlocks = 128;
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, off));
+  return v;
+}
+
+__global__ void __launch_bounds__(kDiagThreads) defect_field_kernel(const double* __restrict__ f, int nx, int ny,
+                                                                     const double* __restrict__ spec,
+                                                                     double* __restrict__ partials) {
+  const double m = spec[0] / ((double)nx * (double)ny);
+  KSum acc[1] = {{0.0, 0.0}};
+  unsigned long long count = 0;
+  double hmax = -INFINITY, hmin = INFINITY;
+  const size_t n = (size_t)nx * ny;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double v = f[i];
+    if (!(v > m)) continue;
+    const int x = (int)(i % nx), y = (int)(i / nx);
+    const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+    const double* rm = f + (size_t)ym * nx;
+    const double* r0 = f + (size_t)y * nx;
+    const double* rp = f + (size_t)yp * nx;
+    if (v >= rm[xm] && v >= rm[x] && v >= rm[xp] && v >= r0[xm] && v >= r0[xp] && v >= rp[xm] && v >= rp[x] &&
+        v >= rp[xp]) {
+      const double h = v - m;
+      ksum_add(acc[0], h);
+      ++count;
+      hmax = fmax(hmax, h);
+      hmin = fmin(hmin, h);
+    }
+  }
+  __shared__ unsigned long long rc[kDiagThreads / 32];
+  __shared__ double rmax[kDiagThreads / 32], rmin[kDiagThreads / 32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) count += __shfl_down_sync(0xffffffffu, count, off);
+  hmax = warp_max(hmax);
+  hmin = warp_min(hmin);
+  if ((threadIdx.x & 31) == 0) {
+    rc[threadIdx.x >> 5] = count;
+    rmax[threadIdx.x >> 5] = hmax;
+    rmin[threadIdx.x >> 5] = hmin;
+  }
+  block_reduce_store<1>(acc, partials + 5 * blockIdx.x + 1);   // synchronises the CTA
+  if (threadIdx.x == 0) {
+    unsigned long long c = 0;
+    double mx = -INFINITY, mn = INFINITY;
+    for (int w = 0; w < kDiagThreads / 32; ++w) {
+      c += rc[w];
+      mx = fmax(mx, rmax[w]);
+      mn = fmin(mn, rmin[w]);
+    }
+    partials[5 * blockIdx.x] = (double)c;
+    partials[5 * blockIdx.x + 3] = mx;
+    partials[5 * blockIdx.x + 4] = mn;
+  }
+}
+
+// Spectral pass, per CTA at partials[2 * b]: the largest |X_k|^2 with 0 < |k_ref| < 0.95
+// and the largest over k != 0 (the mean only moves the DC entry; the half spectrum
+// holds every magnitude of the full grid).
+__global__ void __launch_bounds__(kDiagThreads) defect_spectral_kernel(const double* __restrict__ spec, int nx,
+                                                                        int ny, double fx, double fy,
+                                                                        double* __restrict__ partials) {
+  const int nxh = nx / 2 + 1;
+  const size_t n = (size_t)ny * nxh;
+  const double two_pi = 6.283185307179586;
+  double psub = 0.0, pall = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    if (i == 0) continue;
+    const int r = (int)(i / nxh), c = (int)(i % nxh);
+    const double re = spec[2 * i], im = spec[2 * i + 1];
+    const double p = re * re + im * im;
+    const int ky_i = r <= (ny - 1) / 2 ? r : r - ny;
+    const double kx = two_pi * ((double)c * fx), ky = two_pi * ((double)ky_i * fy);
+    const double kr = sqrt(kx * kx + ky * ky);
+    pall = fmax(pall, p);
+    if (kr > 1e-9 && kr < 0.95) psub = fmax(psub, p);
+  }
+  __shared__ double rs[kDiagThreads / 32], ra[kDiagThreads / 32];
+  psub = warp_max(psub);
+  pall = warp_max(pall);
+  if ((threadIdx.x & 31) == 0) {
+    rs[threadIdx.x >> 5] = psub;
+    ra[threadIdx.x >> 5] = pall;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kDiagThreads / 32; ++w) {
+      psub = fmax(psub, rs[w]);
+      pall = fmax(pall, ra[w]);
+    }
+    partials[2 * blockIdx.x] = psub;
+    partials[2 * blockIdx.x + 1] = pall;
+  }
+}
+
+// out4 = {peak spread, sub-q ratio, peak count, 0}; NaN where the reference's is NaN
+__global__ void defect_finalize_kernel(const double* __restrict__ fp, const double* __restrict__ sp, int nb,
+                                       double* __restrict__ out4) {
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  const KSum hs = diag_warp_merge(fp + 1, nb, 5);
+  if (threadIdx.x != 0) return;
+  double count = 0.0, mx = -INFINITY, mn = INFINITY, psub = 0.0, pall = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    count += fp[5 * b];
+    mx = fmax(mx, fp[5 * b + 3]);
+    mn = fmin(mn, fp[5 * b + 4]);
+    psub = fmax(psub, sp[2 * b]);
+    pall = fmax(pall, sp[2 * b + 1]);
+  }
+  out4[0] = count > 0 ? (mx - mn) / ((hs.s + hs.c) / count) : NAN;
+  out4[1] = pall > 0 ? psub / pall : NAN;
+  out4[2] = count;
+  out4[3] = 0.0;
+}
+
 }  // namespace
+
+cudaError_t launch_defect_screen(const double* field, const double* spec, int nx, int ny, double fx, double fy,
+                                 double* partials, double* out4, cudaStream_t stream) {
+  double* fp = partials;
+  double* sp = partials + 5 * kDefectBlocks;
+  defect_field_kernel<<<kDefectBlocks, kDiagThreads, 0, stream>>>(field, nx, ny, spec, fp);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  defect_spectral_kernel<<<kDefectBlocks, kDiagThreads, 0, stream>>>(spec, nx, ny, fx, fy, sp);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  defect_finalize_kernel<<<1, 32, 0, stream>>>(fp, sp, kDefectBlocks, out4);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_frozen_moments(const double* field, const double* spec, int nx, int ny, double fx, double fy,
                                   double temp, double g, double v0, double* partials, double* out4,
@@ -204,6 +346,10 @@ cudaError_t launch_diagnose_modes(const double* field, const double* spec, int n
   return cudaGetLastError();
 }
 
-int diagnose_partials_needed() { return 4 * kDiagBlocks > 8 * kFrozenBlocks ? 4 * kDiagBlocks : 8 * kFrozenBlocks; }
+// doubles of plan scratch the diagnostics use: the largest of their partial layouts
+int diagnose_partials_needed() {
+  const int a = 4 * kDiagBlocks, b = 8 * kFrozenBlocks, c = 7 * kDefectBlocks;
+  return a > b ? (a > c ? a : c) : (b > c ? b : c);
+}
 
 }  // namespace pfc

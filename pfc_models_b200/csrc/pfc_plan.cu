@@ -1381,3 +1381,18 @@ extern "C" int pfc_frozen_moments(pfc_plan* h, const double* dev_field, const do
   if (e != cudaSuccess) return fail(PFC_E_CUDA, "pfc_frozen_moments: launch failed: %s", cudaGetErrorString(e));
   return PFC_OK;
 }
+
+extern "C" int pfc_defect_screen(pfc_plan* h, const double* dev_field, const double* dev_spectrum, double lx_ref,
+                                 double ly_ref, double* dev_out4, void* stream) {
+  if (!h) return fail(PFC_E_ARG, "pfc_defect_screen: null plan");
+  if (!dev_field || !dev_spectrum || !dev_out4) return fail(PFC_E_ARG, "pfc_defect_screen: null device pointer");
+  if (!(lx_ref > 0.0) || !(ly_ref > 0.0) || !std::isfinite(lx_ref) || !std::isfinite(ly_ref))
+    return fail(PFC_E_ARG, "pfc_defect_screen: box %g x %g must be finite and > 0", lx_ref, ly_ref);
+  if (h->npartials < (size_t)diagnose_partials_needed())
+    return fail(PFC_E_STATE, "pfc_defect_screen: plan scratch too small");
+  const double fx = 1.0 / (h->nx * (lx_ref / h->nx)), fy = 1.0 / (h->ny * (ly_ref / h->ny));
+  cudaError_t e = launch_defect_screen(dev_field, dev_spectrum, h->nx, h->ny, fx, fy, h->partials, dev_out4,
+                                       static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return fail(PFC_E_CUDA, "pfc_defect_screen: launch failed: %s", cudaGetErrorString(e));
+  return PFC_OK;
+}

@@ -62,6 +62,8 @@ cudaError_t launch_diagnose_modes(const double* field, const double* spec, int n
 cudaError_t launch_frozen_moments(const double* field, const double* spec, int nx, int ny, double fx, double fy,
                                   double temp, double g, double v0, double* partials, double* out4,
                                   cudaStream_t stream);
+cudaError_t launch_defect_screen(const double* field, const double* spec, int nx, int ny, double fx, double fy,
+                                 double* partials, double* out4, cudaStream_t stream);
 int diagnose_partials_needed();
 
 // Vacancy location on a local density field (pfc_track.cu), count > 0.

@@ -140,29 +140,42 @@ def _log_params(params):
     return float(p["beta"]), float(p["g"]), 1.0, float(p.get("q0", 1.0))
 
 
+def _ref_box(c):
+    """The q00 = 1 box of a cell (Mx rectangular cells of width 4 pi / sqrt 3, My of 4 pi)."""
+    return c["Mx"] * 4 * np.pi / np.sqrt(3.0), c["My"] * 4 * np.pi
+
+
+def _field_and_spectrum(state, c):
+    """(plan, device field, device spectrum, keep-alive) of a Simulation of this package
+    (its own field and spectrum) or of an array of the cell's grid (its exact values on
+    the device, the spectrum from an FP64 plan of the cell's q00 = 1 box)."""
+    import torch
+    plan = getattr(state, "plan", None)
+    if plan is not None:
+        return plan, plan.get_state(), plan.get_spectrum(_lib.SPEC_N_HAT_NOW), None
+    from . import stdpfc
+    phi = np.ascontiguousarray(np.asarray(state, dtype=float))
+    nx, ny = c["uNx"] * c["Mx"], c["uNy"] * c["My"]
+    if phi.shape != (ny, nx):
+        raise ValueError(f"state has shape {phi.shape}, the cell's grid is {(ny, nx)}")
+    lx, ly = _ref_box(c)
+    prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.1, g=0.0, dt=0.01)
+    holder = stdpfc.BuildB200_Simulation(prm, stdpfc.Build2DGeometry(nx, ny, lx, ly), precision="fp64")
+    holder.State.n[...] = phi
+    plan = holder.plan
+    field = torch.as_tensor(phi, device=plan.device)
+    return plan, field, plan.get_spectrum(_lib.SPEC_N_HAT_NOW), holder
+
+
 def frozen_field(state, params, temp, cell):
     """FrozenField of a logPFC field (the adapter's `frozen_field`, logpfc_cpu/
     phase_diagram.py:503-505). `state` is a Simulation of this package (its field and
-    spectrum stay on the device) or an array of the cell's grid (copied to the device
-    into a plan of the cell's q00 = 1 box)."""
+    spectrum stay on the device) or an array of the cell's grid."""
     import torch
     beta, g, v0, q0 = _log_params(params)
     c = _cell(cell)
-    lx = c["Mx"] * 4 * np.pi / np.sqrt(3.0)
-    ly = c["My"] * 4 * np.pi
-    plan = getattr(state, "plan", None)
-    if plan is None:
-        from . import stdpfc
-        phi = np.asarray(state, dtype=float)
-        nx, ny = c["uNx"] * c["Mx"], c["uNy"] * c["My"]
-        if phi.shape != (ny, nx):
-            raise ValueError(f"state has shape {phi.shape}, the cell's grid is {(ny, nx)}")
-        prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=beta, q0=q0, epsilon=float(temp), g=g, dt=0.01)
-        holder = stdpfc.BuildB200_Simulation(prm, stdpfc.Build2DGeometry(nx, ny, lx, ly), precision="fp64")
-        holder.State.n[...] = phi
-        plan = holder.plan
-    f = plan.get_state()
-    spec = plan.get_spectrum(_lib.SPEC_N_HAT_NOW)
+    lx, ly = _ref_box(c)
+    plan, f, spec, _keep = _field_and_spectrum(state, c)
     out = torch.empty(4, dtype=torch.float64, device=f.device)
     stream = ctypes.c_void_p(torch.cuda.current_stream(f.device).cuda_stream)
     _lib.check(plan.lib.pfc_frozen_moments(plan.handle, ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(spec.data_ptr()),
@@ -170,3 +183,25 @@ def frozen_field(state, params, temp, cell):
                                            stream))
     v = out.cpu().tolist()
     return FrozenField(v[:3], v[3], beta, q0)
+
+
+PEAK_SPREAD_MAX = 0.20
+SUBQ_RATIO_MAX = 1e-3
+
+
+def defect_diagnostics(state, cell):
+    """The logPFC adapter's record-only defect screen for frozen_q (logpfc_cpu/
+    phase_diagram.py:509-528) on the device: peak_spread, subq_ratio, n_peaks and
+    defect_flag (either above PEAK_SPREAD_MAX / SUBQ_RATIO_MAX). `state` as for
+    frozen_field."""
+    import torch
+    c = _cell(cell)
+    lx, ly = _ref_box(c)
+    plan, f, spec, _keep = _field_and_spectrum(state, c)
+    out = torch.empty(4, dtype=torch.float64, device=f.device)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(f.device).cuda_stream)
+    _lib.check(plan.lib.pfc_defect_screen(plan.handle, ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(spec.data_ptr()),
+                                          float(lx), float(ly), ctypes.c_void_p(out.data_ptr()), stream))
+    spread, ratio, n_peaks, _ = out.cpu().tolist()
+    return dict(peak_spread=spread, subq_ratio=ratio, n_peaks=int(n_peaks),
+                defect_flag=bool(spread > PEAK_SPREAD_MAX or ratio > SUBQ_RATIO_MAX))

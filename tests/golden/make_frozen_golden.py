@@ -12,8 +12,10 @@ For the three parameter sets of the reference's own test
 1 + 0.05 N(0, 1) noise from default_rng(1)), records the field, the reference's
 FrozenField moments A = (A0, A1, A2), its local term, q_opt and f(q) at five q, plus the
 adapter's free energy of the same field in the box rescaled by each q (the reference
-test's consistency check). The adapter runs the reference's logpfc_cpu simulation
-with the pyFFTW stand-in of `pyfftw_standin/`.
+test's consistency check), and the reference's `defect_diagnostics` (peak spread, sub-q
+ratio, peak count, flag) of those fields and of the clean ansatz with and without one
+vacancy. The adapter runs the reference's logpfc_cpu simulation with the pyFFTW
+stand-in of `pyfftw_standin/`.
 """
 import os
 import sys
@@ -49,7 +51,24 @@ def main(ref_root):
         out[f"qopt_{k}"] = np.array([ff.q_opt()])
         out[f"f_{k}"] = np.array([float(ff.f(q)) for q in QS])
         out[f"f_adapter_{k}"] = np.array(f_adapter)
-        print(k, ff.A.tolist(), ff.local, ff.q_opt())
+        dd = ad.defect_diagnostics(phi, CELL)
+        out[f"defect_{k}"] = np.array([dd["peak_spread"], dd["subq_ratio"], dd["n_peaks"], float(dd["defect_flag"])])
+        print(k, ff.A.tolist(), ff.local, ff.q_opt(), dd)
+    # defect screen on the clean ansatz and on the ansatz with one vacancy
+    params = {'beta': 0.5, 'g': -2.0, 'v0': 1.0}
+    sim = ad.build(params, 'triangle', CELL, H2L, -0.9, 0.7, 1.0, 0.01)
+    clean = np.ascontiguousarray(ad.get_state(sim), dtype=np.float64)
+    vac = clean.copy()
+    ny, nx = vac.shape
+    iy, ix = np.unravel_index(np.argmax(clean[ny // 4: 3 * ny // 4, nx // 4: 3 * nx // 4]), (ny // 2, nx // 2))
+    iy, ix = iy + ny // 4, ix + nx // 4
+    yy, xx = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    vac = vac - 0.6 * (clean[iy, ix] - clean.mean()) * np.exp(-((yy - iy) ** 2 + (xx - ix) ** 2) / 4.0)
+    for name, field in (("clean", clean), ("vacancy", vac)):
+        dd = ad.defect_diagnostics(field, CELL)
+        out[f"dfield_{name}"] = field
+        out[f"dres_{name}"] = np.array([dd["peak_spread"], dd["subq_ratio"], dd["n_peaks"], float(dd["defect_flag"])])
+        print(name, dd)
     np.savez_compressed(os.path.join(HERE, "frozen.npz"), **out)
 
 

@@ -14,7 +14,9 @@ Frozen-field moments (logpfc_cpu/phase_diagram.py:465-505) likewise: the oracle 
 the reference's FrozenField (tests/golden/frozen.npz, make_frozen_golden.py), the device
 moments within 1e-12 relative, and the reference test's property that f(q) equals the
 free energy of the field in the box scaled by q, here within 1e-11 through this
-package's own logPFC reduction.
+package's own logPFC reduction. The defect screen (logpfc_cpu/phase_diagram.py:509-528):
+oracle equal to the reference's, device peak count and flag exact, spread and ratio within
+1e-9 relative.
 """
 import ctypes
 import math
@@ -186,3 +188,33 @@ def test_frozen_f_equals_free_energy_in_the_rescaled_box(golden):
             F = float(sim.CalculateFreeEnergy())
             assert float(ff.f(q)) == pytest.approx(F, rel=1e-11, abs=1e-12)
             assert F == pytest.approx(f_ref, rel=1e-11, abs=1e-12)
+
+
+# ---------------------------------------------------------------- defect screen
+def _defect_cases(d):
+    for k in range(3):
+        yield f"phi_{k}", d[f"phi_{k}"], d[f"defect_{k}"]
+    for name in ("clean", "vacancy"):
+        yield name, d[f"dfield_{name}"], d[f"dres_{name}"]
+
+
+def test_oracle_defect_screen_matches_reference(golden):
+    d = golden("frozen")
+    flags = []
+    for name, phi, want in _defect_cases(d):
+        assert orc.defect_screen(phi, FROZEN_CELL) == (want[0], want[1], int(want[2])), name
+        flags.append(bool(want[3]))
+    assert flags == [False, False, False, False, True]    # the vacancy is the one flagged
+
+
+@pytest.mark.gpu
+def test_device_defect_screen_matches_reference(golden):
+    """Peak count and flag exactly; spread and sub-q ratio within 1e-9 relative, or 1e-12
+    absolute where the reference's value is round-off (the clean ansatz)."""
+    d = golden("frozen")
+    for name, phi, want in _defect_cases(d):
+        dd = diagnostics.defect_diagnostics(phi, FROZEN_CELL)
+        assert dd["n_peaks"] == int(want[2]), name
+        assert dd["defect_flag"] == bool(want[3]), name
+        assert dd["peak_spread"] == pytest.approx(want[0], rel=1e-9, abs=1e-12), name
+        assert dd["subq_ratio"] == pytest.approx(want[1], rel=1e-9, abs=1e-12), name
