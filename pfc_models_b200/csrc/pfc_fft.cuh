@@ -218,10 +218,10 @@ __device__ __forceinline__ void stockham_pass(cplx<T>* buf, int n, int ns, const
     if (j < nr) {
       const int k = j % ns;
       if (k != 0) {
-        const cplx<T>* w = tw + k * (R - 1);
+        const cplx<T>* w = tw + k;   // table [q - 1][k]
 #pragma unroll
         for (int q = 1; q < R; ++q) {
-          cplx<T> t = w[q - 1];
+          cplx<T> t = w[(q - 1) * ns];
           if (INV) t.y = -t.y;
           v[b][q] = cmul(v[b][q], t);
         }

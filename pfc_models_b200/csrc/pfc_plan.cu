@@ -94,8 +94,9 @@ void build_fft(int n, const std::vector<int>& radices, std::vector<long double>&
     d.radix[p] = R;
     d.ns[p] = ns;
     d.twoff[p] = (int)(tw.size() / 2);
-    for (int k = 0; k < ns; ++k)
-      for (int q = 1; q < R; ++q) {
+    // [q - 1][k]: the lanes of a warp (consecutive k) read consecutive entries
+    for (int q = 1; q < R; ++q)
+      for (int k = 0; k < ns; ++k) {
         const long long num = (long long)q * k % ((long long)ns * R);
         const long double ang = -twopi * (long double)num / (long double)(ns * R);
         tw.push_back(cosl(ang));
