@@ -196,9 +196,20 @@ template <int R, class T> struct MaxBfly {
 // Radix sets compiled into a kernel: powers of two only, or every supported radix.
 enum : int { kRadixPow2 = 0, kRadixAll = 1 };
 
+// One transform's exchange buffer in shared memory, with one pad element per 16 (index i
+// lives at i + i / 16): the stores of a small-stride pass, R elements apart across lanes,
+// then fall on different banks for the 16 lanes an 8-byte access serves at once.
+constexpr int kGenericPadShift = 4;
+__host__ __device__ constexpr int generic_pad(int i) { return i + (i >> kGenericPadShift); }
+template <class T>
+struct PadBuf {
+  cplx<T>* p;
+  __device__ __forceinline__ cplx<T>& operator[](int i) const { return p[generic_pad(i)]; }
+};
+
 // One in-place Stockham pass over a transform of length n at `buf`.
 template <int R, bool INV, class T>
-__device__ __forceinline__ void stockham_pass(cplx<T>* buf, int n, int ns, const cplx<T>* __restrict__ tw,
+__device__ __forceinline__ void stockham_pass(PadBuf<T> buf, int n, int ns, const cplx<T>* __restrict__ tw,
                                               const cplx<T>* __restrict__ roots, int lt, int tpf) {
   constexpr int MB = MaxBfly<R, T>::value;
   const int nr = n / R;
@@ -237,7 +248,7 @@ __device__ __forceinline__ void stockham_pass(cplx<T>* buf, int n, int ns, const
 
 // Runs every pass of `d` on buf. All threads of the CTA must call this with the same d.
 template <bool INV, int RSET, class T>
-__device__ __forceinline__ void fft_run(cplx<T>* buf, const FftDesc& d, const cplx<T>* __restrict__ twbase, int lt, int tpf) {
+__device__ __forceinline__ void fft_run(PadBuf<T> buf, const FftDesc& d, const cplx<T>* __restrict__ twbase, int lt, int tpf) {
   for (int p = 0; p < d.npass; ++p) {
     const cplx<T>* tw = twbase + d.twoff[p];
     const cplx<T>* roots = d.rootoff[p] >= 0 ? twbase + d.rootoff[p] : nullptr;

@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(LB, MINB) row_kernel(RowArgs<T> a) {
   const int f = threadIdx.x / tpf, lt = threadIdx.x - f * tpf;
   const int y = y0 + f;
   const bool valid = (y < ny);
-  cplx<T>* buf = sm + f * ld;
+  const PadBuf<T> buf{sm + f * ld};   // padded exchange buffer of this transform
   const bool dev = (sizeof(T) == 4);
 
   if (MODE != kRowForward) {
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(LB, MINB) row_kernel(RowArgs<T> a) {
       const int r = i % rows, kx = i / rows;
       cplx<T> v = mk(T(0), T(0));
       if (y0 + r < ny) v = a.in[(size_t)kx * ny + (y0 + r)];
-      sm[r * ld + kx] = v;
+      sm[r * ld + generic_pad(kx)] = v;
     }
     __syncthreads();
     // pre-process pairs (k, m-k) of the inverse real transform
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(LB, MINB) row_kernel(RowArgs<T> a) {
     __syncthreads();
     for (int i = threadIdx.x; i < rows * m; i += blockDim.x) {
       const int r = i % rows, kx = i / rows;
-      if (y0 + r < ny) a.out[(size_t)kx * ny + (y0 + r)] = sm[r * ld + kx];
+      if (y0 + r < ny) a.out[(size_t)kx * ny + (y0 + r)] = sm[r * ld + generic_pad(kx)];
     }
     return;
   }
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
   const int f = threadIdx.x / tpf, lt = threadIdx.x - f * tpf;
   const int kx = c0 + f;
   const bool valid = kx < m;
-  cplx<T>* buf = sm + f * ld;
+  const PadBuf<T> buf{sm + f * ld};   // padded exchange buffer of this transform
 
   if (MODE == kColParseval || MODE == kColExport) {
     // no transform: direct pass over n_hat
@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
       const int c = i / ny, ky = i - c * ny;
       cplx<T> v = mk(T(0), T(0));
       if (c0 + c < m) v = a.in[(size_t)c0 * ny + i];
-      sm[c * ld + ky] = v;
+      sm[c * ld + generic_pad(ky)] = v;
     }
     __syncthreads();
     fft_run<false, RSET>(buf, a.fft, a.tw, lt, tpf);
@@ -588,7 +588,7 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
   for (int i = threadIdx.x; i < cols * ny; i += blockDim.x) {
     const int c = i / ny, ky = i - c * ny;
     if (c0 + c < m) {
-      const cplx<T> v = sm[c * ld + ky];
+      const cplx<T> v = sm[c * ld + generic_pad(ky)];
       a.wout[(size_t)c0 * ny + i] = mk(s * v.x, s * v.y);
     }
   }

@@ -874,7 +874,10 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   const int min_ctas = 2 * std::max(n_sm, 1);
   {
     h->row_tpf = threads_per_fft(rrow, m, h->fp32);
-    h->row_ld = m + 1;
+    // padded row (generic_pad) plus one, odd, so that the transposing tile accesses of
+    // consecutive rows start on different banks
+    h->row_ld = generic_pad(m - 1) + 2;
+    if (h->row_ld % 2 == 0) ++h->row_ld;
     if (h->row_tpf > kBlockMax && h->row_rset == kRadixPow2 && h->row_tpf <= 1024) h->row_rset = kRadixPow2Big;
     const int kBlockMax = h->row_rset == kRadixPow2Big ? 1024 : pfc_block_max;
     if (h->row_tpf > kBlockMax)
@@ -895,7 +898,8 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   }
   {
     h->col_tpf = threads_per_fft(rcol, p->ny, h->fp32);
-    h->col_ld = p->ny;
+    h->col_ld = generic_pad(p->ny - 1) + 2;   // padded column plus one
+    if (h->col_ld % 2 == 0) ++h->col_ld;
     if (h->col_tpf > kBlockMax && h->col_rset == kRadixPow2 && h->col_tpf <= 1024) h->col_rset = kRadixPow2Big;
     const int kBlockMax = h->col_rset == kRadixPow2Big ? 1024 : pfc_block_max;
     if (h->col_tpf > kBlockMax)
