@@ -193,8 +193,10 @@ template <int R, class T> struct MaxBfly {
                              : ((MaxElems<T>::value / R) > 0 ? (MaxElems<T>::value / R) : 1);
 };
 
-// Radix sets compiled into a kernel: powers of two only, or every supported radix.
-enum : int { kRadixPow2 = 0, kRadixAll = 1 };
+// Radix sets compiled into a kernel: powers of two only, every supported radix, or the
+// radices of grids with prime factors 2, 3, 5 and 7 only (a smaller kernel than the full
+// set, which also carries the radix-11 and radix-13 butterflies).
+enum : int { kRadixPow2 = 0, kRadixAll = 1, kRadixSmall = 4 };
 
 // One transform's exchange buffer in shared memory, with one pad element per 16 (index i
 // lives at i + i / 16): the stores of a small-stride pass, R elements apart across lanes,
@@ -257,6 +259,17 @@ __device__ __forceinline__ void fft_run(PadBuf<T> buf, const FftDesc& d, const c
       switch (d.radix[p]) {
         case 2: stockham_pass<2, INV>(buf, d.n, ns, tw, roots, lt, tpf); break;
         case 4: stockham_pass<4, INV>(buf, d.n, ns, tw, roots, lt, tpf); break;
+        case 8: stockham_pass<8, INV>(buf, d.n, ns, tw, roots, lt, tpf); break;
+        case 16: stockham_pass<16, INV>(buf, d.n, ns, tw, roots, lt, tpf); break;
+        default: break;  // rejected on the host
+      }
+    } else if constexpr (RSET == kRadixSmall) {
+      switch (d.radix[p]) {
+        case 2: stockham_pass<2, INV>(buf, d.n, ns, tw, roots, lt, tpf); break;
+        case 3: stockham_pass<3, INV>(buf, d.n, ns, tw, roots, lt, tpf); break;
+        case 4: stockham_pass<4, INV>(buf, d.n, ns, tw, roots, lt, tpf); break;
+        case 5: stockham_pass<5, INV>(buf, d.n, ns, tw, roots, lt, tpf); break;
+        case 7: stockham_pass<7, INV>(buf, d.n, ns, tw, roots, lt, tpf); break;
         case 8: stockham_pass<8, INV>(buf, d.n, ns, tw, roots, lt, tpf); break;
         case 16: stockham_pass<16, INV>(buf, d.n, ns, tw, roots, lt, tpf); break;
         default: break;  // rejected on the host

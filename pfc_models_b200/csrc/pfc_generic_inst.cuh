@@ -19,6 +19,15 @@ void* pick_row(int model, int rset) {
                  : (void*)row_kernel<T, MODE, kModelStd, kRadixAll, 256, 2>;
     rset = kRadixAll;
   }
+  if (rset == kRadixSmallDense) {
+    if constexpr (sizeof(T) == 4 && MODE == kRowStep)
+      return log ? (void*)row_kernel<T, MODE, kModelLog, kRadixSmall, 256, 2>
+                 : (void*)row_kernel<T, MODE, kModelStd, kRadixSmall, 256, 2>;
+    rset = kRadixSmall;
+  }
+  if (rset == kRadixSmall)
+    return log ? (void*)row_kernel<T, MODE, kModelLog, kRadixSmall, 256>
+               : (void*)row_kernel<T, MODE, kModelStd, kRadixSmall, 256>;
   if (rset == kRadixPow2Big)
     return log ? (void*)row_kernel<T, MODE, kModelLog, kRadixPow2, 1024>
                : (void*)row_kernel<T, MODE, kModelStd, kRadixPow2, 1024>;
@@ -35,6 +44,11 @@ void* pick_col(int rset) {
     if constexpr (sizeof(T) == 4 && MODE == kColStep) return (void*)col_kernel<T, MODE, kRadixAll, 256, 2>;
     rset = kRadixAll;
   }
+  if (rset == kRadixSmallDense) {
+    if constexpr (sizeof(T) == 4 && MODE == kColStep) return (void*)col_kernel<T, MODE, kRadixSmall, 256, 2>;
+    rset = kRadixSmall;
+  }
+  if (rset == kRadixSmall && MODE != kColParseval && MODE != kColExport) return (void*)col_kernel<T, MODE, kRadixSmall, 256>;
   if (rset == kRadixPow2Big) return (void*)col_kernel<T, MODE, kRadixPow2, 1024>;
   if (MODE == kColParseval || MODE == kColExport || rset == kRadixPow2) return (void*)col_kernel<T, MODE, kRadixPow2, 256>;
   return (void*)col_kernel<T, MODE, kRadixAll, 256>;

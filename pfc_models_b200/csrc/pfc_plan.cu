@@ -832,11 +832,19 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   h->fp32 = (p->precision == PFC_FP32_MIXED);
   h->nx = p->nx; h->ny = p->ny; h->m = m; h->nyh = p->ny / 2 + 1;
   h->nspec = (size_t)m * p->ny;
-  h->row_rset = all_pow2(rrow) ? kRadixPow2 : kRadixAll;
-  h->col_rset = all_pow2(rcol) ? kRadixPow2 : kRadixAll;
+  auto rset_of = [](const std::vector<int>& r) {
+    if (all_pow2(r)) return (int)kRadixPow2;
+    for (int x : r)
+      if (x == 11 || x == 13) return (int)kRadixAll;
+    return (int)kRadixSmall;
+  };
+  h->row_rset = rset_of(rrow);
+  h->col_rset = rset_of(rcol);
   if (h->fp32 && (long long)p->nx * p->ny >= kDenseMinSites) {
-    if (h->row_rset == kRadixAll) h->row_rset = kRadixAllDense;
-    if (h->col_rset == kRadixAll) h->col_rset = kRadixAllDense;
+    for (int* r : {&h->row_rset, &h->col_rset}) {
+      if (*r == kRadixAll) *r = kRadixAllDense;
+      else if (*r == kRadixSmall) *r = kRadixSmallDense;
+    }
   }
   h->elt = h->fp32 ? sizeof(float2) : sizeof(double2);
   cudaGetDevice(&h->device);

@@ -17,6 +17,9 @@ constexpr int kRadixPow2Big = 2;
 // registers, with some spills) instead of one: faster for large FP32 grids, slower for
 // small grids and in FP64 (measured on B200). Modes other than the step use kRadixAll.
 constexpr int kRadixAllDense = 3;
+// Grids with prime factors 2, 3, 5, 7 only: the smaller radix set (kRadixSmall), and its
+// two-CTA step build as above.
+constexpr int kRadixSmallDense = 5;
 constexpr long long kDenseMinSites = 1LL << 20;
 
 // log2 sizes of the power-of-two step kernels: row transforms of M = nx/2 points,
