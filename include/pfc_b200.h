@@ -175,8 +175,9 @@ int64_t pfc_launch_count(pfc_plan* plan);
  * kernels and nonlinearity parameters (g, clamp, min_phi) form a class; each pass
  * of a step is one launch per class with one grid row per plan, reading that
  * plan's buffers from a device table. Whole blocks of 16 steps replay a recorded
- * CUDA graph. All plans must use the power-of-two step kernels, one precision and
- * one device (current when the batch is created); at most 65535 plans. The batch
+ * CUDA graph. Power-of-two and mixed-radix plans may be mixed (each kind forms its own
+ * classes); all plans must use one precision and one device (current when the batch is
+ * created); at most 65535 plans. The batch
  * borrows the plans: destroy it before them. Each plan keeps its own state, so
  * pfc_reduce / pfc_get_state work on any of them between batch steps.
  */

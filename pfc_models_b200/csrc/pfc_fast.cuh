@@ -169,19 +169,6 @@ __device__ __forceinline__ void fast_mid(cplx<T>* buf, cplx<T>* v, int t, int g,
   }
 }
 
-// Buffers of one plan of a batch (pfc_batch_*): the step kernels of a batched launch
-// take their per-plan pointers from entry blockIdx.y of a device table of these.
-struct BatchBufs {
-  const void* w;        // W (row input, column output)
-  void* v;              // V (row output, column input)
-  const void* nin;      // n_hat of the current state (hi in the FP32 form)
-  void* nout;           // n_hat of the next state
-  const void* nin_lo;   // FP32 form: the residual arrays of the two states
-  void* nout_lo;
-  const void* coef;     // (A - 1, Bg), working precision
-  const void* coef64;   // FP32 form: (A - 1, Bg) in FP64
-  const double* scal;   // deviation-form scalars
-};
 
 template <class T>
 struct FastRowArgs {

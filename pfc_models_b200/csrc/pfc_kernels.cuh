@@ -124,6 +124,20 @@ __device__ __forceinline__ float nonlin_dev(float d, float c1, float c2, float i
 }
 
 // ---------------------------------------------------------------- arguments
+// Buffers of one plan of a batch (pfc_batch_*): the step kernels of a batched launch
+// take their per-plan pointers from entry blockIdx.y of a device table of these.
+struct BatchBufs {
+  const void* w;        // W (row input, column output)
+  void* v;              // V (row output, column input)
+  const void* nin;      // n_hat of the current state (hi in the FP32 form)
+  void* nout;           // n_hat of the next state
+  const void* nin_lo;   // FP32 form: the residual arrays of the two states
+  void* nout_lo;
+  const void* coef;     // (A - 1, Bg), working precision
+  const void* coef64;   // FP32 form: (A - 1, Bg) in FP64
+  const double* scal;   // deviation-form scalars
+};
+
 template <class T>
 struct RowArgs {
   int nx, ny, m, rows, tpf, ld;
@@ -139,6 +153,7 @@ struct RowArgs {
   double* partials;         // per-CTA compensated sums
   int clamp;
   double g, min_phi, min_log, epsilon;
+  const BatchBufs* batch;   // step mode of a batch: per-plan W, V and scalars at [blockIdx.y]
 };
 
 // The spectral state and the update n_hat' = n_hat + (A - 1) n_hat + Bg N_hat.
@@ -172,6 +187,7 @@ struct ColArgs {
   double fx, fy;                // 1/(nx dx), 1/(ny dy): k = 2 pi idx f
   double beta, q0, epsilon, w;  // L_mu, L_f, Gaussian width
   const double* scal;           // device scalar block (export adds the deviation-form DC)
+  const BatchBufs* batch;       // step mode of a batch: per-plan buffers at [blockIdx.y]
 };
 
 // Element i of a spectral state (hi + lo in the FP32 form when with_lo).
@@ -241,13 +257,23 @@ __global__ void __launch_bounds__(LB, MINB) row_kernel(RowArgs<T> a) {
   const bool valid = (y < ny);
   const PadBuf<T> buf{sm + f * ld};   // padded exchange buffer of this transform
   const bool dev = (sizeof(T) == 4);
+  // per-plan buffers: this plan's, or in a batched step launch plan blockIdx.y's
+  const cplx<T>* a_in = a.in;
+  cplx<T>* a_out = a.out;
+  const double* a_scal = a.scal;
+  if (a.batch) {
+    const BatchBufs& bb = a.batch[blockIdx.y];
+    a_in = static_cast<const cplx<T>*>(bb.w);
+    a_out = static_cast<cplx<T>*>(bb.v);
+    a_scal = bb.scal;
+  }
 
   if (MODE != kRowForward) {
     // packed spectra, column-major [kx][y]: `rows` consecutive y per kx
     for (int i = threadIdx.x; i < rows * m; i += blockDim.x) {
       const int r = i % rows, kx = i / rows;
       cplx<T> v = mk(T(0), T(0));
-      if (y0 + r < ny) v = a.in[(size_t)kx * ny + (y0 + r)];
+      if (y0 + r < ny) v = a_in[(size_t)kx * ny + (y0 + r)];
       sm[r * ld + generic_pad(kx)] = v;
     }
     __syncthreads();
@@ -270,7 +296,7 @@ __global__ void __launch_bounds__(LB, MINB) row_kernel(RowArgs<T> a) {
     // buf[j] = x[2j] + i x[2j+1]
   } else {
     // real FP64 field (ny, nx), row-major; deviation form subtracts the mean
-    const double mean = dev ? a.scal[kScalMean] : 0.0;
+    const double mean = dev ? a_scal[kScalMean] : 0.0;
     const double2* src = reinterpret_cast<const double2*>(a.in_real + (size_t)y * a.nx);
     for (int j = lt; j < m; j += tpf) {
       cplx<T> v = mk(T(0), T(0));
@@ -285,11 +311,11 @@ __global__ void __launch_bounds__(LB, MINB) row_kernel(RowArgs<T> a) {
 
   if (MODE == kRowStep) {
     if (dev) {
-      const float c1 = (float)a.scal[kScalC1], c2 = (float)a.scal[kScalC2];
-      const float inv = (float)a.scal[kScalInvMean];
-      const double inv_d = a.scal[kScalInvMean];
+      const float c1 = (float)a_scal[kScalC1], c2 = (float)a_scal[kScalC2];
+      const float inv = (float)a_scal[kScalInvMean];
+      const double inv_d = a_scal[kScalInvMean];
       const double mphi_rel = a.min_phi * inv_d;
-      const float lmin = (float)a.scal[kScalLogMin];
+      const float lmin = (float)a_scal[kScalLogMin];
       for (int j = lt; j < m; j += tpf) {
         const cplx<T> z = buf[j];
         buf[j] = mk((T)nonlin_dev<MODEL>((float)z.x, c1, c2, inv, inv_d, a.clamp, mphi_rel, lmin),
@@ -325,7 +351,7 @@ __global__ void __launch_bounds__(LB, MINB) row_kernel(RowArgs<T> a) {
     __syncthreads();
     for (int i = threadIdx.x; i < rows * m; i += blockDim.x) {
       const int r = i % rows, kx = i / rows;
-      if (y0 + r < ny) a.out[(size_t)kx * ny + (y0 + r)] = sm[r * ld + generic_pad(kx)];
+      if (y0 + r < ny) a_out[(size_t)kx * ny + (y0 + r)] = sm[r * ld + generic_pad(kx)];
     }
     return;
   }
@@ -348,7 +374,7 @@ __global__ void __launch_bounds__(LB, MINB) row_kernel(RowArgs<T> a) {
 
   if (MODE == kRowReduce) {
     // sums of: raw value (mean), free-energy polynomial, nonlinear mu
-    const double mean = dev ? a.scal[kScalMean] : 0.0;
+    const double mean = dev ? a_scal[kScalMean] : 0.0;
     const double eps = a.epsilon, g = a.g;
     KSum acc[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
     if (valid) {
@@ -394,6 +420,26 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
   const int kx = c0 + f;
   const bool valid = kx < m;
   const PadBuf<T> buf{sm + f * ld};   // padded exchange buffer of this transform
+  // per-plan buffers: this plan's, or in a batched step launch plan blockIdx.y's
+  const cplx<T>* a_in = a.in;
+  const void* a_nin = a.nin;
+  const cplx<float>* a_nin_lo = a.nin_lo;
+  void* a_nout = a.nout;
+  cplx<float>* a_nout_lo = a.nout_lo;
+  cplx<T>* a_wout = a.wout;
+  const cplx<T>* a_coef = a.coef;
+  const cplx<double>* a_coef64 = a.coef64;
+  if (a.batch) {
+    const BatchBufs& bb = a.batch[blockIdx.y];
+    a_in = static_cast<const cplx<T>*>(bb.v);
+    a_nin = bb.nin;
+    a_nin_lo = static_cast<const cplx<float>*>(bb.nin_lo);
+    a_nout = bb.nout;
+    a_nout_lo = static_cast<cplx<float>*>(bb.nout_lo);
+    a_wout = static_cast<cplx<T>*>(const_cast<void*>(bb.w));
+    a_coef = static_cast<const cplx<T>*>(bb.coef);
+    a_coef64 = static_cast<const cplx<double>*>(bb.coef64);
+  }
 
   if (MODE == kColParseval || MODE == kColExport) {
     // no transform: direct pass over n_hat
@@ -441,7 +487,7 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
     for (int i = threadIdx.x; i < cols * ny; i += blockDim.x) {
       const int c = i / ny, ky = i - c * ny;
       cplx<T> v = mk(T(0), T(0));
-      if (c0 + c < m) v = a.in[(size_t)c0 * ny + i];
+      if (c0 + c < m) v = a_in[(size_t)c0 * ny + i];
       sm[c * ld + generic_pad(ky)] = v;
     }
     __syncthreads();
@@ -454,7 +500,7 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
       for (int ky = lt; ky < ny; ky += tpf) {
         cplx<T> v = buf[ky];
         if (a.dev_form && kx == 0 && ky == 0) { v.x = T(0); buf[0] = v; }
-        state_st<T>(a.nout, a.nout_lo, cb + ky, mk((double)v.x, (double)v.y), true);   // lo = 0
+        state_st<T>(a_nout, a_nout_lo, cb + ky, mk((double)v.x, (double)v.y), true);   // lo = 0
       }
     }
     __syncthreads();
@@ -467,10 +513,10 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
         const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
         // the packed column holds kx = 0 (slow near ky = 0): always at full precision
         bool s0, sM;
-        const cplx<double> c0v = coef_ld<T>(a.coef, a.coef64, ky, a.slow_tau, true, s0);
-        const cplx<double> cMv = coef_ld<T>(a.coef, a.coef64, (size_t)m * nyh + ky, a.slow_tau, true, sM);
-        const cplx<double> pk = state_ld<T>(a.nin, a.nin_lo, cb + ky, true);
-        const cplx<double> pkp = state_ld<T>(a.nin, a.nin_lo, cb + kyp, true);
+        const cplx<double> c0v = coef_ld<T>(a_coef, a_coef64, ky, a.slow_tau, true, s0);
+        const cplx<double> cMv = coef_ld<T>(a_coef, a_coef64, (size_t)m * nyh + ky, a.slow_tau, true, sM);
+        const cplx<double> pk = state_ld<T>(a_nin, a_nin_lo, cb + ky, true);
+        const cplx<double> pkp = state_ld<T>(a_nin, a_nin_lo, cb + kyp, true);
         cplx<double> h0, hm, g0, gm;
         unpack_pair(pk, pkp, h0, hm);
         unpack_pair(qk, qkp, g0, gm);
@@ -478,10 +524,10 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
         const cplx<double> hmn = hm + cMv.x * hm + cMv.y * gm;
         const cplx<double> ok = h0n + mul_i(hmn);
         const cplx<double> okp = conj(h0n) + mul_i(conj(hmn));
-        state_st<T>(a.nout, a.nout_lo, cb + ky, ok, true);
+        state_st<T>(a_nout, a_nout_lo, cb + ky, ok, true);
         buf[ky] = mk((T)ok.x, (T)ok.y);
         if (kyp != ky) {
-          state_st<T>(a.nout, a.nout_lo, cb + kyp, okp, true);
+          state_st<T>(a_nout, a_nout_lo, cb + kyp, okp, true);
           buf[kyp] = mk((T)okp.x, (T)okp.y);
         }
       }
@@ -491,7 +537,7 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
       // behind an earlier pair's stores); arithmetic as coef_ld / state_ld / state_st
       constexpr int CH = 2;
       const size_t cb = (size_t)kx * ny;
-      const cplx<T>* nin = static_cast<const cplx<T>*>(a.nin);
+      const cplx<T>* nin = static_cast<const cplx<T>*>(a_nin);
       for (int ky0 = lt; ky0 <= ny / 2; ky0 += CH * tpf) {
         cplx<T> cw[CH], ph[CH], pph[CH];
 #pragma unroll
@@ -499,7 +545,7 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
           const int ky = ky0 + j * tpf;
           if (ky <= ny / 2) {
             const int kyp = ky == 0 ? 0 : ny - ky;
-            cw[j] = a.coef[(size_t)kx * nyh + ky];
+            cw[j] = a_coef[(size_t)kx * nyh + ky];
             ph[j] = nin[cb + ky];
             pph[j] = nin[cb + kyp];
           }
@@ -512,11 +558,11 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
           const cplx<T> qkt = buf[ky], qkpt = buf[kyp];
           const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
           const bool slow = sizeof(T) == 8 || fabs((double)cw[j].x) < (double)a.slow_tau;
-          const cplx<double> c = (sizeof(T) == 4 && slow) ? a.coef64[(size_t)kx * nyh + ky]
+          const cplx<double> c = (sizeof(T) == 4 && slow) ? a_coef64[(size_t)kx * nyh + ky]
                                                            : mk((double)cw[j].x, (double)cw[j].y);
           cplx<double> pk = mk((double)ph[j].x, (double)ph[j].y), pkp = mk((double)pph[j].x, (double)pph[j].y);
           if (sizeof(T) == 4 && slow) {
-            const cplx<float> l = a.nin_lo[cb + ky], lp = a.nin_lo[cb + kyp];
+            const cplx<float> l = a_nin_lo[cb + ky], lp = a_nin_lo[cb + kyp];
             pk.x += (double)l.x;
             pk.y += (double)l.y;
             pkp.x += (double)lp.x;
@@ -524,10 +570,10 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
           }
           const cplx<double> ok = pk + c.x * pk + c.y * qk;
           const cplx<double> okp = pkp + c.x * pkp + c.y * qkp;
-          state_st<T>(a.nout, a.nout_lo, cb + ky, ok, slow);
+          state_st<T>(a_nout, a_nout_lo, cb + ky, ok, slow);
           buf[ky] = mk((T)ok.x, (T)ok.y);
           if (kyp != ky) {
-            state_st<T>(a.nout, a.nout_lo, cb + kyp, okp, slow);
+            state_st<T>(a_nout, a_nout_lo, cb + kyp, okp, slow);
             buf[kyp] = mk((T)okp.x, (T)okp.y);
           }
         }
@@ -556,8 +602,8 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
             default: mn[h] = 1.0; mq[h] = 0.0; break;
           }
         }
-        const cplx<double> pk = state_ld<T>(a.nin, a.nin_lo, cb + ky, true);
-        const cplx<double> pkp = state_ld<T>(a.nin, a.nin_lo, cb + kyp, true);
+        const cplx<double> pk = state_ld<T>(a_nin, a_nin_lo, cb + ky, true);
+        const cplx<double> pkp = state_ld<T>(a_nin, a_nin_lo, cb + kyp, true);
         cplx<double> qk = mk(0.0, 0.0), qkp = qk;
         if (need_v) {
           qk = mk((double)buf[ky].x, (double)buf[ky].y);
@@ -589,7 +635,7 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
     const int c = i / ny, ky = i - c * ny;
     if (c0 + c < m) {
       const cplx<T> v = sm[c * ld + generic_pad(ky)];
-      a.wout[(size_t)c0 * ny + i] = mk(s * v.x, s * v.y);
+      a_wout[(size_t)c0 * ny + i] = mk(s * v.x, s * v.y);
     }
   }
 }

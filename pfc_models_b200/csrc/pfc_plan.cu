@@ -245,20 +245,20 @@ template <class T, int MODE>
 void* pick_col(int rset) { return GenericInst<T>::col(MODE, rset); }
 
 template <class T, int MODE>
-int launch_row(pfc_plan* h, const RowArgs<T>& a, cudaStream_t s) {
+int launch_row(pfc_plan* h, const RowArgs<T>& a, cudaStream_t s, int count = 1) {
   void* fn = pick_row<T, MODE>(h->prob.model, h->row_rset);
   void* args[] = {(void*)&a};
-  cudaError_t e = cudaLaunchKernel(fn, dim3(h->row_grid), dim3(h->rows * h->row_tpf), args, h->row_smem, s);
+  cudaError_t e = cudaLaunchKernel(fn, dim3(h->row_grid, count), dim3(h->rows * h->row_tpf), args, h->row_smem, s);
   ++h->launches;
   if (e != cudaSuccess) return fail(PFC_E_CUDA, "row kernel launch failed: %s", cudaGetErrorString(e));
   return PFC_OK;
 }
 
 template <class T, int MODE>
-int launch_col(pfc_plan* h, const ColArgs<T>& a, cudaStream_t s) {
+int launch_col(pfc_plan* h, const ColArgs<T>& a, cudaStream_t s, int count = 1) {
   void* fn = pick_col<T, MODE>(h->col_rset);
   void* args[] = {(void*)&a};
-  cudaError_t e = cudaLaunchKernel(fn, dim3(h->col_grid), dim3(h->cols * h->col_tpf), args, h->col_smem, s);
+  cudaError_t e = cudaLaunchKernel(fn, dim3(h->col_grid, count), dim3(h->cols * h->col_tpf), args, h->col_smem, s);
   ++h->launches;
   if (e != cudaSuccess) return fail(PFC_E_CUDA, "column kernel launch failed: %s", cudaGetErrorString(e));
   return PFC_OK;
@@ -438,7 +438,8 @@ int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
   RowArgs<T> ra = row_args<T>(h);
   ra.in = reinterpret_cast<const cplx<T>*>(h->W);
   ra.out = reinterpret_cast<cplx<T>*>(h->V);
-  return launch_row<T, kRowStep>(h, ra, s);
+  ra.batch = table;
+  return launch_row<T, kRowStep>(h, ra, s, count);
 }
 
 // One column pass of a step: V, n_hat[cur] -> n_hat[cur ^ 1], W (batched as above).
@@ -474,7 +475,8 @@ int launch_step_col(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
   ca.nout = h->nhat[h->cur ^ 1];
   ca.nin_lo = static_cast<const cplx<float>*>(h->nhat_lo[h->cur]);
   ca.nout_lo = static_cast<cplx<float>*>(h->nhat_lo[h->cur ^ 1]);
-  return launch_col<T, kColStep>(h, ca, s);
+  ca.batch = table;
+  return launch_col<T, kColStep>(h, ca, s, count);
 }
 
 // ---- entry point bodies, templated on the working precision
@@ -1130,8 +1132,6 @@ int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out) {
   *out = nullptr;
   for (int i = 0; i < count; ++i) {
     if (!plans[i]) return fail(PFC_E_ARG, "pfc_batch_create: null plan %d", i);
-    if (!plans[i]->fast)
-      return fail(PFC_E_ARG, "pfc_batch_create: plan %d does not use the power-of-two step kernels", i);
     if (plans[i]->fp32 != plans[0]->fp32) return fail(PFC_E_ARG, "pfc_batch_create: plans mix precisions");
     if (plans[i]->device != plans[0]->device) return fail(PFC_E_ARG, "pfc_batch_create: plans on different devices");
     for (int j = 0; j < i; ++j)
@@ -1146,8 +1146,11 @@ int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out) {
     for (auto& c : b->classes) {
       // everything the step kernels take from the plan besides the per-plan table entries
       const pfc_plan* r = c.plans[0];
-      if (r->fast_row_fn == h->fast_row_fn && r->fast_col_fn == h->fast_col_fn && r->nx == h->nx &&
-          r->ny == h->ny && r->prob.g == h->prob.g && r->prob.clamp_log == h->prob.clamp_log &&
+      // (mixed-radix plans of one size and precision share the FFT description, twiddle
+      // tables and launch shape, all of which come from plans[0] of the class)
+      if (r->fast == h->fast && r->fast_row_fn == h->fast_row_fn && r->fast_col_fn == h->fast_col_fn &&
+          r->row_rset == h->row_rset && r->col_rset == h->col_rset && r->prob.model == h->prob.model &&
+          r->nx == h->nx && r->ny == h->ny && r->prob.g == h->prob.g && r->prob.clamp_log == h->prob.clamp_log &&
           r->prob.min_phi == h->prob.min_phi) {
         cls = &c;
         break;

@@ -479,9 +479,9 @@ class Simulation:
 
 class Batch:
     """Independent simulations stepped in lockstep through pfc_batch_* (one launch per
-    class and pass). Accepts `Simulation` objects or `Plan`s; they must all use the
-    power-of-two step kernels, one precision and one device. The batch borrows the
-    plans: close it before them."""
+    class and pass). Accepts `Simulation` objects or `Plan`s of any supported grid (the
+    power-of-two and the mixed-radix kernels both batch); they must use one precision and
+    one device. The batch borrows the plans: close it before them."""
 
     def __init__(self, items):
         self.items = list(items)

@@ -111,7 +111,7 @@ def test_launch_modes_match_serialised_launches(precision, model):
     assert all(s.Reduce() == ref.Reduce() for s in sims)
 
 
-def test_batch_rejects_mixed_parity_and_unsupported_plans():
+def test_batch_rejects_mixed_parity_precisions_and_repeats():
     s1 = _std_sim(64, 64, -0.3, -0.3, "fp32", seed=0)
     s2 = _std_sim(64, 64, -0.3, -0.3, "fp32", seed=1)
     s1.TimeStep()
@@ -122,12 +122,6 @@ def test_batch_rejects_mixed_parity_and_unsupported_plans():
     s2.TimeStep()
     b.step(2)
     b.close()
-    prm = stdpfc.BuildStdPFCModelParameters(epsilon=-0.3, g=0.0, dt=0.5)
-    geom = stdpfc.Build2DGeometry(64, 64, 16 * np.pi, 16 * np.pi)
-    gen = stdpfc.BuildB200_Simulation(prm, geom, precision="fp32", kernels="generic")
-    with pytest.raises(_lib.PfcError) as e:
-        Batch([s1, gen])
-    assert e.value.code == _lib.PFC_E_ARG
     f64 = _std_sim(64, 64, -0.3, -0.3, "fp64", seed=0)
     with pytest.raises(_lib.PfcError) as e:
         Batch([s1, f64])
@@ -135,6 +129,47 @@ def test_batch_rejects_mixed_parity_and_unsupported_plans():
     with pytest.raises(_lib.PfcError) as e:
         Batch([s1, s1])
     assert e.value.code == _lib.PFC_E_ARG
+
+
+def _generic_mix(precision, graphs, pdl=None):
+    """Mixed-radix and power-of-two plans in one batch: 224x392 std (x2), 96x80 log,
+    448^2 std, and a 64^2 std forced onto the mixed-radix kernels next to a 64^2 std on
+    the power-of-two ones."""
+    specs = [("std", 224, 392, -0.3, -0.3, "auto"), ("std", 224, 392, -0.25, -0.2, "auto"),
+             ("log", 96, 80, None, None, "auto"), ("std", 448, 448, -0.5, -0.4, "auto"),
+             ("std", 64, 64, -0.3, -0.3, "generic"), ("std", 64, 64, -0.3, -0.3, "auto")]
+    sims = []
+    for i, (mdl, nx, ny, eps, mean, kern) in enumerate(specs):
+        if mdl == "std":
+            sims.append(_std_sim(nx, ny, eps, mean, precision, seed=10 + i, graphs=graphs, pdl=pdl, kernels=kern))
+        else:
+            sims.append(_log_sim(nx, ny, precision, seed=10 + i, graphs=graphs, pdl=pdl, kernels=kern))
+    return sims
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_of_mixed_radix_plans_matches_individual_plans(precision):
+    """Grids with factors 3 and 7 (the phase-diagram cells' kind) batch like the
+    power-of-two ones: 37 and then 21 steps equal each plan stepped on its own."""
+    ref = _generic_mix(precision, graphs=False, pdl=False)
+    for s in ref:
+        s.TimeSteps(37)
+    sims = _generic_mix(precision, graphs=True)
+    assert [s.plan.variant()["fast"] for s in sims] == [0, 0, 0, 0, 0, 1]
+    b = Batch(sims)
+    assert b.classes == 5
+    b.step(37)
+    for i, (s, r) in enumerate(zip(sims, ref)):
+        assert np.array_equal(_field(s), _field(r)), i
+    b.step(21)
+    for s in ref:
+        s.TimeSteps(21)
+    for i, (s, r) in enumerate(zip(sims, ref)):
+        assert np.array_equal(_field(s), _field(r)), i
+    red = b.reduce()
+    for i, (s, r) in enumerate(zip(sims, ref)):
+        assert tuple(red[i]) == pytest.approx(r.Reduce(), rel=1e-15, abs=1e-300)
+    b.close()
 
 
 @pytest.mark.parametrize("kernels", ["auto", "generic"])
