@@ -1,0 +1,587 @@
+"""Phase-diagram relaxation on B200 plans: the stdPFC and logPFC adapters and a batched
+`Get_f_ABC`.
+
+The reference computes a point of a phase diagram by relaxing a 3-mode crystal ansatz
+at a fixed box scale q00 (src/pfc_models/phase_diagram/q0star.py:329-407, `Get_f_ABC`):
+blocks of stepT time units are stepped, the free energy is checked after each block, a
+block that raised f (or went NaN) is rolled back and redone at dt/divs in divs
+sub-blocks (recursively, to maxDepth; :261-307), and the evaluation stops when f and the
+leading amplitude have converged, the fit is poor, the amplitude vanished or totalT ran
+out. A phase diagram is hundreds of such evaluations, each on a small cell grid.
+
+* `StdAdapter` / `LogAdapter` implement the reference adapters' contract
+  (models/stdpfc_cpu/phase_diagram.py:219-296, models/logpfc_cpu/phase_diagram.py:
+  238-321: SLUG, STRUCTURES, validate_*, build, get/set_state, get/set_time, get_dt,
+  step, free_energy, diagnose) on this package's plans, so the reference's own
+  `MinimizeFreeEnergy` can drive them unchanged.
+* `get_f_abc` is `Get_f_ABC` for one point on one plan (also the path for adaptive dt);
+  `get_f_abc_batch` runs many points in lockstep through `simulation.Batch`: one launch
+  per size class and pass for all members, device-side snapshots for the rollbacks, one
+  device-to-host copy of every member's f per block, and the reference's decisions per
+  member on the host. A member whose block must be rolled back leaves the lockstep for
+  that block and runs the recursion on its own plans; a member that stops leaves the
+  batch. Because a batch step is bit-identical to the same steps of the plan alone, the
+  batch returns exactly what `get_f_abc` returns for each point.
+
+The ansatz is built on the host with the reference's NumPy operations
+(`_build3Mode`, stdpfc_cpu/phase_diagram.py:171-182 and logpfc_cpu/phase_diagram.py:
+182-200, the log one rescaled to stay positive), so both start from the same bits; the
+ansatz noise follows q0star.py:227-244 (relative noise from default_rng(seed), mean
+restored).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import diagnostics as _diag
+from . import logpfc as _logpfc
+from . import stdpfc as _stdpfc
+from .spectral import Build2DGeometry
+from .simulation import Batch
+
+# stop reasons (q0star.py:103-109)
+STOP_CONVERGED = 'converged'
+STOP_MAX_DEPTH = 'max_depth'
+STOP_NAN = 'nan'
+STOP_POOR_FIT = 'poor_fit'
+STOP_MIN_AMPLITUDE = 'min_amplitude'
+STOP_TOTALT = 'totalT'
+FAILED_STOPS = (STOP_MAX_DEPTH, STOP_NAN)
+
+
+class MaxDepthReached(RuntimeError):
+    """The rollback recursion reached maxDepth (q0star.py:112-118); `nan` tells whether
+    the last block went NaN."""
+
+    def __init__(self, message, nan=False):
+        super().__init__(message)
+        self.nan = nan
+
+
+@dataclass(frozen=True)
+class RelaxSettings:
+    """Relaxation settings with the reference's names and defaults (q0star.py:124-150)."""
+    dt: float
+    totalT: float
+    stepT: float
+    divs: int
+    maxDepth: int
+    requiredFitness: float | None
+    minimumA: float
+    fTol: float = 1e-12
+    ATol: float = 1e-6
+    seed: int = 0
+    noise: float = 1e-10
+    dtMax: float | None = None
+    dtRate: float = 1e-8
+    dtGrow: float = 2.0
+    dtChecks: int = 10
+
+
+@dataclass
+class RelaxResult:
+    """One evaluation: `Get_f_ABC`'s return (f, fitness, *amplitudes) and what the
+    reference leaves in `last_stop`, `last_steps`, `last_dt_max` and `last_state`."""
+    f: float
+    fitness: float
+    amplitudes: tuple
+    stop: str
+    steps: int
+    dt_max: float
+    state: np.ndarray | None = None
+
+    def values(self):
+        return (self.f, self.fitness, *self.amplitudes)
+
+
+# ---------------------------------------------------------------- adapters
+_PARAM_KEYS = ('beta', 'g', 'v0', 'Gamma', 'q0')
+_ANSATZ_KEYS = ('mode', 'A1', 'A2', 'A3')
+
+
+@dataclass(frozen=True)
+class LogStructure:
+    """A logPFC target lattice: the stdPFC mode sets with the log ansatz's amplitude
+    bound `amplitudeMax` (logpfc_cpu/phase_diagram.py:57-99; honeycomb 1/6)."""
+    name: str
+    kvectors: tuple
+    amplitudeSign: int
+    amplitudeMax: float
+    maxima_per_cell: int | None
+
+
+LOG_STRUCTURES = {
+    name: LogStructure(st.name, st.kvectors, st.amplitudeSign, 1.0 / 6 if name == 'honeycomb' else st.amplitudeScale,
+                       st.maxima_per_cell)
+    for name, st in _diag.STRUCTURES.items()
+}
+
+
+class _Adapter:
+    """The adapter contract shared by both models; subclasses set the model."""
+    SLUG = None
+    STRUCTURES = None
+    FIELD = None
+
+    def __init__(self, precision='fp64', device=None):
+        self.precision = precision
+        self.device = device
+
+    # -- validation (stdpfc_cpu/phase_diagram.py:104-154)
+    def validate_params(self, params):
+        p = dict(params)
+        unknown = sorted(set(p) - set(_PARAM_KEYS))
+        if unknown:
+            raise ValueError(f'{self.SLUG}: unknown model parameters {unknown}; allowed {list(_PARAM_KEYS)}')
+        missing = [k for k in ('beta', 'g') if k not in p]
+        if missing:
+            raise ValueError(f'{self.SLUG}: missing model parameters {missing}')
+        v0 = float(p.get('v0', 1.0))
+        if v0 != 1.0:
+            raise ValueError(f'{self.SLUG}: v0={v0} not supported; the quartic coefficient is 1 in the step')
+        return {'beta': float(p['beta']), 'g': float(p['g']), 'v0': 1.0,
+                'Gamma': float(p.get('Gamma', 1.0)), 'q0': float(p.get('q0', 1.0))}
+
+    def validate_cell(self, cell):
+        try:
+            return _diag._cell(cell)
+        except ValueError as e:
+            raise ValueError(f'{self.SLUG}: {e}') from None
+
+    def validate_ansatz(self, ansatz):
+        a = dict(ansatz)
+        if sorted(a) != sorted(_ANSATZ_KEYS):
+            raise ValueError(f'{self.SLUG}: ansatz needs exactly {list(_ANSATZ_KEYS)}, got {sorted(a)}')
+        if not isinstance(a['mode'], str):
+            raise ValueError(f'{self.SLUG}: ansatz mode must be a string label')
+        return {'mode': a['mode'], 'A1': float(a['A1']), 'A2': float(a['A2']), 'A3': float(a['A3'])}
+
+    def _structure(self, structure):
+        return self.STRUCTURES[structure] if isinstance(structure, str) else structure
+
+    # -- box and ansatz
+    @staticmethod
+    def box(cell, q00):
+        """Rectangular cell of the triangular lattice with its first shell at q00
+        (stdpfc_cpu/phase_diagram.py:161-167)."""
+        nx, ny = cell['uNx'] * cell['Mx'], cell['uNy'] * cell['My']
+        a = 4 * np.pi / (3 ** 0.5 * q00)
+        h = 4 * np.pi / q00
+        return Build2DGeometry(Nx=nx, Ny=ny, Lx=cell['Mx'] * a, Ly=cell['My'] * h)
+
+    @staticmethod
+    def three_mode(structure, cell, mean, A, B, C):
+        """The field with the given mean and 1-, 2-, 3-mode amplitudes, by the inverse
+        real FFT of the sparse spectrum (stdpfc_cpu/phase_diagram.py:171-182)."""
+        nx, ny = cell['uNx'] * cell['Mx'], cell['uNy'] * cell['My']
+        size = nx * ny
+        hat = np.zeros((ny, nx), dtype=complex)
+        hat[0, 0] = mean * size
+        for pos, amp in zip(structure.kvectors, (A, B, C)):
+            rows, cols = np.array(pos).T
+            hat[rows * cell['My'], cols * cell['Mx']] = amp * size
+        return np.fft.irfftn(hat, s=(ny, nx), axes=(0, 1)).real
+
+    # -- contract
+    def build(self, params, structure, cell, ansatz, temp, meanDensity, q00, dt, state=None, nThreads=1):
+        """Model + box at q00 + (the ansatz if state is None, else the state) -> Simulation."""
+        params = self.validate_params(params)
+        structure = self._structure(structure)
+        cell = self.validate_cell(cell)
+        ansatz = self.validate_ansatz(ansatz)
+        field = self.ansatz_field(structure, cell, ansatz, meanDensity) if state is None else state
+        sim = self._simulation(params, temp, dt, meanDensity, self.box(cell, q00))
+        getattr(sim.State, self.FIELD)[...] = field
+        return sim
+
+    def get_state(self, sim):
+        return sim.plan.get_state().cpu().numpy()
+
+    def set_state(self, sim, state):
+        getattr(sim.State, self.FIELD)[...] = state
+
+    def get_time(self, sim):
+        return sim.t
+
+    def set_time(self, sim, t):
+        sim.State.t = t
+
+    def get_dt(self, sim):
+        return sim.Model.dt
+
+    def step(self, sim):
+        sim.TimeStep()
+
+    def free_energy(self, sim):
+        return sim.CalculateFreeEnergy()
+
+    # -- hooks of the relaxation driver (optional in an adapter; see _hook)
+    def step_many(self, sim, n):
+        """n steps in one call (graph replay, no host round trip between steps)."""
+        sim.TimeSteps(n)
+
+    def snapshot(self, sim, out=None):
+        """The state as a device array (into `out` when given); `set_state` takes it back."""
+        return sim.plan.get_state(out)
+
+    def release(self, sim):
+        sim.plan.close()
+
+    def lockstep(self, sims):
+        return _PlanLockstep(sims)
+
+
+class _PlanLockstep:
+    """Simulations stepped together through one `Batch`; F of all of them in one copy."""
+
+    def __init__(self, sims):
+        self.batch = Batch(sims)
+
+    def step(self, n):
+        self.batch.step(n)
+
+    def free_energies(self):
+        return self.batch.reduce()[:, 0]
+
+    def close(self):
+        self.batch.close()
+
+
+class _LoopLockstep:
+    """The same interface for an adapter without batches: one member after another."""
+
+    def __init__(self, ad, sims):
+        self.ad, self.sims = ad, list(sims)
+
+    def step(self, n):
+        for sim in self.sims:
+            _steps(self.ad, sim, n)
+
+    def free_energies(self):
+        return np.array([self.ad.free_energy(sim) for sim in self.sims], dtype=float)
+
+    def close(self):
+        pass
+
+
+def _steps(ad, sim, n):
+    if hasattr(ad, 'step_many'):
+        ad.step_many(sim, n)
+    else:
+        for _ in range(n):
+            ad.step(sim)
+
+
+def _snapshot(ad, sim, out=None):
+    return ad.snapshot(sim, out) if hasattr(ad, 'snapshot') else ad.get_state(sim)
+
+
+def _release(ad, sim):
+    if hasattr(ad, 'release'):
+        ad.release(sim)
+
+
+def _lockstep(ad, sims):
+    return ad.lockstep(sims) if hasattr(ad, 'lockstep') else _LoopLockstep(ad, sims)
+
+
+class StdAdapter(_Adapter):
+    """stdPFC adapter (models/stdpfc_cpu/phase_diagram.py): absolute amplitudes, no
+    rescale of the ansatz."""
+    SLUG = 'stdpfc_b200'
+    STRUCTURES = _diag.STRUCTURES
+    FIELD = 'n'
+
+    def ansatz_field(self, structure, cell, ansatz, mean):
+        s = structure.amplitudeSign * structure.amplitudeScale
+        return self.three_mode(structure, cell, mean, s * ansatz['A1'], s * ansatz['A2'], s * ansatz['A3'])
+
+    def _simulation(self, params, temp, dt, mean, geometry):
+        model = _stdpfc.BuildStdPFCModelParameters(Gamma=params['Gamma'], beta=params['beta'], q0=params['q0'],
+                                                   epsilon=temp, g=params['g'], dt=dt, meanDensity=mean)
+        return _stdpfc.BuildB200_Simulation(model, geometry, precision=self.precision, device=self.device)
+
+    def diagnose(self, sim, structure, cell):
+        """fitness, (|A|, |B|, |C|) and maxima per cell on the device
+        (stdpfc_cpu/phase_diagram.py:286-296)."""
+        d = _diag.diagnose(sim, self._structure(structure), self.validate_cell(cell))
+        return _diag.Diagnostics(d.fitness, d.amplitudes, {'maxima_per_cell': d.details['maxima_per_cell']})
+
+
+class LogAdapter(_Adapter):
+    """logPFC adapter (models/logpfc_cpu/phase_diagram.py): amplitudes in units of the
+    mean density, the 3-mode field rescaled towards the mean where it would go negative."""
+    SLUG = 'logpfc_b200'
+    STRUCTURES = LOG_STRUCTURES
+    FIELD = 'phi'
+
+    @classmethod
+    def _positive(cls, field, mean):
+        low = field.min()
+        if low < 0:     # logpfc_cpu/phase_diagram.py:196-199
+            field = mean + (field - mean) * mean / (mean - low)
+        return field
+
+    def ansatz_field(self, structure, cell, ansatz, mean):
+        s = structure.amplitudeSign * structure.amplitudeMax * mean
+        return self._positive(self.three_mode(structure, cell, mean, s * ansatz['A1'], s * ansatz['A2'],
+                                              s * ansatz['A3']), mean)
+
+    def _simulation(self, params, temp, dt, mean, geometry):
+        model = _logpfc.BuildLogPFCModelParameters(Gamma=params['Gamma'], beta=params['beta'], q0=params['q0'],
+                                                   epsilon=temp, g=params['g'], dt=dt, meanDensity=mean)
+        return _logpfc.BuildB200_Simulation(model, geometry, precision=self.precision, device=self.device)
+
+    def diagnose(self, sim, structure, cell):
+        """logpfc_cpu/phase_diagram.py:211-223, 309-321: the device's absolute amplitudes
+        divided by the mean. Where the rebuilt 3-mode field stays non-negative (its
+        minimum is taken on the host from the four numbers) the fitness is the device's;
+        where the reference would rescale it, the fitness is recomputed from a host copy
+        of the field against the rescaled 3-mode field."""
+        st, c = self._structure(structure), self.validate_cell(cell)
+        d = _diag.diagnose(sim, st, c)
+        mean = d.details['mean']
+        amps = tuple(abs(a / mean) for a in d.amplitudes)
+        sign = st.amplitudeSign
+        rebuilt = self.three_mode(st, c, mean, *(sign * a * mean for a in amps))
+        fitness = d.fitness
+        if rebuilt.min() < 0:
+            field = sim.plan.get_state().cpu().numpy()
+            rebuilt = self._positive(rebuilt, mean)
+            fitness = 1 - float(np.abs(np.power(field - rebuilt, 2).mean()))
+        return _diag.Diagnostics(fitness, amps, {'maxima_per_cell': d.details['maxima_per_cell']})
+
+
+# ---------------------------------------------------------------- one evaluation
+class _Run:
+    """Settings of one set of evaluations (the MinimizeFreeEnergy attributes the
+    relaxation reads, q0star.py:174-224)."""
+
+    def __init__(self, adapter, params, structure, cell, ansatz, relax):
+        self.ad = adapter
+        self.params = adapter.validate_params(params)
+        self.structure = adapter._structure(structure)
+        self.cell = adapter.validate_cell(cell)
+        self.ansatz = adapter.validate_ansatz(ansatz)
+        self.relax = relax
+
+    def generate(self, temp, mean, q00, dt, state=None):
+        """q0star.py:227-252: build, and add the seeded relative noise to a fresh ansatz."""
+        ad, r = self.ad, self.relax
+        sim = ad.build(self.params, self.structure, self.cell, self.ansatz, temp, mean, q00, dt, state=state)
+        if state is None and r.noise:
+            rng = np.random.default_rng(r.seed)
+            phi = ad.get_state(sim)
+            m = phi.mean()
+            phi = phi * (1.0 + r.noise * rng.standard_normal(phi.shape))
+            ad.set_state(sim, phi + (m - phi.mean()))
+        return sim
+
+    def amplitude(self, sim):
+        return self.ad.diagnose(sim, self.structure, self.cell).amplitudes[0]
+
+    def take_step(self, sim, point, stepT, depth, counter, f_last=None):
+        """One block on one plan with the rollback recursion (q0star.py:261-307); returns
+        delta f. `counter` is a one-element list of steps taken."""
+        ad, r = self.ad, self.relax
+        dt = ad.get_dt(sim)
+        mini = int(round(stepT / dt))
+        phi_last = _snapshot(ad, sim)
+        t_last = ad.get_time(sim)
+        f_last = ad.free_energy(sim) if f_last is None else f_last
+        _steps(ad, sim, mini)
+        counter[0] += mini
+        f = ad.free_energy(sim)
+        delta_f = f - f_last
+        if np.isnan(f) or delta_f > r.fTol * abs(f_last):
+            return self.rollback(sim, point, stepT, depth, counter, phi_last, t_last, f_last, bool(np.isnan(f)))
+        return delta_f
+
+    def rollback(self, sim, point, stepT, depth, counter, phi_last, t_last, f_last, nan):
+        """Restore the block's start and redo it at dt/divs in divs sub-blocks
+        (q0star.py:278-305)."""
+        ad, r = self.ad, self.relax
+        ad.set_state(sim, phi_last)
+        ad.set_time(sim, t_last)
+        if depth >= r.maxDepth:
+            raise MaxDepthReached(f'Max recursion depth reached at t={ad.get_time(sim):0.6f}', nan=nan)
+        divs = r.divs
+        sub = self.generate(*point, ad.get_dt(sim) / divs, state=phi_last)
+        try:
+            ad.set_time(sub, ad.get_time(sim))
+            for _ in range(divs):
+                self.take_step(sub, point, stepT / divs, depth + 1, counter)
+                ad.set_state(sim, _snapshot(ad, sub))
+                ad.set_time(sim, ad.get_time(sub))
+        finally:
+            _release(ad, sub)
+        return ad.free_energy(sim) - f_last
+
+    def adapt_dt(self, sim, point, stepT, delta_f, f, A, A_last, dt_max):
+        """q0star.py:309-327: the next block's dt from the block's relative rate; a new
+        plan only where dt changes. Returns (sim, dt_max)."""
+        ad, r = self.ad, self.relax
+        dt = ad.get_dt(sim)
+        rate = max(abs(delta_f) / max(abs(f), 1e-300), abs(A - A_last) / max(A, 1e-300)) / stepT
+        target = r.dtMax / np.sqrt(1.0 + (rate / r.dtRate) ** 2)
+        target = min(max(target, r.dt), r.dtMax, dt * r.dtGrow)
+        mini = int(np.ceil(stepT / target - 1e-9))
+        new = stepT / mini
+        if abs(new - dt) <= 1e-12 * dt:
+            return sim, dt_max
+        t = ad.get_time(sim)
+        fresh = self.generate(*point, new, state=_snapshot(ad, sim))
+        ad.set_time(fresh, t)
+        _release(ad, sim)
+        return fresh, max(dt_max, new)
+
+    def first_dt(self):
+        r = self.relax
+        return r.stepT / int(np.ceil(r.stepT / r.dt))
+
+    def check(self, sim, delta_f, f_last, A_last):
+        """The stop tests after a block (q0star.py:384-398): (stop or None, A)."""
+        r = self.relax
+        diag = self.ad.diagnose(sim, self.structure, self.cell)
+        fitness, A = diag.fitness, diag.amplitudes[0]
+        if r.requiredFitness is not None and fitness < r.requiredFitness:
+            return STOP_POOR_FIT, A
+        if A < r.minimumA:
+            return STOP_MIN_AMPLITUDE, A
+        if abs(delta_f) <= r.fTol * abs(f_last) and abs(A - A_last) <= r.ATol * A:
+            return STOP_CONVERGED, A
+        return None, A
+
+    def finish(self, sim, stop, steps, dt_max, keep_state):
+        f = self.ad.free_energy(sim)
+        diag = self.ad.diagnose(sim, self.structure, self.cell)
+        state = self.ad.get_state(sim) if keep_state else None
+        return RelaxResult(float(f), float(diag.fitness), tuple(float(a) for a in diag.amplitudes), stop, steps,
+                           float(dt_max), state)
+
+
+def get_f_abc(adapter, params, structure, cell, ansatz, relax, temp, meanDensity, q00, state=None,
+              keep_state=False):
+    """`Get_f_ABC` (q0star.py:329-407) for one point on one plan; returns a RelaxResult."""
+    run = _Run(adapter, params, structure, cell, ansatz, relax)
+    return _single(run, (temp, meanDensity, q00), state, keep_state)
+
+
+def _single(run, point, state, keep_state):
+    ad, r = run.ad, run.relax
+    blocks = int(r.totalT / r.stepT)
+    sim = run.generate(*point, run.first_dt(), state=state)
+    try:
+        f_last = ad.free_energy(sim)
+        A_last = run.amplitude(sim)
+        stop, counter, dt_max = STOP_TOTALT, [0], ad.get_dt(sim)
+        for _ in range(blocks):
+            try:
+                if r.dtMax is None:
+                    delta_f = run.take_step(sim, point, r.stepT, 0, counter, f_last)
+                else:       # sub-blocks with dt adapted after each (q0star.py:362-372)
+                    f0, sub_t = f_last, r.stepT / r.dtChecks
+                    As = A_last
+                    for k in range(r.dtChecks):
+                        d_sub = run.take_step(sim, point, sub_t, 0, counter)
+                        fs_new = ad.free_energy(sim)
+                        As_new = run.amplitude(sim)
+                        if k < r.dtChecks - 1:
+                            sim, dt_max = run.adapt_dt(sim, point, sub_t, d_sub, fs_new, As_new, As, dt_max)
+                        As = As_new
+                    delta_f = ad.free_energy(sim) - f0
+            except MaxDepthReached as e:
+                stop = STOP_NAN if e.nan else STOP_MAX_DEPTH
+                break
+            f_last = ad.free_energy(sim)
+            reason, A = run.check(sim, delta_f, f_last, A_last)
+            if reason is not None:
+                stop = reason
+                break
+            if r.dtMax is not None:
+                sim, dt_max = run.adapt_dt(sim, point, r.stepT / r.dtChecks, delta_f / r.dtChecks, f_last, A,
+                                           A_last, dt_max)
+            A_last = A
+        return run.finish(sim, stop, counter[0], dt_max, keep_state)
+    finally:
+        _release(ad, sim)
+
+
+# ---------------------------------------------------------------- many evaluations
+class _Member:
+    def __init__(self, index, point, sim, f_last, A_last):
+        self.index, self.point, self.sim = index, point, sim
+        self.f_last, self.A_last = f_last, A_last
+        self.counter = [0]
+        self.snapshot = None
+
+
+def get_f_abc_batch(adapter, params, structure, cell, ansatz, relax, points, states=None, keep_state=False):
+    """`Get_f_ABC` for every (temp, meanDensity, q00) of `points`, the members stepped
+    together (see the module docstring). Returns RelaxResults in the order of `points`,
+    each equal to what `get_f_abc` returns for that point. With adaptive dt
+    (relax.dtMax set) every member has its own dt schedule, so the points run one after
+    another through `get_f_abc`."""
+    run = _Run(adapter, params, structure, cell, ansatz, relax)
+    points = [tuple(float(v) for v in p) for p in points]
+    states = [None] * len(points) if states is None else list(states)
+    if len(states) != len(points):
+        raise ValueError('states must match points')
+    if relax.dtMax is not None:
+        return [_single(run, p, s, keep_state) for p, s in zip(points, states)]
+    ad, r = run.ad, run.relax
+    dt = run.first_dt()
+    mini = int(round(r.stepT / dt))
+    results = [None] * len(points)
+    members = []
+    batch, in_batch = None, None
+    try:
+        for i, (p, s) in enumerate(zip(points, states)):
+            sim = run.generate(*p, dt, state=s)
+            members.append(_Member(i, p, sim, ad.free_energy(sim), run.amplitude(sim)))
+        active = list(members)
+        for _ in range(int(r.totalT / r.stepT)):
+            if not active:
+                break
+            if in_batch != [m.index for m in active]:
+                if batch is not None:
+                    batch.close()
+                batch = _lockstep(ad, [m.sim for m in active])
+                in_batch = [m.index for m in active]
+            for m in active:
+                m.snapshot = _snapshot(ad, m.sim, m.snapshot)
+                m.t_last = ad.get_time(m.sim)
+            batch.step(mini)
+            fs = batch.free_energies()
+            still = []
+            for m, f in zip(active, fs):
+                m.counter[0] += mini
+                delta_f = f - m.f_last
+                stop = None
+                if np.isnan(f) or delta_f > r.fTol * abs(m.f_last):
+                    try:
+                        delta_f = run.rollback(m.sim, m.point, r.stepT, 0, m.counter, m.snapshot, m.t_last,
+                                               m.f_last, bool(np.isnan(f)))
+                    except MaxDepthReached as e:
+                        stop = STOP_NAN if e.nan else STOP_MAX_DEPTH
+                    if stop is None:
+                        f = ad.free_energy(m.sim)
+                if stop is None:
+                    m.f_last = f
+                    stop, A = run.check(m.sim, delta_f, m.f_last, m.A_last)
+                    m.A_last = A
+                if stop is None:
+                    still.append(m)
+                else:
+                    results[m.index] = run.finish(m.sim, stop, m.counter[0], dt, keep_state)
+            active = still
+        for m in active:
+            results[m.index] = run.finish(m.sim, STOP_TOTALT, m.counter[0], dt, keep_state)
+        return results
+    finally:
+        if batch is not None:
+            batch.close()
+        for m in members:
+            _release(ad, m.sim)

@@ -1,0 +1,258 @@
+"""Batched Get_f_ABC relaxation (pfc_models_b200.phase_diagram) against the reference's
+phase_diagram/q0star.py:261-407.
+
+CPU: the driver's decisions (convergence, rollback to dt/divs, NaN and depth stops,
+poor fit, the amplitude guard, adaptive dt) on a toy adapter whose f and amplitudes are
+closed-form functions of time; the batched driver must return exactly what the
+one-point driver returns for every point, rollbacks included.
+
+GPU: the logPFC adapter on B200 plans at the three points that the reference's own test
+pins (tests/test_phase_diagram_q0star.py:44-58, 489-510: MinimizeFreeEnergy.Get_f_ABC
+with run_vals[2] on the 14 x 24, 2 x 1 cell, beta 0.5, g -2): the stop, the step count
+exactly (2000, 2000, and 22000 for the honeycomb, whose dt = 0.1 blocks go NaN and are
+redone at dt 0.01), f within 1e-12 absolute (the reference test's bound for its
+honeycomb value; the converged f differ here only by the FFT's round-off), fitness and
+amplitudes within 1e-12 absolute (the reference test's bound). The same three points as
+one batch must give the one-point results bit for bit.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from pfc_models_b200 import phase_diagram as pd
+
+
+# ---------------------------------------------------------------- toy model
+class _Diag:
+    def __init__(self, fitness, amplitudes):
+        self.fitness, self.amplitudes, self.details = fitness, amplitudes, {}
+
+
+class _Toy:
+    def __init__(self, floor, fitness, dt, state, regime):
+        self.floor, self.fitness, self.dt, self.x, self.t, self.regime = floor, fitness, dt, state, 0.0, regime
+
+
+class ToyAdapter:
+    """f = floor(q00) + |x|^2 with x decaying by (1 - dt/2) per step; regimes by mean
+    density: 0.75 goes NaN after t = 5 unless dt <= 0.05, 0.9 goes NaN after t = 5 at
+    any dt, 0.6 keeps f fixed while the amplitude grows as 3e-6 e^t up to 0.3."""
+    QSTAR = 1.03
+    T_BAD = 5.0
+    DT_OK = 0.05
+
+    def __init__(self):
+        self.dts, self.from_state, self.steps = [], 0, 0
+
+    def validate_params(self, p):
+        return dict(p)
+
+    def validate_cell(self, c):
+        return dict(c)
+
+    def validate_ansatz(self, a):
+        return dict(a)
+
+    def _structure(self, s):
+        return s
+
+    def build(self, params, structure, cell, ansatz, temp, meanDensity, q00, dt, state=None, nThreads=1):
+        self.dts.append(dt)
+        regime = {0.75: 'stiff', 0.9: 'nan', 0.6: 'seed'}.get(meanDensity, 'plain')
+        floor = temp + meanDensity ** 2 + (q00 - self.QSTAR) ** 2
+        x = np.full(4, 0.0 if regime == 'seed' else 0.5) if state is None else np.array(state)
+        if state is not None:
+            self.from_state += 1
+        return _Toy(floor, 1.0 - (q00 - self.QSTAR) ** 2, dt, x, regime)
+
+    def get_state(self, sim):
+        return sim.x.copy()
+
+    def set_state(self, sim, state):
+        sim.x[...] = state
+
+    def get_time(self, sim):
+        return sim.t
+
+    def set_time(self, sim, t):
+        sim.t = t
+
+    def get_dt(self, sim):
+        return sim.dt
+
+    def step(self, sim):
+        self.steps += 1
+        sim.x *= 1 - 0.5 * sim.dt
+        sim.t += sim.dt
+        if sim.t >= self.T_BAD and (sim.regime == 'nan' or (sim.regime == 'stiff' and sim.dt > self.DT_OK)):
+            sim.x[...] = np.nan
+
+    def free_energy(self, sim):
+        return sim.floor + float(np.mean(sim.x ** 2))
+
+    def diagnose(self, sim, structure, cell):
+        a = min(0.3, 3e-6 * math.exp(sim.t)) if sim.regime == 'seed' else 0.3
+        return _Diag(sim.fitness, (a, 0.0))
+
+
+TOY = pd.RelaxSettings(dt=0.1, totalT=1e4, stepT=10.0, divs=10, maxDepth=4, requiredFitness=0.99, minimumA=1e-6)
+
+
+def _one(ad, rho, q00=1.0, relax=TOY):
+    return pd.get_f_abc(ad, {}, 'blob', {}, {}, relax, 0.1, rho, q00)
+
+
+def test_converges_in_whole_blocks():
+    ad = ToyAdapter()
+    r = _one(ad, 0.5)
+    assert r.stop == pd.STOP_CONVERGED
+    assert r.f == pytest.approx(0.1 + 0.25 + (1.0 - ToyAdapter.QSTAR) ** 2, abs=1e-11)
+    assert r.steps == ad.steps and r.steps % 100 == 0 and ad.from_state == 0
+
+
+def test_rollback_redoes_the_block_at_dt_over_divs():
+    ad = ToyAdapter()
+    r = _one(ad, 0.75)
+    assert r.stop == pd.STOP_CONVERGED and np.isfinite(r.f)
+    assert min(ad.dts) == pytest.approx(0.01) and ad.from_state >= 1
+    assert r.steps == ad.steps
+
+
+def test_nan_at_every_dt_stops_at_max_depth():
+    ad = ToyAdapter()
+    r = _one(ad, 0.9)
+    assert r.stop == pd.STOP_NAN and np.isfinite(r.f)
+    assert min(ad.dts) == pytest.approx(TOY.dt / TOY.divs ** TOY.maxDepth)
+
+
+def test_amplitude_guard_waits_for_a_growing_seed():
+    r = _one(ToyAdapter(), 0.6)        # A: 0.066 at t = 10, 0.3 at t = 20 and 30
+    assert r.stop == pd.STOP_CONVERGED and r.amplitudes[0] == 0.3 and r.steps == 300
+
+
+def test_poor_fit_and_minimum_amplitude_stops():
+    assert _one(ToyAdapter(), 0.5, q00=1.3).stop == pd.STOP_POOR_FIT      # fitness 1 - 0.27^2
+    relax = pd.RelaxSettings(dt=0.1, totalT=1e4, stepT=10.0, divs=10, maxDepth=4, requiredFitness=None,
+                             minimumA=0.5)
+    assert _one(ToyAdapter(), 0.5, relax=relax).stop == pd.STOP_MIN_AMPLITUDE
+
+
+def test_total_time_stop():
+    relax = pd.RelaxSettings(dt=0.1, totalT=20.0, stepT=10.0, divs=10, maxDepth=4, requiredFitness=None,
+                             minimumA=1e-6)
+    r = _one(ToyAdapter(), 0.6, relax=relax)
+    assert r.stop == pd.STOP_TOTALT and r.steps == 200
+
+
+def test_adaptive_dt_grows_the_step():
+    relax = pd.RelaxSettings(dt=0.1, totalT=1e4, stepT=10.0, divs=10, maxDepth=4, requiredFitness=0.99,
+                             minimumA=1e-6, dtMax=1.0)
+    r = _one(ToyAdapter(), 0.5, relax=relax)
+    assert r.stop == pd.STOP_CONVERGED and r.dt_max > 0.1
+
+
+def test_batch_returns_the_one_point_results():
+    points = [(0.1, 0.5, 1.0), (0.1, 0.75, 1.0), (0.1, 0.9, 1.0), (0.1, 0.6, 1.0), (0.1, 0.5, 1.3),
+              (0.2, 0.5, 0.98)]
+    ad = ToyAdapter()
+    got = pd.get_f_abc_batch(ad, {}, 'blob', {}, {}, TOY, points)
+    batch_steps = ad.steps
+    want, total = [], 0
+    for p in points:
+        one = ToyAdapter()
+        want.append(pd.get_f_abc(one, {}, 'blob', {}, {}, TOY, *p))
+        total += one.steps
+    for g, w in zip(got, want):
+        assert (g.values(), g.stop, g.steps, g.dt_max) == (w.values(), w.stop, w.steps, w.dt_max)
+    assert batch_steps == total == sum(g.steps for g in got)
+    assert [g.stop for g in got] == [pd.STOP_CONVERGED, pd.STOP_CONVERGED, pd.STOP_NAN, pd.STOP_CONVERGED,
+                                     pd.STOP_POOR_FIT, pd.STOP_CONVERGED]
+
+
+def test_adapter_validation_and_log_ansatz():
+    ad = pd.LogAdapter()
+    with pytest.raises(ValueError, match='v0'):
+        ad.validate_params({'beta': 1.0, 'g': 0.0, 'v0': 2.0})
+    with pytest.raises(ValueError, match='missing'):
+        ad.validate_params({'beta': 1.0})
+    with pytest.raises(ValueError, match='cell'):
+        ad.validate_cell({'uNx': 14, 'uNy': 24, 'Mx': 2})
+    with pytest.raises(ValueError, match='ansatz'):
+        ad.validate_ansatz({'mode': 'L2H', 'A1': 1.0})
+    cell = dict(uNx=14, uNy=24, Mx=2, My=1)
+    st = ad.STRUCTURES['triangle']
+    # a large ansatz is rescaled towards the mean until its minimum is zero
+    big = ad.ansatz_field(st, cell, dict(mode='H2L', A1=3.0, A2=1.0, A3=0.5), 0.5)
+    assert big.min() == pytest.approx(0.0, abs=1e-15) and big.mean() == pytest.approx(0.5, abs=1e-15)
+    small = ad.ansatz_field(st, cell, dict(mode='L2H', A1=1e-5, A2=1e-6, A3=1e-7), 0.63)
+    assert small.min() > 0.62
+    assert pd.LOG_STRUCTURES['honeycomb'].amplitudeMax == 1.0 / 6
+    g = ad.box(cell, 1.0)
+    assert (g.Nx, g.Ny) == (28, 24) and g.Lx == pytest.approx(2 * 4 * math.pi / math.sqrt(3))
+
+
+# ---------------------------------------------------------------- B200 plans
+RELAX = pd.RelaxSettings(dt=0.1, totalT=1e6, stepT=1e2, divs=10, maxDepth=4, requiredFitness=0.99, minimumA=1e-6)
+CELL = dict(uNx=14, uNy=24, Mx=2, My=1)
+ANSATZ = dict(mode='L2H', A1=1e-5, A2=1e-6, A3=1e-7)
+LOG_PARAMS = dict(beta=0.5, g=-2.0, v0=1.0)
+# structure, eps, phi, q00, f, fitness, A, B, C, steps: the reference test's pinned values
+PINNED = [
+    ('triangle', -0.9, 0.63, 0.9638831589013295, -0.553594984894113, 0.9997633941916881, 0.33320928950407136,
+     0.03198014374195086, 0.003245425514830756, 2000),
+    ('honeycomb', -0.9, 1.2, 1.0, -0.7600664077521084, None, None, None, None, 22000),
+    ('stripe', -0.9, 0.88, 1.0, -0.6617397486488582, 0.99983068778873, 0.4718018020045463, 0.021804312871064338,
+     0.005226927920294405, 2000),
+]
+
+
+def _check_pinned(r, ref):
+    structure, _, _, _, f, fitness, A, B, C, steps = ref
+    assert r.stop == pd.STOP_CONVERGED, structure
+    assert r.steps == steps, structure
+    assert r.f == pytest.approx(f, abs=1e-12), structure
+    if fitness is not None:
+        assert (r.fitness, *r.amplitudes) == pytest.approx((fitness, A, B, C), abs=1e-12), structure
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('ref', PINNED, ids=[p[0] for p in PINNED])
+def test_log_get_f_abc_matches_the_reference_pins(ref):
+    structure, eps, phi, q00 = ref[:4]
+    r = pd.get_f_abc(pd.LogAdapter(), LOG_PARAMS, structure, CELL, ANSATZ, RELAX, eps, phi, q00)
+    _check_pinned(r, ref)
+
+
+@pytest.mark.gpu
+def test_log_batch_equals_one_point_runs_bit_for_bit():
+    """The three pinned points and two more q00 of the triangle, one batch per
+    structure, against the one-point driver."""
+    ad = pd.LogAdapter()
+    for structure in ('triangle', 'honeycomb', 'stripe'):
+        refs = [p for p in PINNED if p[0] == structure]
+        points = [p[1:4] for p in refs]
+        if structure == 'triangle':
+            points += [(-0.9, 0.63, 0.95), (-0.9, 0.63, 0.98)]
+        got = pd.get_f_abc_batch(ad, LOG_PARAMS, structure, CELL, ANSATZ, RELAX, points)
+        for g, p in zip(got, points):
+            w = pd.get_f_abc(ad, LOG_PARAMS, structure, CELL, ANSATZ, RELAX, *p)
+            assert (g.values(), g.stop, g.steps) == (w.values(), w.stop, w.steps), (structure, p)
+        _check_pinned(got[0], refs[0])
+
+
+@pytest.mark.gpu
+def test_std_adapter_relaxes_a_triangle():
+    """stdPFC through the same driver: a 16 x 28 cell at eps -0.25, nbar -0.25 relaxes to a
+    converged triangle whose fitness and first amplitude the device and the host agree on."""
+    ad = pd.StdAdapter()
+    relax = pd.RelaxSettings(dt=0.5, totalT=2e4, stepT=50.0, divs=10, maxDepth=3, requiredFitness=0.9,
+                             minimumA=1e-6)
+    cell = dict(uNx=16, uNy=28, Mx=1, My=1)
+    params = dict(beta=1.0, g=0.0)
+    ansatz = dict(mode='L2H', A1=0.5, A2=0.0, A3=0.0)
+    r = pd.get_f_abc(ad, params, 'triangle', cell, ansatz, relax, -0.25, -0.25, 1.0, keep_state=True)
+    assert r.stop == pd.STOP_CONVERGED
+    assert r.fitness > 0.99 and r.amplitudes[0] > 0.05
+    b = pd.get_f_abc_batch(ad, params, 'triangle', cell, ansatz, relax, [(-0.25, -0.25, 1.0), (-0.25, -0.25, 0.97)])
+    assert (b[0].values(), b[0].steps) == (r.values(), r.steps)
