@@ -22,6 +22,9 @@ out. A phase diagram is hundreds of such evaluations, each on a small cell grid.
   that block and runs the recursion on its own plans; a member that stops leaves the
   batch. Because a batch step is bit-identical to the same steps of the plan alone, the
   batch returns exactly what `get_f_abc` returns for each point.
+* `find_q0star_batch` is `Find_q0Star` (q0star.py:409-478: passes of q00 scans refined
+  by a cubic spline of f(q00)) for many (temp, meanDensity) at once, each pass one
+  `get_f_abc_batch` over every target's q00 points; `find_q0star` is the one-target form.
 
 The ansatz is built on the host with the reference's NumPy operations
 (`_build3Mode`, stdpfc_cpu/phase_diagram.py:171-182 and logpfc_cpu/phase_diagram.py:
@@ -585,3 +588,133 @@ def get_f_abc_batch(adapter, params, structure, cell, ansatz, relax, points, sta
             batch.close()
         for m in members:
             _release(ad, m.sim)
+
+
+# ---------------------------------------------------------------- q0* search
+MSG_INSUFFICIENT_POINTS = 'Insufficient points found that satisfy fitness constraints.'
+MSG_NO_LOCAL_MINIMUM = 'No local minimum found for q00.'
+STATUS_OK = 'ok'
+STATUS_INSUFFICIENT_POINTS = 'insufficient_points'
+STATUS_NO_LOCAL_MINIMUM = 'no_local_minimum'
+
+
+class InsufficientPoints(Exception):
+    """Too few accepted q00 points (q0star.py:87-88)."""
+
+
+class NoLocalMinimum(Exception):
+    """The spline of f(q00) has no usable minimum (q0star.py:91-92)."""
+
+
+@dataclass(frozen=True)
+class QScanSettings:
+    """q00 scan settings with the reference's names and defaults (q0star.py:153-164)."""
+    passes: int
+    Deltaq: float
+    q00_Steps: int
+    Deltaq_Refinement: float
+    q00_start: float = 1.0
+    minPoints: int = 5
+
+
+@dataclass
+class Q0StarResult:
+    """One (temp, meanDensity): q0*, f at q0*, and the status and message that the
+    reference's scan_density records for it (NaN q0* and fmin unless the status is ok)."""
+    temp: float
+    meanDensity: float
+    q0star: float
+    fmin: float
+    status: str
+    message: str
+
+
+def _q_range(q_best, dq, n):
+    return np.linspace(q_best - n // 2 * dq, q_best + n // 2 * dq, n, endpoint=True)
+
+
+def _refine(q00_range, f_values, fit_values, A_values, relax, min_points):
+    """One pass's decision (q0star.py:441-478): accept the points whose fitness and
+    amplitude pass, spline f over the contiguous accepted run around the lowest accepted
+    f, and return (the minimum of the spline nearest that point, the spline)."""
+    from scipy.interpolate import CubicSpline
+    rf = -np.inf if relax.requiredFitness is None else relax.requiredFitness
+    accepted = (fit_values >= rf) & (A_values >= relax.minimumA)
+    if q00_range[accepted].size < min_points:
+        raise InsufficientPoints(MSG_INSUFFICIENT_POINTS)
+    q_min = q00_range[accepted][np.argmin(f_values[accepted])]
+    i_min = np.flatnonzero(accepted)[np.argmin(f_values[accepted])]
+    lo, hi = i_min, i_min
+    while lo > 0 and accepted[lo - 1]:
+        lo -= 1
+    while hi < accepted.size - 1 and accepted[hi + 1]:
+        hi += 1
+    if hi - lo + 1 < min_points:
+        raise InsufficientPoints(MSG_INSUFFICIENT_POINTS)
+    spline = CubicSpline(q00_range[lo:hi + 1], f_values[lo:hi + 1])
+    roots = spline.derivative().roots(extrapolate=False)
+    roots = roots[spline.derivative(2)(roots) > 0]
+    if roots.size == 0:
+        raise NoLocalMinimum(MSG_NO_LOCAL_MINIMUM)
+    return np.abs(min(roots, key=lambda x: abs(x - q_min))), spline
+
+
+def find_q0star_batch(adapter, params, structure, cell, ansatz, relax, qscan, targets, min_points=None,
+                      record=None):
+    """`Find_q0Star` (q0star.py:409-478) for every (temp, meanDensity) of `targets`: pass
+    k of all targets still searching is one `get_f_abc_batch` over all their q00 points
+    (passes x q00_Steps evaluations per target). Returns Q0StarResults in the order of
+    `targets`; a target whose pass raised InsufficientPoints or NoLocalMinimum carries that
+    status and message. `record`, if given, receives the reference's per-evaluation dict
+    plus the target's index ('target')."""
+    min_points = qscan.minPoints if min_points is None else min_points
+    targets = [(float(t), float(m)) for t, m in targets]
+    best = [qscan.q00_start] * len(targets)
+    dq = [qscan.Deltaq] * len(targets)
+    spline = [None] * len(targets)
+    status = [None] * len(targets)
+    message = [''] * len(targets)
+    for pass_idx in range(qscan.passes):
+        alive = [j for j in range(len(targets)) if status[j] is None]
+        if not alive:
+            break
+        ranges = {j: _q_range(best[j], dq[j], qscan.q00_Steps) for j in alive}
+        points = [(*targets[j], float(q)) for j in alive for q in ranges[j]]
+        results = get_f_abc_batch(adapter, params, structure, cell, ansatz, relax, points)
+        for k, j in enumerate(alive):
+            rs = results[k * qscan.q00_Steps:(k + 1) * qscan.q00_Steps]
+            f_values = np.array([r.f for r in rs])
+            fit_values = np.array([np.nan if r.stop in FAILED_STOPS else r.fitness for r in rs])
+            A_values = np.array([r.amplitudes[0] for r in rs])
+            if record is not None:
+                for q, r in zip(ranges[j], rs):
+                    record({'target': j, 'pass': pass_idx, 'q00': float(q), 'f': r.f, 'fitness': r.fitness,
+                            'amplitudes': r.amplitudes, 'stop': r.stop, 'steps': r.steps, 'dt_max': r.dt_max})
+            try:
+                best[j], spline[j] = _refine(ranges[j], f_values, fit_values, A_values, relax, min_points)
+            except InsufficientPoints as e:
+                status[j], message[j] = STATUS_INSUFFICIENT_POINTS, str(e)
+            except NoLocalMinimum as e:
+                status[j], message[j] = STATUS_NO_LOCAL_MINIMUM, str(e)
+            else:
+                dq[j] *= qscan.Deltaq_Refinement
+    out = []
+    for j, (t, m) in enumerate(targets):
+        if status[j] is None:
+            out.append(Q0StarResult(t, m, float(best[j]), float(spline[j](best[j])), STATUS_OK, ''))
+        else:
+            out.append(Q0StarResult(t, m, float('nan'), float('nan'), status[j], message[j]))
+    return out
+
+
+def find_q0star(adapter, params, structure, cell, ansatz, relax, qscan, temp, meanDensity, min_points=None,
+                record=None):
+    """`Find_q0Star` for one (temp, meanDensity): returns (q0*, fmin) or raises
+    InsufficientPoints / NoLocalMinimum with the reference's messages."""
+    r = find_q0star_batch(adapter, params, structure, cell, ansatz, relax, qscan, [(temp, meanDensity)],
+                          min_points=min_points, record=record)[0]
+    if r.status == STATUS_INSUFFICIENT_POINTS:
+        raise InsufficientPoints(r.message)
+    if r.status == STATUS_NO_LOCAL_MINIMUM:
+        raise NoLocalMinimum(r.message)
+    return r.q0star, r.fmin

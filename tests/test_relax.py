@@ -256,3 +256,57 @@ def test_std_adapter_relaxes_a_triangle():
     assert r.fitness > 0.99 and r.amplitudes[0] > 0.05
     b = pd.get_f_abc_batch(ad, params, 'triangle', cell, ansatz, relax, [(-0.25, -0.25, 1.0), (-0.25, -0.25, 0.97)])
     assert (b[0].values(), b[0].steps) == (r.values(), r.steps)
+
+
+# ---------------------------------------------------------------- q0* search
+QSCAN = pd.QScanSettings(passes=3, Deltaq=0.02, q00_Steps=21, Deltaq_Refinement=0.05)
+
+
+def test_toy_find_q0star_finds_the_known_minimum():
+    recs = []
+    q, fmin = pd.find_q0star(ToyAdapter(), {}, 'blob', {}, {}, TOY, QSCAN, 0.1, 0.5, record=recs.append)
+    assert q == pytest.approx(ToyAdapter.QSTAR, abs=1e-9)
+    assert fmin == pytest.approx(0.1 + 0.25, abs=1e-10)
+    assert len(recs) == QSCAN.passes * QSCAN.q00_Steps
+    assert [r['pass'] for r in recs[::QSCAN.q00_Steps]] == list(range(QSCAN.passes))
+    # the pass-0 edges (|q00 - 1.03| > 0.1) fail the fitness test and stop after one block
+    assert all(r['stop'] == (pd.STOP_POOR_FIT if r['fitness'] < 0.99 else pd.STOP_CONVERGED) for r in recs)
+
+
+def test_toy_find_q0star_batch_statuses_and_equality():
+    """Several targets in one search equal the one-target searches; a target whose f has
+    no minimum in the window and one with too few accepted points get their statuses."""
+    class Sloped(ToyAdapter):
+        def build(self, params, structure, cell, ansatz, temp, meanDensity, q00, dt, state=None, nThreads=1):
+            sim = super().build(params, structure, cell, ansatz, temp, meanDensity, q00, dt, state, nThreads)
+            if meanDensity == 0.3:          # f linear in q00: no minimum
+                sim.floor, sim.fitness = temp + q00, 1.0
+            if meanDensity == 0.2:          # poor fit everywhere
+                sim.fitness = 0.5
+            return sim
+    targets = [(0.1, 0.5), (0.1, 0.3), (0.2, 0.5), (0.1, 0.2)]
+    got = pd.find_q0star_batch(Sloped(), {}, 'blob', {}, {}, TOY, QSCAN, targets)
+    assert [g.status for g in got] == [pd.STATUS_OK, pd.STATUS_NO_LOCAL_MINIMUM, pd.STATUS_OK,
+                                       pd.STATUS_INSUFFICIENT_POINTS]
+    assert got[1].message == pd.MSG_NO_LOCAL_MINIMUM and got[3].message == pd.MSG_INSUFFICIENT_POINTS
+    assert math.isnan(got[1].q0star) and math.isnan(got[3].fmin)
+    for g, (t, m) in zip(got, targets):
+        if g.status == pd.STATUS_OK:
+            assert (g.q0star, g.fmin) == pd.find_q0star(Sloped(), {}, 'blob', {}, {}, TOY, QSCAN, t, m)
+    with pytest.raises(pd.NoLocalMinimum, match='No local minimum'):
+        pd.find_q0star(Sloped(), {}, 'blob', {}, {}, TOY, QSCAN, 0.1, 0.3)
+
+
+@pytest.mark.gpu
+def test_log_find_q0star_matches_the_reference_pins():
+    """tests/test_phase_diagram_q0star.py:53-56, 529-551: q0* within 1e-8 and fmin within
+    1e-13 at (eps -0.9, phi 0.63); (-0.9, 0.51) and (-0.9, 0.52) have no local minimum.
+    All three searches run as one batched search."""
+    got = pd.find_q0star_batch(pd.LogAdapter(), LOG_PARAMS, 'triangle', CELL, ANSATZ, RELAX, QSCAN,
+                               [(-0.9, 0.63), (-0.9, 0.51), (-0.9, 0.52)])
+    assert got[0].status == pd.STATUS_OK
+    assert got[0].q0star == pytest.approx(0.9638831589507376, abs=1e-8)
+    assert got[0].fmin == pytest.approx(-0.5535949848941145, abs=1e-13)
+    for g in got[1:]:
+        assert (g.status, g.message) == (pd.STATUS_NO_LOCAL_MINIMUM, pd.MSG_NO_LOCAL_MINIMUM)
+        assert math.isnan(g.q0star) and math.isnan(g.fmin)
