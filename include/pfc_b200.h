@@ -144,6 +144,8 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
 #define PFC_FLAG_PDL 4            /* launch the power-of-two step kernels with programmatic
                                      dependent launch: each may start (and send its column's
                                      state towards L2) while the kernel before it drains */
+#define PFC_FLAG_NO_ONE_CTA 8     /* step small FP64 mixed-radix grids with the two-kernel
+                                     step instead of the one-CTA whole-grid kernel */
 /* Variant of the power-of-two step kernels (0 in a field = the precision's default):
  * complex values per thread of the row and of the column kernel (FP32: 8, 16 or 32,
  * default 32; FP64: 8 or 16, default 16) and rows per CTA of the row kernel
@@ -163,6 +165,16 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
 /* The variant a plan uses: out4 = {row values per thread, column values per thread,
  * row tile rows, 1 if the power-of-two step kernels are used} (zeros when not). */
 int pfc_plan_variant(pfc_plan* plan, int32_t* out4);
+
+/* The step path of a plan: PFC_PATH_MIXED_RADIX (row and column kernels of any radix
+ * set), PFC_PATH_POW2 (the power-of-two step kernels) or PFC_PATH_ONE_CTA (FP64 grids
+ * whose spectra and transforms fit one CTA: every step of a pfc_step / pfc_batch_step
+ * call runs in one launch per 2048 steps, one CTA per plan, the grid in shared memory;
+ * the results equal the two-kernel step's). */
+#define PFC_PATH_MIXED_RADIX 0
+#define PFC_PATH_POW2 1
+#define PFC_PATH_ONE_CTA 2
+int pfc_plan_path(pfc_plan* plan, int32_t* path);
 
 /* Kernel launches issued by this plan since creation (for accounting). */
 int64_t pfc_launch_count(pfc_plan* plan);

@@ -21,6 +21,8 @@ FIELD_N, FIELD_MU, FIELD_LOCAL_MU, FIELD_LOCAL_N, FIELD_NONLIN_MU = range(5)
 FIELD_OF_CURRENT = 0x100
 SPEC_N_HAT, SPEC_N_HAT_NOW = 0, 1
 FLAG_GENERIC_ONLY, FLAG_NO_GRAPHS, FLAG_PDL = 1, 2, 4
+FLAG_NO_ONE_CTA = 8
+PATH_MIXED_RADIX, PATH_POW2, PATH_ONE_CTA = 0, 1, 2
 
 
 def flag_variant(ee_row=0, ee_col=0, row_tile=0, col_cta=0, pdl=0):
@@ -48,6 +50,7 @@ SIGNATURES = {
     "pfc_plan_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64)]),
     "pfc_launch_count": (_i64, [_vp]),
     "pfc_plan_variant": (ctypes.c_int, [_vp, ctypes.POINTER(_i32)]),
+    "pfc_plan_path": (ctypes.c_int, [_vp, ctypes.POINTER(_i32)]),
     "pfc_field_mean_noalloc": (ctypes.c_int, [_vp, _i64, _vp, _vp]),
     "pfc_batch_create": (ctypes.c_int, [ctypes.POINTER(_vp), _i32, ctypes.POINTER(_vp)]),
     "pfc_batch_step": (ctypes.c_int, [_vp, _i64, _vp]),

@@ -175,6 +175,12 @@ struct pfc_plan {
   // CUDA graphs of kGraphBlock steps and of one step, one per starting ping-pong parity
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t graph1[2] = {nullptr, nullptr};
+  // small FP64 mixed-radix grids: whole steps in one CTA (pfc_onecta.cu), reading this
+  // plan's buffers from a one-entry table per parity of cur
+  bool onecta = false;
+  int oc_threads = 0, oc_rset = kRadixPow2;
+  size_t oc_smem = 0;
+  pfc::BatchBufs* oc_table[2] = {nullptr, nullptr};
 };
 
 // A batch of plans stepped in lockstep: plans with the same step kernels, sizes and
@@ -535,6 +541,68 @@ int capture_graph(F&& fn, cudaGraphExec_t* out) {
   return rc;
 }
 
+// ---- one-CTA steps (small FP64 mixed-radix grids)
+// Steps per launch of the one-CTA kernel (a launch of 2048 steps of a 28 x 24 grid runs
+// a few milliseconds).
+constexpr long long kOneCtaChunk = 2048;
+
+// The radix set that holds every radix of both transforms.
+int onecta_rset(int a, int b) {
+  if (a == kRadixAll || b == kRadixAll) return kRadixAll;
+  if (a == kRadixSmall || b == kRadixSmall) return kRadixSmall;
+  return (a == kRadixPow2 && b == kRadixPow2) ? kRadixPow2 : -1;
+}
+
+// Chooses the one-CTA path for FP64 mixed-radix plans whose grid fits one CTA: both
+// transforms' threads within kOneCtaMaxThreads and the buffers within 48 KB of shared
+// memory. PFC_FLAG_NO_ONE_CTA keeps the two-kernel step.
+int setup_onecta(pfc_plan* h) {
+  h->onecta = false;
+  if (h->fp32 || h->fast || (h->prob.flags & PFC_FLAG_NO_ONE_CTA)) return PFC_OK;
+  const int rset = onecta_rset(h->row_rset, h->col_rset);
+  if (rset < 0 || !onecta_supported(rset)) return PFC_OK;
+  const int need = std::max(h->ny * h->row_tpf, h->m * h->col_tpf);
+  const int threads = (need + 31) / 32 * 32;
+  const size_t smem = onecta_smem_bytes(h->m, h->ny, h->row_ld, h->col_ld);
+  if (threads > kOneCtaMaxThreads || smem > 48 * 1024) return PFC_OK;
+  for (int p = 0; p < 2; ++p) {
+    BatchBufs b{};
+    b.w = h->W; b.v = h->V; b.nin = h->nhat[p]; b.nout = h->nhat[p ^ 1];
+    b.coef = h->coef; b.scal = h->scal;
+    cudaError_t e = cudaMalloc(&h->oc_table[p], sizeof(BatchBufs));
+    if (e == cudaSuccess) e = cudaMemcpy(h->oc_table[p], &b, sizeof(BatchBufs), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(PFC_E_CUDA, "pfc_plan_create: one-CTA table: %s", cudaGetErrorString(e));
+  }
+  h->onecta = true;
+  h->oc_threads = threads;
+  h->oc_rset = rset;
+  h->oc_smem = smem;
+  return PFC_OK;
+}
+
+// `nsteps` steps of `count` plans of one class (table: their buffers at the current parity).
+int launch_onecta(pfc_plan* h, cudaStream_t s, const BatchBufs* table, int count, long long nsteps) {
+  RowArgs<double> ra = row_args<double>(h);
+  ColArgs<double> ca = col_args<double>(h);
+  cudaError_t e = launch_onecta_step(ra, ca, table, count, nsteps, h->prob.model, h->oc_rset, h->oc_threads,
+                                     h->oc_smem, s);
+  ++h->launches;
+  if (e != cudaSuccess) return fail(PFC_E_CUDA, "one-CTA step launch failed: %s", cudaGetErrorString(e));
+  return PFC_OK;
+}
+
+int onecta_steps(pfc_plan* h, long long nsteps, cudaStream_t s) {
+  for (long long done = 0; done < nsteps;) {
+    const long long k = std::min(nsteps - done, kOneCtaChunk);
+    int rc = launch_onecta(h, s, h->oc_table[h->cur], 1, k);
+    if (rc) return rc;
+    if (k & 1) h->cur ^= 1;
+    h->steps_since_set += k;
+    done += k;
+  }
+  return PFC_OK;
+}
+
 template <class T>
 int step_direct(pfc_plan* h, long long nsteps, cudaStream_t s) {
   for (long long i = 0; i < nsteps; ++i) {
@@ -576,6 +644,7 @@ int replay_steps(pfc_plan* h, cudaGraphExec_t* slot, int len, long long count, c
 // once per starting parity (smaller gaps between the kernels than direct launches).
 template <class T>
 int do_step(pfc_plan* h, long long nsteps, cudaStream_t s) {
+  if (h->onecta) return onecta_steps(h, nsteps, s);
   if (h->prob.flags & PFC_FLAG_NO_GRAPHS) return step_direct<T>(h, nsteps, s);
   const long long blocks = nsteps / kGraphBlock;
   if (blocks > 0) {
@@ -603,7 +672,15 @@ int batch_step_direct(pfc_batch* b, int parity, long long nsteps, cudaStream_t s
     pfc_plan* h = c.plans[0];
     const int n = (int)c.plans.size();
     int p = parity;
-    for (long long i = 0; i < nsteps; ++i) {
+    for (long long done = 0; h->onecta && done < nsteps;) {
+      const long long k = std::min(nsteps - done, kOneCtaChunk);
+      int rc = launch_onecta(h, cs, c.table[p], n, k);
+      if (rc) return rc;
+      b->launches += 1;
+      if (k & 1) p ^= 1;
+      done += k;
+    }
+    for (long long i = 0; !h->onecta && i < nsteps; ++i) {
       int rc = launch_step_row<T>(h, cs, c.table[p], n);
       if (rc) return rc;
       rc = launch_step_col<T>(h, cs, c.table[p], n);
@@ -627,7 +704,9 @@ int do_batch_step(pfc_batch* b, long long nsteps, cudaStream_t s) {
       if (h->cur != parity)
         return fail(PFC_E_STATE, "pfc_batch_step: plans must have taken the same number of steps mod 2");
     }
-  const long long blocks = nsteps / kGraphBlock;
+  bool all_onecta = true;
+  for (auto& c : b->classes) all_onecta = all_onecta && c.plans[0]->onecta;
+  const long long blocks = all_onecta ? 0 : nsteps / kGraphBlock;
   if (blocks > 0) {
     if (!b->graph[parity]) {
       const long long launches = b->launches;
@@ -640,7 +719,9 @@ int do_batch_step(pfc_batch* b, long long nsteps, cudaStream_t s) {
       cudaError_t e = cudaGraphLaunch(b->graph[parity], s);
       if (e != cudaSuccess) return fail(PFC_E_CUDA, "cudaGraphLaunch failed: %s", cudaGetErrorString(e));
     }
-    b->launches += 2LL * (long long)b->classes.size() * kGraphBlock * blocks;
+    long long per_block = 0;
+    for (auto& c : b->classes) per_block += c.plans[0]->onecta ? 1 : 2LL * kGraphBlock;
+    b->launches += per_block * blocks;
   }
   const long long rest = nsteps - blocks * kGraphBlock;
   int rc = batch_step_direct<T>(b, parity, rest, s);   // kGraphBlock is even: parity unchanged
@@ -1011,6 +1092,8 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   }
   int rc = h->fp32 ? set_smem_attrs<float>(h) : set_smem_attrs<double>(h);
   if (rc) return cleanup_fail(rc);
+  rc = setup_onecta(h);
+  if (rc) return cleanup_fail(rc);
   *out = h;
   return PFC_OK;
 }
@@ -1026,6 +1109,8 @@ int pfc_plan_destroy(pfc_plan* h) {
   if (h->partials) cudaFree(h->partials);
   if (h->scal) cudaFree(h->scal);
   if (h->status) cudaFree(h->status);
+  for (auto* t : h->oc_table)
+    if (t) cudaFree(t);
   delete h;
   return PFC_OK;
 }
@@ -1127,6 +1212,12 @@ int pfc_plan_variant(pfc_plan* h, int32_t* o) {
   return PFC_OK;
 }
 
+int pfc_plan_path(pfc_plan* h, int32_t* path) {
+  if (!h || !path) return fail(PFC_E_ARG, "pfc_plan_path: null argument");
+  *path = h->onecta ? PFC_PATH_ONE_CTA : h->fast ? PFC_PATH_POW2 : PFC_PATH_MIXED_RADIX;
+  return PFC_OK;
+}
+
 int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out) {
   if (!plans || count <= 0 || !out) return fail(PFC_E_ARG, "pfc_batch_create: need plans and an output");
   *out = nullptr;
@@ -1148,7 +1239,8 @@ int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out) {
       const pfc_plan* r = c.plans[0];
       // (mixed-radix plans of one size and precision share the FFT description, twiddle
       // tables and launch shape, all of which come from plans[0] of the class)
-      if (r->fast == h->fast && r->fast_row_fn == h->fast_row_fn && r->fast_col_fn == h->fast_col_fn &&
+      if (r->fast == h->fast && r->onecta == h->onecta && r->fast_row_fn == h->fast_row_fn &&
+          r->fast_col_fn == h->fast_col_fn &&
           r->row_rset == h->row_rset && r->col_rset == h->col_rset && r->prob.model == h->prob.model &&
           r->nx == h->nx && r->ny == h->ny && r->prob.g == h->prob.g && r->prob.clamp_log == h->prob.clamp_log &&
           r->prob.min_phi == h->prob.min_phi) {

@@ -69,6 +69,19 @@ cudaError_t launch_defect_screen(const double* field, const double* spec, int nx
                                  double* partials, double* out4, cudaStream_t stream);
 int diagnose_partials_needed();
 
+// Whole-grid step kernel for small FP64 mixed-radix grids (pfc_onecta.cu): one CTA per
+// plan runs nsteps steps with the grid in shared memory; `table` holds the plans'
+// buffers (BatchBufs) at the starting parity, `count` entries.
+template <class T> struct RowArgs;
+template <class T> struct ColArgs;
+struct BatchBufs;
+constexpr int kOneCtaMaxThreads = 256;
+size_t onecta_smem_bytes(int m, int ny, int row_ld, int col_ld);
+bool onecta_supported(int rset);
+cudaError_t launch_onecta_step(const RowArgs<double>& ra, const ColArgs<double>& ca, const BatchBufs* table,
+                               int count, long long nsteps, int model, int rset, int threads, size_t smem,
+                               cudaStream_t stream);
+
 // Vacancy location on a local density field (pfc_track.cu), count > 0.
 cudaError_t launch_locate_vacancies(const double* field, int nx, int ny, double dx, double dy, double* xy,
                                     int count, int32_t* status, cudaStream_t stream);

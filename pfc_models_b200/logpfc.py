@@ -41,9 +41,9 @@ def GetLinearKernel_phi(modelParameters, DerivativeKernels):
 
 class Simulation(_Simulation):
     def __init__(self, modelParameters, geometry, precision="fp64", clamp_log=False, device=None, kernels="auto",
-                 graphs=True, pdl=None):
+                 graphs=True, pdl=None, one_cta=True):
         super().__init__("log", modelParameters, geometry, precision=precision, clamp_log=clamp_log, device=device,
-                         kernels=kernels, graphs=graphs, pdl=pdl)
+                         kernels=kernels, graphs=graphs, pdl=pdl, one_cta=one_cta)
 
     def Get_local_phi(self):
         """Gaussian-coarsened phi (models/logpfc/simulation.py:232-242)."""
@@ -51,9 +51,9 @@ class Simulation(_Simulation):
 
 
 def BuildB200_Simulation(modelParameters, geometry, precision="fp64", clamp_log=False, device=None, kernels="auto",
-                         graphs=True, pdl=None):
+                         graphs=True, pdl=None, one_cta=True):
     return Simulation(modelParameters, geometry, precision=precision, clamp_log=clamp_log, device=device,
-                      kernels=kernels, graphs=graphs, pdl=pdl)
+                      kernels=kernels, graphs=graphs, pdl=pdl, one_cta=one_cta)
 
 
 def BuildCupyGPU_Simulation(modelParameters, geometry, *_, precision="fp64", **__):

@@ -142,6 +142,12 @@ class Plan:
     def launches(self):
         return int(self.lib.pfc_launch_count(self.handle))
 
+    def path(self):
+        """'mixed_radix', 'pow2' or 'one_cta': the step kernels this plan uses."""
+        v = ctypes.c_int32(0)
+        _lib.check(self.lib.pfc_plan_path(self.handle, ctypes.byref(v)))
+        return {_lib.PATH_MIXED_RADIX: "mixed_radix", _lib.PATH_POW2: "pow2", _lib.PATH_ONE_CTA: "one_cta"}[v.value]
+
     def variant(self):
         """{"ee_row", "ee_col", "row_tile", "fast"} of the step kernels this plan uses."""
         o = (ctypes.c_int32 * 4)()
@@ -376,7 +382,7 @@ class Simulation:
     """The reference's Simulation (models/stdpfc/simulation.py:166-268) backed by a plan."""
 
     def __init__(self, model: str, modelParameters, geometry, precision="fp64", clamp_log=False, device=None,
-                 kernels="auto", graphs=True, pdl=None):
+                 kernels="auto", graphs=True, pdl=None, one_cta=True):
         if model not in ("std", "log"):
             raise ValueError(f"model must be 'std' or 'log', got {model!r}")
         if precision not in _PRECISIONS:
@@ -399,6 +405,8 @@ class Simulation:
         prob.flags = _kernel_flags(kernels, prob) | (0 if graphs else _lib.FLAG_NO_GRAPHS)
         if pdl is not None:   # None: as the variant says
             prob.flags = (prob.flags & ~_lib.FLAG_PDL) | (_lib.FLAG_PDL if pdl else 0)
+        if not one_cta:       # small FP64 mixed-radix grids: keep the two-kernel step
+            prob.flags |= _lib.FLAG_NO_ONE_CTA
         self._plan = Plan(prob, device)
         self._version = 0
         self._mu_current = False

@@ -45,9 +45,9 @@ def GetLinearKernel_n(modelParameters, DerivativeKernels):
 
 class Simulation(_Simulation):
     def __init__(self, modelParameters, geometry, precision="fp64", device=None, kernels="auto", graphs=True,
-                 pdl=None):
+                 pdl=None, one_cta=True):
         super().__init__("std", modelParameters, geometry, precision=precision, device=device, kernels=kernels,
-                         graphs=graphs, pdl=pdl)
+                         graphs=graphs, pdl=pdl, one_cta=one_cta)
 
     def Get_local_n(self):
         """Gaussian-coarsened n of the state at the start of the last step, on the host
@@ -56,14 +56,14 @@ class Simulation(_Simulation):
 
 
 def BuildB200_Simulation(modelParameters, geometry, precision="fp64", device=None, kernels="auto", graphs=True,
-                         pdl=None):
+                         pdl=None, one_cta=True):
     """precision: "fp64" (plain) or "fp32" (mixed); kernels: "auto" (power-of-two step
     kernels where the grid allows) or "generic" (mixed-radix kernels everywhere);
     graphs: replay steps from recorded CUDA graphs (blocks of 16 and single steps);
     pdl: let each power-of-two step kernel start while the one before it drains (None:
     as the tuned variant says)."""
     return Simulation(modelParameters, geometry, precision=precision, device=device, kernels=kernels, graphs=graphs,
-                      pdl=pdl)
+                      pdl=pdl, one_cta=one_cta)
 
 
 def BuildCupyGPU_Simulation(modelParameters, geometry, *_, precision="fp64", **__):
