@@ -21,11 +21,71 @@ namespace pfc {
 
 namespace {
 
-// The transforms out of line: each call gets the register allocation it has in the
-// two-kernel step, instead of four inlined copies of every radix's butterflies.
+// One Stockham pass from src to dst with one butterfly per thread at a time: the loads,
+// twiddles, DFT and output positions of stockham_pass (pfc_fft.cuh), out of place, so a
+// thread holds R values instead of all its butterflies and the pass needs one barrier.
+template <int R, bool INV>
+__device__ __forceinline__ void pass_oop(PadBuf<double> src, PadBuf<double> dst, int n, int ns,
+                                         const cplx<double>* __restrict__ tw, const cplx<double>* __restrict__ roots,
+                                         int lt, int tpf) {
+  const int nr = n / R;
+  for (int j = lt; j < nr; j += tpf) {
+    cplx<double> v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = src[j + q * nr];
+    const int k = j % ns;
+    if (k != 0) {
+      const cplx<double>* w = tw + k;   // table [q - 1][k]
+#pragma unroll
+      for (int q = 1; q < R; ++q) {
+        cplx<double> t = w[(q - 1) * ns];
+        if (INV) t.y = -t.y;
+        v[q] = cmul(v[q], t);
+      }
+    }
+    dft<R, INV>(v, roots);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int q = 0; q < R; ++q) dst[base + q * ns] = v[q];
+  }
+  __syncthreads();
+}
+
+// Every pass of d, alternating between buffers a and b (every thread of the CTA calls
+// this); the result is in b when the pass count is odd, else in a.
 template <bool INV, int RSET>
-__device__ __noinline__ void fft_call(cplx<double>* p, const FftDesc* d, const cplx<double>* tw, int lt, int tpf) {
-  fft_run<INV, RSET>(PadBuf<double>{p}, *d, tw, lt, tpf);
+__device__ __forceinline__ void fft_oop(PadBuf<double> a, PadBuf<double> b, const FftDesc& d,
+                                        const cplx<double>* __restrict__ twbase, int lt, int tpf) {
+  PadBuf<double> src = a, dst = b;
+  for (int p = 0; p < d.npass; ++p) {
+    const cplx<double>* tw = twbase + d.twoff[p];
+    const cplx<double>* roots = d.rootoff[p] >= 0 ? twbase + d.rootoff[p] : nullptr;
+    const int ns = d.ns[p];
+    switch (d.radix[p]) {
+      case 2: pass_oop<2, INV>(src, dst, d.n, ns, tw, roots, lt, tpf); break;
+      case 4: pass_oop<4, INV>(src, dst, d.n, ns, tw, roots, lt, tpf); break;
+      case 8: pass_oop<8, INV>(src, dst, d.n, ns, tw, roots, lt, tpf); break;
+      case 16: pass_oop<16, INV>(src, dst, d.n, ns, tw, roots, lt, tpf); break;
+      default:
+        if constexpr (RSET != kRadixPow2) {
+          switch (d.radix[p]) {
+            case 3: pass_oop<3, INV>(src, dst, d.n, ns, tw, roots, lt, tpf); break;
+            case 5: pass_oop<5, INV>(src, dst, d.n, ns, tw, roots, lt, tpf); break;
+            case 7: pass_oop<7, INV>(src, dst, d.n, ns, tw, roots, lt, tpf); break;
+            default:
+              if constexpr (RSET == kRadixAll) {
+                if (d.radix[p] == 11) pass_oop<11, INV>(src, dst, d.n, ns, tw, roots, lt, tpf);
+                else if (d.radix[p] == 13) pass_oop<13, INV>(src, dst, d.n, ns, tw, roots, lt, tpf);
+              }
+              break;
+          }
+        }
+        break;
+    }
+    const PadBuf<double> t = src;
+    src = dst;
+    dst = t;
+  }
 }
 
 template <int MODEL, int RSET>
@@ -36,8 +96,10 @@ __global__ void __launch_bounds__(kOneCtaMaxThreads) onecta_step_kernel(RowArgs<
   const int m = ra.m, ny = ra.ny, ldr = ra.ld, ldc = ca.ld, nyh = ca.nyh;
   const int spec = m * ny;
   cplx<T>* R = reinterpret_cast<cplx<T>*>(smem_raw);   // ny row buffers of ldr
-  cplx<T>* C = R + (size_t)ny * ldr;                      // m column buffers of ldc
-  cplx<T>* S = C + (size_t)m * ldc;                       // n_hat, packed [kx][y]
+  cplx<T>* R2 = R + (size_t)ny * ldr;                     // their pass partners
+  cplx<T>* C = R2 + (size_t)ny * ldr;                     // m column buffers of ldc
+  cplx<T>* C2 = C + (size_t)m * ldc;                      // their pass partners
+  cplx<T>* S = C2 + (size_t)m * ldc;                      // n_hat, packed [kx][y]
   const BatchBufs& bb = table[blockIdx.x];
   cplx<T>* W = static_cast<cplx<T>*>(const_cast<void*>(bb.w));
   cplx<T>* V = static_cast<cplx<T>*>(bb.v);
@@ -59,11 +121,16 @@ __global__ void __launch_bounds__(kOneCtaMaxThreads) onecta_step_kernel(RowArgs<
   constexpr int kIdle = 1 << 20;
   const int ltr = row_on ? tid - fr * tr : kIdle;
   const int ltc = col_on ? tid - fc * tc : kIdle;
-  const PadBuf<T> rbuf{R + (size_t)(row_on ? fr : 0) * ldr};
-  const PadBuf<T> cbuf{C + (size_t)(col_on ? fc : 0) * ldc};
+  const PadBuf<T> rbuf{R + (size_t)(row_on ? fr : 0) * ldr}, rbuf2{R2 + (size_t)(row_on ? fr : 0) * ldr};
+  const PadBuf<T> cbuf{C + (size_t)(col_on ? fc : 0) * ldc}, cbuf2{C2 + (size_t)(col_on ? fc : 0) * ldc};
   const int kx = col_on ? fc : 0;
   const T s = (T)ca.scale;
-  const FftDesc rfft = ra.fft, cfft = ca.fft;
+  const FftDesc& rfft = ra.fft;
+  const FftDesc& cfft = ca.fft;
+  // where a transform's result lands: the partner buffer after an odd pass count; an
+  // inverse and a forward transform together always end in the main buffer
+  const PadBuf<T> xr = (rfft.npass & 1) ? rbuf2 : rbuf, xr2 = (rfft.npass & 1) ? rbuf : rbuf2;
+  const PadBuf<T> xc = (cfft.npass & 1) ? cbuf2 : cbuf, xc2 = (cfft.npass & 1) ? cbuf : cbuf2;
   __syncthreads();
 
   for (long long step = 0; step < nsteps; ++step) {
@@ -88,14 +155,14 @@ __global__ void __launch_bounds__(kOneCtaMaxThreads) onecta_step_kernel(RowArgs<
       }
     }
     __syncthreads();
-    fft_call<true, RSET>(rbuf.p, &rfft, ra.tw, ltr, tr);
+    fft_oop<true, RSET>(rbuf, rbuf2, rfft, ra.tw, ltr, tr);
     for (int j = ltr; j < m; j += tr) {
-      const cplx<T> z = rbuf[j];
-      rbuf[j] = mk((T)nonlin_plain<MODEL>((double)z.x, ra.g, ra.clamp, ra.min_phi, ra.min_log),
+      const cplx<T> z = xr[j];
+      xr[j] = mk((T)nonlin_plain<MODEL>((double)z.x, ra.g, ra.clamp, ra.min_phi, ra.min_log),
                    (T)nonlin_plain<MODEL>((double)z.y, ra.g, ra.clamp, ra.min_phi, ra.min_log));
     }
     __syncthreads();
-    fft_call<false, RSET>(rbuf.p, &rfft, ra.tw, ltr, tr);
+    fft_oop<false, RSET>(xr, xr2, rfft, ra.tw, ltr, tr);
     for (int k = ltr; k <= m / 2; k += tr) {
       if (k == 0) {
         const cplx<T> z = rbuf[0];
@@ -121,11 +188,11 @@ __global__ void __launch_bounds__(kOneCtaMaxThreads) onecta_step_kernel(RowArgs<
     if (last)   // the state this step starts from, in its ping-pong buffer
       for (int i = tid; i < spec; i += nth) P[step & 1][i] = S[i];
     __syncthreads();
-    fft_call<false, RSET>(cbuf.p, &cfft, ca.tw, ltc, tc);
+    fft_oop<false, RSET>(cbuf, cbuf2, cfft, ca.tw, ltc, tc);
     if (col_on && kx == 0) {
       for (int ky = ltc; ky <= ny / 2; ky += tc) {
         const int kyp = ky == 0 ? 0 : ny - ky;
-        const cplx<T> qkt = cbuf[ky], qkpt = cbuf[kyp];
+        const cplx<T> qkt = xc[ky], qkpt = xc[kyp];
         const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
         const cplx<double> c0v = coef[ky];
         const cplx<double> cMv = coef[(size_t)m * nyh + ky];
@@ -139,10 +206,10 @@ __global__ void __launch_bounds__(kOneCtaMaxThreads) onecta_step_kernel(RowArgs<
         const cplx<double> ok = h0n + mul_i(hmn);
         const cplx<double> okp = conj(h0n) + mul_i(conj(hmn));
         S[ky] = ok;
-        cbuf[ky] = mk((T)ok.x, (T)ok.y);
+        xc[ky] = mk((T)ok.x, (T)ok.y);
         if (kyp != ky) {
           S[kyp] = okp;
-          cbuf[kyp] = mk((T)okp.x, (T)okp.y);
+          xc[kyp] = mk((T)okp.x, (T)okp.y);
         }
       }
     } else if (col_on) {
@@ -151,22 +218,22 @@ __global__ void __launch_bounds__(kOneCtaMaxThreads) onecta_step_kernel(RowArgs<
         const int kyp = ky == 0 ? 0 : ny - ky;
         const cplx<T> cw = coef[(size_t)kx * nyh + ky];
         const cplx<T> ph = S[cb + ky], pph = S[cb + kyp];
-        const cplx<T> qkt = cbuf[ky], qkpt = cbuf[kyp];
+        const cplx<T> qkt = xc[ky], qkpt = xc[kyp];
         const cplx<double> qk = mk((double)qkt.x, (double)qkt.y), qkp = mk((double)qkpt.x, (double)qkpt.y);
         const cplx<double> c = mk((double)cw.x, (double)cw.y);
         const cplx<double> pk = mk((double)ph.x, (double)ph.y), pkp = mk((double)pph.x, (double)pph.y);
         const cplx<double> ok = pk + c.x * pk + c.y * qk;
         const cplx<double> okp = pkp + c.x * pkp + c.y * qkp;
         S[cb + ky] = ok;
-        cbuf[ky] = mk((T)ok.x, (T)ok.y);
+        xc[ky] = mk((T)ok.x, (T)ok.y);
         if (kyp != ky) {
           S[cb + kyp] = okp;
-          cbuf[kyp] = mk((T)okp.x, (T)okp.y);
+          xc[kyp] = mk((T)okp.x, (T)okp.y);
         }
       }
     }
     __syncthreads();
-    fft_call<true, RSET>(cbuf.p, &cfft, ca.tw, ltc, tc);
+    fft_oop<true, RSET>(xc, xc2, cfft, ca.tw, ltc, tc);
     for (int ky = ltc; ky < ny; ky += tc) {
       const cplx<T> v = cbuf[ky];
       cbuf[ky] = mk(s * v.x, s * v.y);
@@ -195,7 +262,17 @@ void* pick(int rset) {
 }  // namespace
 
 size_t onecta_smem_bytes(int m, int ny, int row_ld, int col_ld) {
-  return ((size_t)ny * row_ld + (size_t)m * col_ld + (size_t)m * ny) * sizeof(cplx<double>);
+  return (2 * (size_t)ny * row_ld + 2 * (size_t)m * col_ld + (size_t)m * ny) * sizeof(cplx<double>);
+}
+
+cudaError_t onecta_allow_smem(size_t bytes) {
+  for (int model : {kModelStd, kModelLog})
+    for (int rset : {kRadixPow2, kRadixSmall, kRadixAll}) {
+      void* fn = model == kModelLog ? pick<kModelLog>(rset) : pick<kModelStd>(rset);
+      cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+      if (e != cudaSuccess) return e;
+    }
+  return cudaSuccess;
 }
 
 bool onecta_supported(int rset) { return rset == kRadixPow2 || rset == kRadixSmall || rset == kRadixAll; }

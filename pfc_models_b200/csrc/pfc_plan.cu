@@ -178,7 +178,7 @@ struct pfc_plan {
   // small FP64 mixed-radix grids: whole steps in one CTA (pfc_onecta.cu), reading this
   // plan's buffers from a one-entry table per parity of cur
   bool onecta = false;
-  int oc_threads = 0, oc_rset = kRadixPow2;
+  int oc_threads = 0, oc_rset = kRadixPow2, oc_tpf_r = 0, oc_tpf_c = 0;
   size_t oc_smem = 0;
   pfc::BatchBufs* oc_table[2] = {nullptr, nullptr};
 };
@@ -553,18 +553,32 @@ int onecta_rset(int a, int b) {
   return (a == kRadixPow2 && b == kRadixPow2) ? kRadixPow2 : -1;
 }
 
-// Chooses the one-CTA path for FP64 mixed-radix plans whose grid fits one CTA: both
-// transforms' threads within kOneCtaMaxThreads and the buffers within 48 KB of shared
-// memory. PFC_FLAG_NO_ONE_CTA keeps the two-kernel step.
+// Largest butterfly count of a pass of d: threads per transform for one butterfly each.
+int max_butterflies(const FftDesc& d) {
+  int r = 1;
+  for (int p = 0; p < d.npass; ++p) r = std::max(r, d.n / d.radix[p]);
+  return r;
+}
+
+// Chooses the one-CTA path for FP64 mixed-radix plans whose grid fits one CTA: every row
+// (and every column) transform at once within kOneCtaMaxThreads threads, up to one
+// butterfly per thread and pass, and the buffers within kOneCtaMaxSmem of shared memory.
+// PFC_FLAG_NO_ONE_CTA keeps the two-kernel step.
 int setup_onecta(pfc_plan* h) {
   h->onecta = false;
   if (h->fp32 || h->fast || (h->prob.flags & PFC_FLAG_NO_ONE_CTA)) return PFC_OK;
   const int rset = onecta_rset(h->row_rset, h->col_rset);
   if (rset < 0 || !onecta_supported(rset)) return PFC_OK;
-  const int need = std::max(h->ny * h->row_tpf, h->m * h->col_tpf);
+  const int tpf_r = std::min(max_butterflies(h->rowfft), std::max(1, kOneCtaMaxThreads / h->ny));
+  const int tpf_c = std::min(max_butterflies(h->colfft), std::max(1, kOneCtaMaxThreads / h->m));
+  const int need = std::max(h->ny * tpf_r, h->m * tpf_c);
   const int threads = (need + 31) / 32 * 32;
   const size_t smem = onecta_smem_bytes(h->m, h->ny, h->row_ld, h->col_ld);
-  if (threads > kOneCtaMaxThreads || smem > 48 * 1024) return PFC_OK;
+  if (threads > kOneCtaMaxThreads || smem > kOneCtaMaxSmem) return PFC_OK;
+  if (smem > 48 * 1024) {
+    cudaError_t e = onecta_allow_smem(kOneCtaMaxSmem);
+    if (e != cudaSuccess) return fail(PFC_E_CUDA, "pfc_plan_create: one-CTA shared memory: %s", cudaGetErrorString(e));
+  }
   for (int p = 0; p < 2; ++p) {
     BatchBufs b{};
     b.w = h->W; b.v = h->V; b.nin = h->nhat[p]; b.nout = h->nhat[p ^ 1];
@@ -575,6 +589,8 @@ int setup_onecta(pfc_plan* h) {
   }
   h->onecta = true;
   h->oc_threads = threads;
+  h->oc_tpf_r = tpf_r;
+  h->oc_tpf_c = tpf_c;
   h->oc_rset = rset;
   h->oc_smem = smem;
   return PFC_OK;
@@ -584,6 +600,8 @@ int setup_onecta(pfc_plan* h) {
 int launch_onecta(pfc_plan* h, cudaStream_t s, const BatchBufs* table, int count, long long nsteps) {
   RowArgs<double> ra = row_args<double>(h);
   ColArgs<double> ca = col_args<double>(h);
+  ra.tpf = h->oc_tpf_r;
+  ca.tpf = h->oc_tpf_c;
   cudaError_t e = launch_onecta_step(ra, ca, table, count, nsteps, h->prob.model, h->oc_rset, h->oc_threads,
                                      h->oc_smem, s);
   ++h->launches;

@@ -76,7 +76,9 @@ template <class T> struct RowArgs;
 template <class T> struct ColArgs;
 struct BatchBufs;
 constexpr int kOneCtaMaxThreads = 256;
+constexpr size_t kOneCtaMaxSmem = 96 * 1024;   // two CTAs per SM
 size_t onecta_smem_bytes(int m, int ny, int row_ld, int col_ld);
+cudaError_t onecta_allow_smem(size_t bytes);     // raises the kernels' dynamic shared memory limit
 bool onecta_supported(int rset);
 cudaError_t launch_onecta_step(const RowArgs<double>& ra, const ColArgs<double>& ca, const BatchBufs* table,
                                int count, long long nsteps, int model, int rset, int threads, size_t smem,
