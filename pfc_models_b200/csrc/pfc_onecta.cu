@@ -88,8 +88,10 @@ __device__ __forceinline__ void fft_oop(PadBuf<double> a, PadBuf<double> b, cons
   }
 }
 
-template <int MODEL, int RSET>
-__global__ void __launch_bounds__(kOneCtaMaxThreads) onecta_step_kernel(RowArgs<double> ra, ColArgs<double> ca,
+// MINB 1: all registers for one CTA per SM (single plans, small batches); MINB 2: two
+// CTAs per SM (batches with more plans than SMs; a few spilled values).
+template <int MODEL, int RSET, int MINB>
+__global__ void __launch_bounds__(kOneCtaMaxThreads, MINB) onecta_step_kernel(RowArgs<double> ra, ColArgs<double> ca,
                                                                          const BatchBufs* table, long long nsteps) {
   using T = double;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -249,14 +251,19 @@ __global__ void __launch_bounds__(kOneCtaMaxThreads) onecta_step_kernel(RowArgs<
   }
 }
 
-template <int MODEL>
-void* pick(int rset) {
+template <int MODEL, int MINB>
+void* pick_minb(int rset) {
   switch (rset) {
-    case kRadixPow2: return (void*)onecta_step_kernel<MODEL, kRadixPow2>;
-    case kRadixSmall: return (void*)onecta_step_kernel<MODEL, kRadixSmall>;
-    case kRadixAll: return (void*)onecta_step_kernel<MODEL, kRadixAll>;
+    case kRadixPow2: return (void*)onecta_step_kernel<MODEL, kRadixPow2, MINB>;
+    case kRadixSmall: return (void*)onecta_step_kernel<MODEL, kRadixSmall, MINB>;
+    case kRadixAll: return (void*)onecta_step_kernel<MODEL, kRadixAll, MINB>;
     default: return nullptr;
   }
+}
+
+template <int MODEL>
+void* pick(int rset, bool dense) {
+  return dense ? pick_minb<MODEL, 2>(rset) : pick_minb<MODEL, 1>(rset);
 }
 
 }  // namespace
@@ -267,20 +274,21 @@ size_t onecta_smem_bytes(int m, int ny, int row_ld, int col_ld) {
 
 cudaError_t onecta_allow_smem(size_t bytes) {
   for (int model : {kModelStd, kModelLog})
-    for (int rset : {kRadixPow2, kRadixSmall, kRadixAll}) {
-      void* fn = model == kModelLog ? pick<kModelLog>(rset) : pick<kModelStd>(rset);
-      cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-      if (e != cudaSuccess) return e;
-    }
+    for (int rset : {kRadixPow2, kRadixSmall, kRadixAll})
+      for (bool dense : {false, true}) {
+        void* fn = model == kModelLog ? pick<kModelLog>(rset, dense) : pick<kModelStd>(rset, dense);
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+      }
   return cudaSuccess;
 }
 
 bool onecta_supported(int rset) { return rset == kRadixPow2 || rset == kRadixSmall || rset == kRadixAll; }
 
 cudaError_t launch_onecta_step(const RowArgs<double>& ra, const ColArgs<double>& ca, const BatchBufs* table,
-                               int count, long long nsteps, int model, int rset, int threads, size_t smem,
-                               cudaStream_t stream) {
-  void* fn = model == kModelLog ? pick<kModelLog>(rset) : pick<kModelStd>(rset);
+                               int count, long long nsteps, int model, int rset, bool dense, int threads,
+                               size_t smem, cudaStream_t stream) {
+  void* fn = model == kModelLog ? pick<kModelLog>(rset, dense) : pick<kModelStd>(rset, dense);
   if (!fn) return cudaErrorInvalidValue;
   RowArgs<double> r = ra;
   ColArgs<double> c = ca;

@@ -178,7 +178,7 @@ struct pfc_plan {
   // small FP64 mixed-radix grids: whole steps in one CTA (pfc_onecta.cu), reading this
   // plan's buffers from a one-entry table per parity of cur
   bool onecta = false;
-  int oc_threads = 0, oc_rset = kRadixPow2, oc_tpf_r = 0, oc_tpf_c = 0;
+  int oc_threads = 0, oc_rset = kRadixPow2, oc_tpf_r = 0, oc_tpf_c = 0, oc_sms = 0;
   size_t oc_smem = 0;
   pfc::BatchBufs* oc_table[2] = {nullptr, nullptr};
 };
@@ -591,6 +591,7 @@ int setup_onecta(pfc_plan* h) {
   h->oc_threads = threads;
   h->oc_tpf_r = tpf_r;
   h->oc_tpf_c = tpf_c;
+  cudaDeviceGetAttribute(&h->oc_sms, cudaDevAttrMultiProcessorCount, h->device);
   h->oc_rset = rset;
   h->oc_smem = smem;
   return PFC_OK;
@@ -602,8 +603,10 @@ int launch_onecta(pfc_plan* h, cudaStream_t s, const BatchBufs* table, int count
   ColArgs<double> ca = col_args<double>(h);
   ra.tpf = h->oc_tpf_r;
   ca.tpf = h->oc_tpf_c;
-  cudaError_t e = launch_onecta_step(ra, ca, table, count, nsteps, h->prob.model, h->oc_rset, h->oc_threads,
-                                     h->oc_smem, s);
+  // more plans than SMs: the build that fits two CTAs per SM
+  const bool dense = count > h->oc_sms;
+  cudaError_t e = launch_onecta_step(ra, ca, table, count, nsteps, h->prob.model, h->oc_rset, dense,
+                                     h->oc_threads, h->oc_smem, s);
   ++h->launches;
   if (e != cudaSuccess) return fail(PFC_E_CUDA, "one-CTA step launch failed: %s", cudaGetErrorString(e));
   return PFC_OK;

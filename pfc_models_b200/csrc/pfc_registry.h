@@ -81,8 +81,8 @@ size_t onecta_smem_bytes(int m, int ny, int row_ld, int col_ld);
 cudaError_t onecta_allow_smem(size_t bytes);     // raises the kernels' dynamic shared memory limit
 bool onecta_supported(int rset);
 cudaError_t launch_onecta_step(const RowArgs<double>& ra, const ColArgs<double>& ca, const BatchBufs* table,
-                               int count, long long nsteps, int model, int rset, int threads, size_t smem,
-                               cudaStream_t stream);
+                               int count, long long nsteps, int model, int rset, bool dense, int threads,
+                               size_t smem, cudaStream_t stream);
 
 // Vacancy location on a local density field (pfc_track.cu), count > 0.
 cudaError_t launch_locate_vacancies(const double* field, int nx, int ny, double dx, double dy, double* xy,

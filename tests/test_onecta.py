@@ -91,3 +91,20 @@ def test_batch_of_one_cta_plans_equals_plans_alone():
         assert np.array_equal(s.plan.get_state().cpu().numpy(), t.plan.get_state().cpu().numpy()), i
         assert tuple(F[i]) == t.Reduce()
     b.close()
+
+
+@pytest.mark.gpu
+def test_batch_of_more_plans_than_sms_equals_plans_alone():
+    """160 cells: more plans than the B200's 148 SMs, so the batch runs the one-CTA build
+    that fits two CTAs per SM; it must still equal each plan stepped alone."""
+    from pfc_models_b200.simulation import Batch
+    n = 160
+    sims = [_sim("log", 28, 24, True, seed=i, eps=-0.9 + 0.001 * i) for i in range(n)]
+    alone = [_sim("log", 28, 24, True, seed=i, eps=-0.9 + 0.001 * i) for i in range(n)]
+    b = Batch(sims)
+    b.step(101)
+    for s in alone:
+        s.TimeSteps(101)
+    for i, (s, t) in enumerate(zip(sims, alone)):
+        assert np.array_equal(s.plan.get_state().cpu().numpy(), t.plan.get_state().cpu().numpy()), i
+    b.close()
