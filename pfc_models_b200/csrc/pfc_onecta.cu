@@ -52,9 +52,11 @@ __device__ __forceinline__ void pass_oop(PadBuf<double> src, PadBuf<double> dst,
 }
 
 // Every pass of d, alternating between buffers a and b (every thread of the CTA calls
-// this); the result is in b when the pass count is odd, else in a.
+// this); the result is in b when the pass count is odd, else in a. Out of line: the step
+// calls each direction twice, and one copy of the butterflies per direction keeps the
+// kernel's code small enough for the instruction cache.
 template <bool INV, int RSET>
-__device__ __forceinline__ void fft_oop(PadBuf<double> a, PadBuf<double> b, const FftDesc& d,
+__device__ __noinline__ void fft_oop(PadBuf<double> a, PadBuf<double> b, const FftDesc& d,
                                         const cplx<double>* __restrict__ twbase, int lt, int tpf) {
   PadBuf<double> src = a, dst = b;
   for (int p = 0; p < d.npass; ++p) {
