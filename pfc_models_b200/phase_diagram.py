@@ -518,7 +518,8 @@ class _Member:
         self.index, self.point, self.sim = index, point, sim
         self.f_last, self.A_last = f_last, A_last
         self.counter = [0]
-        self.snapshot = None
+        self.snapshot = None     # the state at the start of the block (device array)
+        self.t_last = 0.0        # the time at the start of the block
 
 
 def get_f_abc_batch(adapter, params, structure, cell, ansatz, relax, points, states=None, keep_state=False):

@@ -310,3 +310,40 @@ def test_log_find_q0star_matches_the_reference_pins():
     for g in got[1:]:
         assert (g.status, g.message) == (pd.STATUS_NO_LOCAL_MINIMUM, pd.MSG_NO_LOCAL_MINIMUM)
         assert math.isnan(g.q0star) and math.isnan(g.fmin)
+
+
+def test_batch_from_given_states_keeps_them_noise_free():
+    """The frozen-q use (phase_diagram/frozen_q.py: Get_f_ABC from a given field): no
+    noise is added to a given state, and keep_state returns the field at the stop."""
+    ad = ToyAdapter()
+    relax = pd.RelaxSettings(dt=0.1, totalT=20.0, stepT=10.0, divs=10, maxDepth=4, requiredFitness=None,
+                             minimumA=1e-6, noise=0.5)
+    x0 = np.full(4, 0.25)
+    got = pd.get_f_abc_batch(ad, {}, 'blob', {}, {}, relax, [(0.1, 0.5, 1.0), (0.1, 0.5, 1.03)],
+                             states=[x0, x0 * 2], keep_state=True)
+    decay = (1 - 0.5 * 0.1) ** 200
+    assert got[0].state == pytest.approx(x0 * decay, rel=1e-12)
+    assert got[1].state == pytest.approx(2 * x0 * decay, rel=1e-12)
+    one = pd.get_f_abc(ToyAdapter(), {}, 'blob', {}, {}, relax, 0.1, 0.5, 1.0, state=x0, keep_state=True)
+    assert np.array_equal(one.state, got[0].state) and one.values() == got[0].values()
+    assert pd.get_f_abc_batch(ad, {}, 'blob', {}, {}, relax, []) == []
+    with pytest.raises(ValueError, match='states'):
+        pd.get_f_abc_batch(ad, {}, 'blob', {}, {}, relax, [(0.1, 0.5, 1.0)], states=[x0, x0])
+
+
+def test_fresh_ansatz_noise_is_seeded_and_mean_preserving():
+    """q0star.py:236-244: relative noise from default_rng(seed) with the mean restored,
+    the same draws for every point."""
+    class Flat(ToyAdapter):
+        def build(self, *a, **k):
+            sim = super().build(*a, **k)
+            sim.x = np.linspace(0.2, 0.8, 4) if k.get('state') is None else sim.x
+            return sim
+    relax = pd.RelaxSettings(dt=0.1, totalT=10.0, stepT=10.0, divs=10, maxDepth=4, requiredFitness=None,
+                             minimumA=1e-6, noise=1e-3, seed=3)
+    run = pd._Run(Flat(), {}, 'blob', {}, {}, relax)
+    a, b = run.generate(0.1, 0.5, 1.0, 0.1), run.generate(0.1, 0.5, 1.1, 0.1)
+    base = np.linspace(0.2, 0.8, 4)
+    want = base * (1.0 + 1e-3 * np.random.default_rng(3).standard_normal(4))
+    want = want + (base.mean() - want.mean())
+    assert np.array_equal(a.x, want) and np.array_equal(b.x, want)
