@@ -25,6 +25,8 @@ out. A phase diagram is hundreds of such evaluations, each on a small cell grid.
 * `find_q0star_batch` is `Find_q0Star` (q0star.py:409-478: passes of q00 scans refined
   by a cubic spline of f(q00)) for many (temp, meanDensity) at once, each pass one
   `get_f_abc_batch` over every target's q00 points; `find_q0star` is the one-target form.
+* `scan_density_batch` is `scan_density` (q0star.py:566-635) over those searches, with
+  the reference's result arrays and checkpoint files (fmin.npz, qscan.npz).
 
 The ansatz is built on the host with the reference's NumPy operations
 (`_build3Mode`, stdpfc_cpu/phase_diagram.py:171-182 and logpfc_cpu/phase_diagram.py:
@@ -34,6 +36,8 @@ restored).
 """
 from __future__ import annotations
 
+import os
+import time
 from dataclasses import dataclass
 
 import numpy as np
@@ -719,3 +723,136 @@ def find_q0star(adapter, params, structure, cell, ansatz, relax, qscan, temp, me
     if r.status == STATUS_NO_LOCAL_MINIMUM:
         raise NoLocalMinimum(r.message)
     return r.q0star, r.fmin
+
+
+# ---------------------------------------------------------------- density scans
+FMIN_FILE = 'fmin.npz'
+QSCAN_FILE = 'qscan.npz'
+STATUS_ERROR = 'error'
+
+
+def _fmin_arrays(phi, q0star, fmin, status, message, wall_s):
+    """The per-density arrays of the reference's fmin.npz (q0star.py:500-509)."""
+    return {'phi': np.asarray(phi, dtype=float), 'q0star': np.asarray(q0star, dtype=float),
+            'fmin': np.asarray(fmin, dtype=float), 'status': np.asarray(status, dtype=str),
+            'message': np.asarray(message, dtype=str), 'wall_s': np.asarray(wall_s, dtype=float)}
+
+
+def _qscan_arrays(rows, seed, noise):
+    """The per-evaluation arrays of the reference's qscan.npz (q0star.py:512-532):
+    amplitudes padded with NaN to the widest row."""
+    k = max((len(r['amplitudes']) for r in rows), default=0)
+    amplitudes = np.full((len(rows), k), np.nan)
+    for j, r in enumerate(rows):
+        amplitudes[j, :len(r['amplitudes'])] = r['amplitudes']
+    return {'phi_index': np.asarray([r['phi_index'] for r in rows], dtype=np.int64),
+            'pass_index': np.asarray([r['pass_index'] for r in rows], dtype=np.int64),
+            'q00': np.asarray([r['q00'] for r in rows], dtype=float),
+            'f': np.asarray([r['f'] for r in rows], dtype=float),
+            'fitness': np.asarray([r['fitness'] for r in rows], dtype=float),
+            'amplitudes': amplitudes,
+            'stop': np.asarray([r['stop'] for r in rows], dtype=str),
+            'steps': np.asarray([r['steps'] for r in rows], dtype=np.int64),
+            'dt_max': np.asarray([r['dt_max'] for r in rows], dtype=float),
+            'seed': np.asarray(seed, dtype=np.int64), 'noise': np.asarray(noise, dtype=float)}
+
+
+def _save_npz_atomic(path, arrays):
+    tmp = path + '.tmp'
+    with open(tmp, 'wb') as fh:
+        np.savez(fh, **arrays)
+    os.replace(tmp, path)
+
+
+def _load_checkpoint(checkpoint, phi):
+    """(old fmin arrays, indices with a status, their q-scan rows), or None without a
+    checkpoint; a checkpoint of another density list is refused (q0star.py:535-563)."""
+    path = os.path.join(checkpoint, FMIN_FILE)
+    if not os.path.exists(path):
+        return None
+    with np.load(path, allow_pickle=False) as z:
+        old = {k: z[k] for k in z.files}
+    if old['phi'].shape != phi.shape or not np.array_equal(old['phi'], phi):
+        raise ValueError(f'{path} holds a different density list; refusing to resume into it')
+    done = {i for i, s in enumerate(old['status']) if str(s)}
+    rows = []
+    qpath = os.path.join(checkpoint, QSCAN_FILE)
+    if os.path.exists(qpath):
+        with np.load(qpath, allow_pickle=False) as z:
+            q = {k: z[k] for k in z.files}
+        for j in range(q['q00'].size):
+            i = int(q['phi_index'][j])
+            if i not in done:
+                continue
+            amps = q['amplitudes'][j]
+            rows.append({'phi_index': i, 'pass_index': int(q['pass_index'][j]), 'q00': float(q['q00'][j]),
+                         'f': float(q['f'][j]), 'fitness': float(q['fitness'][j]),
+                         'amplitudes': tuple(float(a) for a in amps[~np.isnan(amps)]), 'stop': str(q['stop'][j]),
+                         'steps': int(q['steps'][j]), 'dt_max': float(q['dt_max'][j])})
+    return old, done, rows
+
+
+def scan_density_batch(adapter, params, structure, cell, ansatz, relax, qscan, temp, densities, checkpoint=None,
+                       chunk=None):
+    """`scan_density` (q0star.py:566-635): q0* and fmin over a density list at one
+    temperature, with the reference's result arrays, status codes and checkpoint files
+    (fmin.npz and qscan.npz, rewritten atomically; a restart skips the densities that have
+    a status). The densities run as batched searches (`find_q0star_batch`) of `chunk`
+    densities (default: all), a checkpoint after each; `wall_s` is the chunk's wall time
+    shared evenly by its densities. A chunk that raises anything but the two search
+    failures is redone one density at a time, so the error costs that density only
+    (status 'error', message 'Type: text')."""
+    phi = np.asarray(list(densities), dtype=float)
+    n = phi.size
+    q0star, fmin = [np.nan] * n, [np.nan] * n
+    status, message, wall_s = [''] * n, [''] * n, [np.nan] * n
+    rows, done = [], set()
+    if checkpoint is not None:
+        prev = _load_checkpoint(checkpoint, phi)
+        if prev is not None:
+            old, done, rows = prev
+            for i in done:
+                q0star[i], fmin[i] = float(old['q0star'][i]), float(old['fmin'][i])
+                status[i], message[i] = str(old['status'][i]), str(old['message'][i])
+                wall_s[i] = float(old['wall_s'][i])
+    todo = [i for i in range(n) if i not in done]
+    size = len(todo) if not chunk else int(chunk)
+    prov = (relax.seed, relax.noise)
+
+    def search(indices):
+        recs = []
+        t0 = time.perf_counter()
+        res = find_q0star_batch(adapter, params, structure, cell, ansatz, relax, qscan,
+                                [(temp, phi[i]) for i in indices], record=recs.append)
+        return res, recs, time.perf_counter() - t0
+
+    for c0 in range(0, len(todo), max(size, 1)):
+        part = todo[c0:c0 + max(size, 1)]
+        try:
+            outs = [search(part)]
+            groups = [part]
+        except Exception:
+            outs, groups = [], []
+            for i in part:
+                try:
+                    outs.append(search([i]))
+                except Exception as e:
+                    status[i], message[i] = STATUS_ERROR, f'{type(e).__name__}: {e}'
+                    wall_s[i] = 0.0
+                    continue
+                groups.append([i])
+        for (res, recs, wall), idx in zip(outs, groups):
+            for r, i in zip(res, idx):
+                q0star[i], fmin[i], status[i], message[i] = r.q0star, r.fmin, r.status, r.message
+                wall_s[i] = wall / len(idx)
+            for r in recs:
+                rows.append({'phi_index': idx[r['target']], 'pass_index': r['pass'], 'q00': r['q00'], 'f': r['f'],
+                             'fitness': r['fitness'], 'amplitudes': r['amplitudes'], 'stop': r['stop'],
+                             'steps': r['steps'], 'dt_max': r['dt_max']})
+        if checkpoint is not None:
+            _save_npz_atomic(os.path.join(checkpoint, QSCAN_FILE), _qscan_arrays(rows, *prov))
+            _save_npz_atomic(os.path.join(checkpoint, FMIN_FILE),
+                             _fmin_arrays(phi, q0star, fmin, status, message, wall_s))
+    result = _fmin_arrays(phi, q0star, fmin, status, message, wall_s)
+    result['qscan'] = _qscan_arrays(rows, *prov)
+    return result

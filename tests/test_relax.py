@@ -347,3 +347,68 @@ def test_fresh_ansatz_noise_is_seeded_and_mean_preserving():
     want = base * (1.0 + 1e-3 * np.random.default_rng(3).standard_normal(4))
     want = want + (base.mean() - want.mean())
     assert np.array_equal(a.x, want) and np.array_equal(b.x, want)
+
+
+# ---------------------------------------------------------------- density scans
+class ScanToy(ToyAdapter):
+    """Regimes by mean density: 0.3 no minimum (f linear in q00), 0.2 poor fit
+    everywhere, negative densities fail to build, 0.45 fails in a step after t = 5,
+    `interrupt_at` raises KeyboardInterrupt in build."""
+    interrupt_at = None
+
+    def build(self, params, structure, cell, ansatz, temp, meanDensity, q00, dt, state=None, nThreads=1):
+        if meanDensity == self.interrupt_at:
+            raise KeyboardInterrupt
+        if meanDensity < 0:
+            raise ValueError('negative density')
+        sim = super().build(params, structure, cell, ansatz, temp, meanDensity, q00, dt, state, nThreads)
+        if meanDensity == 0.3:
+            sim.floor, sim.fitness = temp + q00, 1.0
+        if meanDensity == 0.2:
+            sim.fitness = 0.5
+        sim.boom = meanDensity == 0.45
+        return sim
+
+    def step(self, sim):
+        super().step(sim)
+        if sim.boom and sim.t >= self.T_BAD:
+            raise ValueError('toy step failed')
+
+
+def _scan(ad, densities, **kw):
+    return pd.scan_density_batch(ad, {}, 'blob', {}, {}, TOY, QSCAN, 0.1, densities, **kw)
+
+
+def test_scan_density_statuses_and_arrays():
+    r = _scan(ScanToy(), [0.5, 0.3, 0.2, -1.0, 0.45])
+    assert list(r['status']) == ['ok', 'no_local_minimum', 'insufficient_points', 'error', 'error']
+    assert list(r['message']) == ['', pd.MSG_NO_LOCAL_MINIMUM, pd.MSG_INSUFFICIENT_POINTS,
+                                  'ValueError: negative density', 'ValueError: toy step failed']
+    assert r['q0star'][0] == pytest.approx(ToyAdapter.QSTAR, abs=1e-9)
+    assert np.isnan(r['q0star'][1:]).all() and np.isnan(r['fmin'][1:]).all()
+    qs = r['qscan']
+    assert np.bincount(qs['phi_index'], minlength=5).tolist() == [63, 21, 21, 0, 0]
+    assert qs['amplitudes'].shape == (105, 2)
+    assert set(qs) == {'phi_index', 'pass_index', 'q00', 'f', 'fitness', 'amplitudes', 'stop', 'steps', 'dt_max',
+                       'seed', 'noise'}
+    assert (int(qs['seed']), float(qs['noise'])) == (0, 1e-10)
+    # the batched search equals the one-density searches
+    q, f = pd.find_q0star(ScanToy(), {}, 'blob', {}, {}, TOY, QSCAN, 0.1, 0.5)
+    assert (r['q0star'][0], r['fmin'][0]) == (q, f)
+
+
+def test_scan_density_checkpoint_and_resume(tmp_path):
+    densities = [0.5, 0.3, 0.55, 0.2]
+    fresh = _scan(ScanToy(), densities)
+    ad = ScanToy()
+    ad.interrupt_at = 0.55
+    with pytest.raises(KeyboardInterrupt):
+        _scan(ad, densities, checkpoint=str(tmp_path), chunk=1)
+    with np.load(tmp_path / pd.FMIN_FILE) as z:
+        assert list(z['status']) == ['ok', 'no_local_minimum', '', '']
+    resumed = _scan(ScanToy(), densities, checkpoint=str(tmp_path), chunk=2)
+    for k in ('q0star', 'fmin', 'status', 'message'):
+        assert np.array_equal(resumed[k], fresh[k]) or np.allclose(resumed[k], fresh[k], equal_nan=True), k
+    assert resumed['qscan']['q00'].size == fresh['qscan']['q00'].size
+    with pytest.raises(ValueError, match='different density list'):
+        _scan(ScanToy(), [0.5, 0.3], checkpoint=str(tmp_path))
