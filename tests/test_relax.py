@@ -412,3 +412,19 @@ def test_scan_density_checkpoint_and_resume(tmp_path):
     assert resumed['qscan']['q00'].size == fresh['qscan']['q00'].size
     with pytest.raises(ValueError, match='different density list'):
         _scan(ScanToy(), [0.5, 0.3], checkpoint=str(tmp_path))
+
+
+@pytest.mark.gpu
+def test_log_scan_density_with_checkpoint(tmp_path):
+    """The reference test's ok and no-local-minimum points through the batched density
+    scan on B200 plans, with checkpoint files: the ok point's q0* and fmin equal the
+    batched search's pins, and a rerun resumes everything from the files."""
+    got = pd.scan_density_batch(pd.LogAdapter(), LOG_PARAMS, 'triangle', CELL, ANSATZ, RELAX, QSCAN, -0.9,
+                                [0.63, 0.51], checkpoint=str(tmp_path))
+    assert list(got['status']) == [pd.STATUS_OK, pd.STATUS_NO_LOCAL_MINIMUM]
+    assert got['q0star'][0] == pytest.approx(0.9638831589507376, abs=1e-8)
+    assert got['fmin'][0] == pytest.approx(-0.5535949848941145, abs=1e-13)
+    again = pd.scan_density_batch(pd.LogAdapter(), LOG_PARAMS, 'triangle', CELL, ANSATZ, RELAX, QSCAN, -0.9,
+                                  [0.63, 0.51], checkpoint=str(tmp_path))
+    assert np.array_equal(again['q0star'][:1], got['q0star'][:1]) and list(again['status']) == list(got['status'])
+    assert np.array_equal(again['qscan']['f'], got['qscan']['f'])
