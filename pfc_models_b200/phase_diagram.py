@@ -38,7 +38,7 @@ from __future__ import annotations
 
 import os
 import time
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 
@@ -359,6 +359,16 @@ class LogAdapter(_Adapter):
             rebuilt = self._positive(rebuilt, mean)
             fitness = 1 - float(np.abs(np.power(field - rebuilt, 2).mean()))
         return _diag.Diagnostics(fitness, amps, {'maxima_per_cell': d.details['maxima_per_cell']})
+
+    def frozen_field(self, state, params, temp, cell):
+        """f(q) and q_opt of a field frozen on the grid (logpfc_cpu/phase_diagram.py:
+        465-505), moments on the device."""
+        return _diag.frozen_field(state, params, temp, cell)
+
+    def defect_diagnostics(self, state, cell):
+        """Peak spread, sub-q ratio, peak count and flag (logpfc_cpu/phase_diagram.py:
+        509-528), on the device."""
+        return _diag.defect_diagnostics(state, cell)
 
 
 # ---------------------------------------------------------------- one evaluation
@@ -856,3 +866,128 @@ def scan_density_batch(adapter, params, structure, cell, ansatz, relax, qscan, t
     result = _fmin_arrays(phi, q0star, fmin, status, message, wall_s)
     result['qscan'] = _qscan_arrays(rows, *prov)
     return result
+
+
+# ---------------------------------------------------------------- frozen-q search
+STATUS_NOT_CONVERGED = 'not_converged'
+FROZEN_SCHEDULE = (1e-6, 1e-8, 1e-10, 1e-12)
+
+
+@dataclass(frozen=True)
+class FrozenQSettings:
+    """Settings of the frozen-q search with the reference's names and defaults
+    (phase_diagram/frozen_q.py:52-61): fTol per stage (the last is the final one), qTol
+    on |q_opt - q| at the final stage, maxIter relax/jump iterations, and the edge pass
+    of the density scan."""
+    schedule: tuple = FROZEN_SCHEDULE
+    qTol: float = 1e-8
+    maxIter: int = 40
+    edge: bool = True
+    maxPast: int = 3
+
+
+def _stage_relax(relax, settings, stage):
+    """The relaxation settings of a stage (frozen_q.py:85-90): that stage's fTol, and ATol
+    loosened with it except at the final stage."""
+    f_tol = float(settings.schedule[stage])
+    a_tol = relax.ATol if stage == len(settings.schedule) - 1 else max(relax.ATol, 1e6 * f_tol)
+    return replace(relax, fTol=f_tol, ATol=a_tol)
+
+
+def solve_frozen_q_batch(adapter, params, structure, cell, ansatz, relax, settings, temp, densities,
+                         q_start=1.0, states=None):
+    """`MinimizeFrozenQ.solve` (frozen_q.py:92-148) for every density at once: each
+    iteration relaxes every unfinished density at its box scale q from its carried field
+    (the densities at one stage of the fTol schedule in one `get_f_abc_batch`), then moves q
+    to q_opt of the relaxed field frozen on the grid (`adapter.frozen_field`), tightening
+    fTol stage by stage, until |q_opt - q| < qTol at the final stage with a converged
+    stop. Returns one record per density with the reference's fields (status, q = q_opt
+    of the final field, q_relaxed, f, f_frozen, fitness, A1.., stop, steps, iters, wall_s,
+    q_start, message, and the adapter's defect diagnostics where it has them); statuses
+    'ok', 'not_converged', a rejected relaxation's stop, or 'error'."""
+    if not hasattr(adapter, 'frozen_field'):
+        raise ValueError(f'adapter {getattr(adapter, "SLUG", adapter)!r} has no frozen_field')
+    if len(settings.schedule) < 1:
+        raise ValueError('schedule needs at least one fTol')
+    params = adapter.validate_params(params)
+    cell = adapter.validate_cell(cell)
+    dens = [float(p) for p in densities]
+    n = len(dens)
+    last_stage = len(settings.schedule) - 1
+    t0 = time.perf_counter()
+    q = [float(q_start)] * n
+    carry = [None] * n if states is None else list(states)
+    stage, steps, last = [0] * n, [0] * n, [None] * n
+    phi = [None] * n
+    error = [None] * n
+    active = list(range(n))
+    for it in range(settings.maxIter):
+        if not active:
+            break
+        nxt = []
+        for stg in sorted({stage[i] for i in active}):
+            group = [i for i in active if stage[i] == stg]
+            rs = _stage_relax(relax, settings, stg)
+            try:
+                res = get_f_abc_batch(adapter, params, structure, cell, ansatz, rs,
+                                      [(temp, dens[i], q[i]) for i in group], states=[carry[i] for i in group],
+                                      keep_state=True)
+            except Exception:   # isolate the failing density, as independent solves would
+                res = []
+                for i in group:
+                    try:
+                        res.append(get_f_abc(adapter, params, structure, cell, ansatz, rs, temp, dens[i], q[i],
+                                             state=carry[i], keep_state=True))
+                    except Exception as e:  # noqa: BLE001
+                        error[i] = f'{type(e).__name__}: {e}'
+                        res.append(None)
+            for i, r in zip(group, res):
+                if r is None:
+                    continue
+                try:
+                    steps[i] += r.steps
+                    phi[i] = r.state
+                    ff = adapter.frozen_field(r.state, params, temp, cell)
+                    qn = float(ff.q_opt())
+                    last[i] = dict(q=q[i], q_opt=qn, f=float(r.f), f_frozen=float(ff.f(qn)),
+                                   fitness=float(r.fitness), amps=[float(a) for a in r.amplitudes], stop=r.stop,
+                                   it=it)
+                except Exception as e:  # noqa: BLE001
+                    error[i] = f'{type(e).__name__}: {e}'
+                    continue
+                if r.stop not in (STOP_CONVERGED, STOP_TOTALT):
+                    continue
+                dq = qn - q[i]
+                carry[i], q[i] = r.state, qn
+                if stage[i] < last_stage:
+                    stage[i] += 1
+                elif abs(dq) < settings.qTol and r.stop == STOP_CONVERGED:
+                    continue
+                nxt.append(i)
+        active = sorted(nxt)
+    wall = (time.perf_counter() - t0) / max(n, 1)
+    out = []
+    dd = getattr(adapter, 'defect_diagnostics', None)
+    for i in range(n):
+        rec = dict(method='frozen-q', q_start=float(q_start), message='')
+        if error[i] is not None:
+            rec.update(status=STATUS_ERROR, message=error[i], steps=steps[i], wall_s=wall)
+            out.append(rec)
+            continue
+        lt = last[i]
+        ok = lt['stop'] == STOP_CONVERGED and stage[i] == last_stage and abs(lt['q_opt'] - lt['q']) < settings.qTol
+        if ok:
+            status = STATUS_OK
+        elif lt['stop'] in (STOP_CONVERGED, STOP_TOTALT):
+            status = STATUS_NOT_CONVERGED
+        else:
+            status = lt['stop']
+        rec.update(status=status, q=lt['q_opt'], q_relaxed=lt['q'], f=lt['f'], f_frozen=lt['f_frozen'],
+                   fitness=lt['fitness'], stop=lt['stop'], steps=steps[i], iters=lt['it'] + 1)
+        for j, a in enumerate(lt['amps']):
+            rec[f'A{j + 1}'] = a
+        if dd is not None and phi[i] is not None:
+            rec.update(dd(phi[i], cell))
+        rec['wall_s'] = wall
+        out.append(rec)
+    return out

@@ -428,3 +428,76 @@ def test_log_scan_density_with_checkpoint(tmp_path):
                                   [0.63, 0.51], checkpoint=str(tmp_path))
     assert np.array_equal(again['q0star'][:1], got['q0star'][:1]) and list(again['status']) == list(got['status'])
     assert np.array_equal(again['qscan']['f'], got['qscan']['f'])
+
+
+# ---------------------------------------------------------------- frozen-q search
+class _Frozen:
+    def __init__(self, q):
+        self.q = q
+
+    def q_opt(self):
+        return ToyAdapter.QSTAR + 0.5 * (self.q - ToyAdapter.QSTAR)
+
+    def f(self, q):
+        return 0.35 + (q - ToyAdapter.QSTAR) ** 2
+
+
+class FrozenToy(ToyAdapter):
+    """The toy with the box scale carried in its state (last element), and a frozen
+    field whose q_opt halves the distance to QSTAR: the frozen-q iteration converges
+    geometrically."""
+
+    def build(self, params, structure, cell, ansatz, temp, meanDensity, q00, dt, state=None, nThreads=1):
+        sim = super().build(params, structure, cell, ansatz, temp, meanDensity, q00, dt,
+                            None if state is None else np.asarray(state)[:-1], nThreads)
+        sim.q = q00
+        return sim
+
+    def get_state(self, sim):
+        return np.append(sim.x, sim.q)
+
+    def set_state(self, sim, state):
+        sim.x[...] = np.asarray(state)[:-1]
+
+    def frozen_field(self, state, params, temp, cell):
+        return _Frozen(float(np.asarray(state)[-1]))
+
+
+def test_frozen_q_batch_converges_and_equals_one_density_solves():
+    s = pd.FrozenQSettings()
+    relax = pd.RelaxSettings(dt=0.1, totalT=1e4, stepT=10.0, divs=10, maxDepth=4, requiredFitness=0.99,
+                             minimumA=1e-6)
+    got = pd.solve_frozen_q_batch(FrozenToy(), {}, 'blob', {}, {}, relax, s, 0.1, [0.5, 0.55, 0.9])
+    assert [g['status'] for g in got] == [pd.STATUS_OK, pd.STATUS_OK, pd.STOP_NAN]
+    for g in got[:2]:
+        assert g['q'] == pytest.approx(ToyAdapter.QSTAR, abs=2e-8)
+        assert abs(g['q'] - g['q_relaxed']) < s.qTol and g['stop'] == pd.STOP_CONVERGED
+        assert g['iters'] > len(s.schedule) and g['A1'] == 0.3
+    for g, rho in zip(got, [0.5, 0.55, 0.9]):
+        one = pd.solve_frozen_q_batch(FrozenToy(), {}, 'blob', {}, {}, relax, s, 0.1, [rho])[0]
+        keys = set(g) - {'wall_s'}
+        assert {k: g[k] for k in keys} == {k: one[k] for k in keys}
+    with pytest.raises(ValueError, match='frozen_field'):
+        pd.solve_frozen_q_batch(ToyAdapter(), {}, 'blob', {}, {}, relax, s, 0.1, [0.5])
+
+
+def test_frozen_q_stage_settings():
+    relax = pd.RelaxSettings(dt=0.1, totalT=1e4, stepT=10.0, divs=10, maxDepth=4, requiredFitness=0.99,
+                             minimumA=1e-6)
+    s = pd.FrozenQSettings()
+    r0, r3 = pd._stage_relax(relax, s, 0), pd._stage_relax(relax, s, 3)
+    assert (r0.fTol, r0.ATol) == (1e-6, 1.0) and (r3.fTol, r3.ATol) == (1e-12, relax.ATol)
+
+
+@pytest.mark.gpu
+def test_log_frozen_q_agrees_with_the_pinned_q0star():
+    """The reference's agreement bounds between the frozen-q search and Find_q0Star
+    (tests/test_phase_diagram_frozen_q.py:69-83: q within 1e-5, f within 1e-9, f_frozen
+    within 1e-10 of f), here against the pinned Find_q0Star result at (-0.9, 0.63) with
+    the q0* test's relaxation settings."""
+    got = pd.solve_frozen_q_batch(pd.LogAdapter(), LOG_PARAMS, 'triangle', CELL, ANSATZ, RELAX,
+                                  pd.FrozenQSettings(), -0.9, [0.63])[0]
+    assert got['status'] == pd.STATUS_OK
+    assert abs(got['q'] - 0.9638831589507376) < 1e-5
+    assert abs(got['f'] - (-0.5535949848941145)) < 1e-9
+    assert abs(got['f_frozen'] - got['f']) < 1e-10
