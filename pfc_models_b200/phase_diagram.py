@@ -27,6 +27,9 @@ out. A phase diagram is hundreds of such evaluations, each on a small cell grid.
   `get_f_abc_batch` over every target's q00 points; `find_q0star` is the one-target form.
 * `scan_density_batch` is `scan_density` (q0star.py:566-635) over those searches, with
   the reference's result arrays and checkpoint files (fmin.npz, qscan.npz).
+* `solve_frozen_q_batch` / `scan_density_frozen` are the frozen-q search
+  (phase_diagram/frozen_q.py:92-243: relax at q, jump q to the frozen field's q_opt,
+  tighten fTol) for many densities in lockstep, with the reference's edge pass.
 
 The ansatz is built on the host with the reference's NumPy operations
 (`_build3Mode`, stdpfc_cpu/phase_diagram.py:171-182 and logpfc_cpu/phase_diagram.py:
@@ -991,3 +994,86 @@ def solve_frozen_q_batch(adapter, params, structure, cell, ansatz, relax, settin
         rec['wall_s'] = wall
         out.append(rec)
     return out
+
+
+def _is_ok(r):
+    return r is not None and r.get('status') == STATUS_OK
+
+
+def edge_walks(grid, results):
+    """(i, d) for every accepted grid index i whose neighbour i + d (d = -1, +1) is not
+    accepted (frozen_q.py:166-177). `grid`: sorted densities; `results`: density -> record."""
+    out = []
+    for i, p in enumerate(grid):
+        if not _is_ok(results.get(p)):
+            continue
+        for d in (-1, 1):
+            j = i + d
+            if 0 <= j < len(grid) and not _is_ok(results.get(grid[j])):
+                out.append((i, d))
+    return out
+
+
+def edge_walk(solve, grid, results, i, d, maxPast=3):
+    """From accepted index i outward in direction d, reruns each non-accepted density by
+    `solve(phi, q_start)` from a fresh ansatz at q_start = q* of grid[i], until an
+    accepted original, the grid's end, or maxPast failures in a row (frozen_q.py:
+    180-196). Returns the records with q_start, edge_from and edge_dir."""
+    q_seed = float(results[grid[i]]['q'])
+    out, fails, j = [], 0, i + d
+    while 0 <= j < len(grid) and fails < maxPast:
+        p = grid[j]
+        if _is_ok(results.get(p)):
+            break
+        r = dict(solve(p, q_seed))
+        r.update(phi=p, q_start=q_seed, edge_from=grid[i], edge_dir=d, pass_='edge')
+        out.append(r)
+        fails = 0 if _is_ok(r) else fails + 1
+        j += d
+    return out
+
+
+def merge_edge(results, edge_records):
+    """`results` with every accepted edge record in place of a non-accepted original (the
+    lowest f among several accepted edge records of one density; frozen_q.py:199-210)."""
+    out = dict(results)
+    for r in edge_records:
+        if not _is_ok(r):
+            continue
+        p = r['phi']
+        cur = out.get(p)
+        if not _is_ok(cur) or (cur.get('pass_') == 'edge' and r['f'] < cur['f']):
+            out[p] = r
+    return out
+
+
+def scan_density_frozen(adapter, params, structure, cell, ansatz, relax, settings, temp, densities, q_start=1.0,
+                        record=None, done=None):
+    """The frozen-q density scan (frozen_q.py:213-243): pass 1 solves every density not
+    in `done` (density -> pass-1 record) from q_start, all of them in one
+    `solve_frozen_q_batch`; pass 2 (settings.edge) walks outward from the accepted
+    densities. `record(rec)` is called after every solve. Returns (final, pass1, edge) as
+    the reference does."""
+    grid = [float(p) for p in densities]
+    if any(b <= a for a, b in zip(grid, grid[1:])):
+        raise ValueError('densities must be strictly increasing')
+    pass1 = dict(done or {})
+    todo = [p for p in grid if p not in pass1]
+    if todo:
+        for p, r in zip(todo, solve_frozen_q_batch(adapter, params, structure, cell, ansatz, relax, settings, temp,
+                                                   todo, q_start=q_start)):
+            r.update(phi=p, pass_='indep')
+            pass1[p] = r
+            if record is not None:
+                record(r)
+    edge = []
+    if settings.edge:
+        def solve(p, q):
+            r = solve_frozen_q_batch(adapter, params, structure, cell, ansatz, relax, settings, temp, [p],
+                                     q_start=q)[0]
+            if record is not None:
+                record({**r, 'phi': p, 'pass_': 'edge'})
+            return r
+        for i, d in edge_walks(grid, pass1):
+            edge += edge_walk(solve, grid, pass1, i, d, settings.maxPast)
+    return merge_edge(pass1, edge), pass1, edge

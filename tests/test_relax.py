@@ -501,3 +501,45 @@ def test_log_frozen_q_agrees_with_the_pinned_q0star():
     assert abs(got['q'] - 0.9638831589507376) < 1e-5
     assert abs(got['f'] - (-0.5535949848941145)) < 1e-9
     assert abs(got['f_frozen'] - got['f']) < 1e-10
+
+
+def test_frozen_edge_helpers():
+    grid = [0.1, 0.2, 0.3, 0.4, 0.5]
+    res = {0.1: {'status': 'poor_fit'}, 0.2: {'status': 'ok', 'q': 0.97, 'f': -1.0},
+           0.3: {'status': 'ok', 'q': 0.98, 'f': -1.1}, 0.4: {'status': 'poor_fit'}, 0.5: {'status': 'poor_fit'}}
+    assert pd.edge_walks(grid, res) == [(1, -1), (2, 1)]
+    calls = []
+
+    def solve(p, q):
+        calls.append((p, q))
+        return {'status': 'ok' if p == 0.4 else 'poor_fit', 'q': q, 'f': -2.0}
+    recs = pd.edge_walk(solve, grid, res, 2, 1, maxPast=3)
+    assert calls == [(0.4, 0.98), (0.5, 0.98)]
+    merged = pd.merge_edge(res, recs)
+    assert merged[0.4]['status'] == 'ok' and merged[0.4]['edge_from'] == 0.3
+    assert merged[0.5]['status'] == 'poor_fit'
+    # two accepted edge records of one density: the lower f wins
+    two = pd.merge_edge({0.4: {'status': 'poor_fit'}},
+                        [{'status': 'ok', 'phi': 0.4, 'f': -1.0, 'pass_': 'edge'},
+                         {'status': 'ok', 'phi': 0.4, 'f': -3.0, 'pass_': 'edge'}])
+    assert two[0.4]['f'] == -3.0
+
+
+def test_frozen_density_scan_batches_pass_one_and_walks_edges():
+    s = pd.FrozenQSettings()
+    relax = pd.RelaxSettings(dt=0.1, totalT=1e4, stepT=10.0, divs=10, maxDepth=4, requiredFitness=0.99,
+                             minimumA=1e-6)
+    recs = []
+    final, pass1, edge = pd.scan_density_frozen(FrozenToy(), {}, 'blob', {}, {}, relax, s, 0.1,
+                                                [0.5, 0.55, 0.9], record=recs.append)
+    assert [pass1[p]['status'] for p in (0.5, 0.55, 0.9)] == [pd.STATUS_OK, pd.STATUS_OK, pd.STOP_NAN]
+    assert [(r['phi'], r['q_start'], r['edge_from']) for r in edge] == [(0.9, pass1[0.55]['q'], 0.55)]
+    assert final[0.9]['status'] == pd.STOP_NAN and final[0.5] is pass1[0.5]
+    assert len(recs) == 4
+    with pytest.raises(ValueError, match='increasing'):
+        pd.scan_density_frozen(FrozenToy(), {}, 'blob', {}, {}, relax, s, 0.1, [0.5, 0.5])
+    # densities with a pass-1 record are not solved again
+    again = []
+    pd.scan_density_frozen(FrozenToy(), {}, 'blob', {}, {}, relax, s, 0.1, [0.5, 0.55, 0.9], record=again.append,
+                           done=pass1)
+    assert [r['pass_'] for r in again] == ['edge']
