@@ -108,3 +108,22 @@ def test_batch_of_more_plans_than_sms_equals_plans_alone():
     for i, (s, t) in enumerate(zip(sims, alone)):
         assert np.array_equal(s.plan.get_state().cpu().numpy(), t.plan.get_state().cpu().numpy()), i
     b.close()
+
+
+@pytest.mark.gpu
+def test_batch_mixing_one_cta_and_two_kernel_classes_equals_plans_alone():
+    """A batch with a one-CTA class (28 x 24 log) and a two-kernel class (64 x 56 std):
+    its 16-step graphs hold one one-CTA launch per block next to the row and column
+    launches of the other class; 37 steps equal each plan stepped alone."""
+    from pfc_models_b200.simulation import Batch
+    sims = [_sim("log", 28, 24, True, seed=1), _sim("std", 64, 56, True, seed=2), _sim("log", 28, 24, True, seed=3)]
+    alone = [_sim("log", 28, 24, True, seed=1), _sim("std", 64, 56, True, seed=2), _sim("log", 28, 24, True, seed=3)]
+    assert [s.plan.path() for s in sims] == ["one_cta", "mixed_radix", "one_cta"]
+    b = Batch(sims)
+    assert b.classes == 2
+    b.step(37)
+    for s in alone:
+        s.TimeSteps(37)
+    for i, (s, t) in enumerate(zip(sims, alone)):
+        assert np.array_equal(s.plan.get_state().cpu().numpy(), t.plan.get_state().cpu().numpy()), i
+    b.close()
