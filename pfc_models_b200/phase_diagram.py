@@ -130,7 +130,12 @@ LOG_STRUCTURES = {
 
 
 class _Adapter:
-    """The adapter contract shared by both models; subclasses set the model."""
+    """The adapter contract shared by both models; subclasses set the model.
+
+    `precision` is the plans' form: "fp64" (the default) resolves f to round-off, as the
+    relaxation's default tolerances assume (fTol 1e-12 relative per block); "fp32"
+    (FP32-mixed) resolves the free energy to about 1e-7 relative, so its relaxations need an
+    fTol above that or they run to totalT. Small FP64 cells step with the one-CTA kernel."""
     SLUG = None
     STRUCTURES = None
     FIELD = None

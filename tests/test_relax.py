@@ -543,3 +543,16 @@ def test_frozen_density_scan_batches_pass_one_and_walks_edges():
     pd.scan_density_frozen(FrozenToy(), {}, 'blob', {}, {}, relax, s, 0.1, [0.5, 0.55, 0.9], record=again.append,
                            done=pass1)
     assert [r['pass_'] for r in again] == ['edge']
+
+
+def test_log_ansatz_equals_the_reference_build(golden):
+    """The reference adapter's clean H2L triangle ansatz at mean 0.7 (the 'dfield_clean'
+    field of tests/golden/frozen.npz, made by make_frozen_golden.py through
+    logpfc_cpu/phase_diagram.py `build` + `get_state`) equals this adapter's host-built
+    ansatz bit for bit."""
+    d = golden("frozen")
+    ad = pd.LogAdapter()
+    got = ad.ansatz_field(ad.STRUCTURES['triangle'], dict(uNx=14, uNy=24, Mx=2, My=1),
+                          dict(mode='H2L', A1=0.9, A2=0.0, A3=0.0), 0.7)
+    assert got.shape == d["dfield_clean"].shape
+    assert np.array_equal(got, d["dfield_clean"])
