@@ -1,0 +1,125 @@
+"""The relaxation driver (pfc_models_b200.phase_diagram) on the oracle's CPU stepper: a
+logPFC adapter whose simulations are oracle.pfc_oracle.OracleSim (the reference's CPU
+step restated in NumPy) and whose diagnose is the oracle's restatement of the adapters'
+fitness (diagnose_modes, divided by the mean as logpfc_cpu/phase_diagram.py:211-223
+does). Driven by `get_f_abc`, it must reproduce the values the reference's own test pins
+for MinimizeFreeEnergy.Get_f_ABC (tests/test_phase_diagram_q0star.py:44-58, 489-510):
+the stop and the step count exactly, f within 1e-12 and fitness and amplitudes within
+1e-12 (the oracle's FFT is NumPy's, the reference's pyFFTW's, so the converged values
+differ by round-off only). This pins the driver's decisions on the real model without a
+GPU; the B200 plans are held to the same pins in test_relax.py."""
+import numpy as np
+import pytest
+
+from oracle import pfc_oracle as orc
+from pfc_models_b200 import diagnostics, phase_diagram as pd
+
+from test_relax import ANSATZ, CELL, LOG_PARAMS, PINNED, RELAX, _check_pinned
+
+
+class _OSim:
+    def __init__(self, sim, dt):
+        self.o, self.dt = sim, dt
+
+    @property
+    def t(self):
+        return self.o.t
+
+
+class OracleLogAdapter(pd.LogAdapter):
+    """LogAdapter with the oracle's CPU stepper in place of B200 plans; counts the
+    fitness evaluations that took the reference's rescaled branch."""
+    rescaled = 0
+
+    def _simulation(self, params, temp, dt, mean, geometry):
+        g = orc.build_geometry(geometry.Nx, geometry.Ny, geometry.Lx, geometry.Ly)
+        p = orc.Params(Gamma=params['Gamma'], beta=params['beta'], q0=params['q0'], epsilon=temp, g=params['g'],
+                       dt=dt)
+        return _OSim(orc.OracleSim("log", p, g), dt)
+
+    def build(self, params, structure, cell, ansatz, temp, meanDensity, q00, dt, state=None, nThreads=1):
+        params = self.validate_params(params)
+        structure = self._structure(structure)
+        cell = self.validate_cell(cell)
+        ansatz = self.validate_ansatz(ansatz)
+        field = self.ansatz_field(structure, cell, ansatz, meanDensity) if state is None else state
+        sim = self._simulation(params, temp, dt, meanDensity, self.box(cell, q00))
+        sim.o.set_field(field)
+        return sim
+
+    def get_state(self, sim):
+        return sim.o.n.copy()
+
+    def set_state(self, sim, state):
+        sim.o.set_field(state)
+
+    def get_time(self, sim):
+        return sim.o.t
+
+    def set_time(self, sim, t):
+        sim.o.t = t
+
+    def get_dt(self, sim):
+        return sim.dt
+
+    def step(self, sim):
+        sim.o.step()
+
+    def step_many(self, sim, n):
+        for _ in range(n):
+            sim.o.step()
+
+    def snapshot(self, sim, out=None):
+        return sim.o.n.copy()
+
+    def release(self, sim):
+        pass
+
+    def lockstep(self, sims):
+        return pd._LoopLockstep(self, sims)
+
+    def free_energy(self, sim):
+        return sim.o.free_energy()
+
+    def diagnose(self, sim, structure, cell):
+        st, c = self._structure(structure), self.validate_cell(cell)
+        rows, cols, sets = diagnostics.mode_table(st, c)
+        mode_sets = [(rows[sets == s], cols[sets == s]) for s in range(3)]
+        n = sim.o.n
+        fitness, A, B, C, _ = orc.diagnose_modes(n, mode_sets, st.amplitudeSign, c['Mx'] * c['My'])
+        mean = np.fft.rfft2(n)[0, 0].real / n.size
+        amps = tuple(abs(a / mean) for a in (A, B, C))
+        rebuilt = self.three_mode(st, c, mean, *(st.amplitudeSign * a * mean for a in amps))
+        if rebuilt.min() < 0:   # the reference rescales the rebuilt field towards the mean
+            self.rescaled += 1
+            fitness = 1 - float(np.abs(np.power(n - self._positive(rebuilt, mean), 2).mean()))
+        return diagnostics.Diagnostics(fitness, amps, {})
+
+
+@pytest.mark.parametrize('ref', [p for p in PINNED if p[0] != 'honeycomb'], ids=['triangle', 'stripe'])
+def test_oracle_relaxation_reproduces_the_reference_pins(ref):
+    structure, eps, phi, q00 = ref[:4]
+    r = pd.get_f_abc(OracleLogAdapter(), LOG_PARAMS, structure, CELL, ANSATZ, RELAX, eps, phi, q00)
+    _check_pinned(r, ref)
+
+
+def test_oracle_relaxation_rolls_back_the_honeycomb_like_the_reference():
+    """dt = 0.1 goes NaN in the honeycomb's first blocks; both are redone at dt 0.01 in ten
+    sub-blocks (22000 steps), and f converges to the reference's value within 1e-12. On the
+    way the rebuilt 3-mode field goes negative, so the log fitness's rescaled branch
+    (logpfc_cpu/phase_diagram.py:196-199) is part of what the pins hold."""
+    ref = next(p for p in PINNED if p[0] == 'honeycomb')
+    ad = OracleLogAdapter()
+    r = pd.get_f_abc(ad, LOG_PARAMS, 'honeycomb', CELL, ANSATZ, RELAX, *ref[1:4])
+    _check_pinned(r, ref)
+    assert ad.rescaled > 0      # some fitness checks on the way take the rescaled branch
+
+
+def test_oracle_batch_driver_returns_the_pins():
+    """The batched driver over the same adapter (its lockstep is a loop over the CPU
+    simulations) returns the pinned triangle and stripe results."""
+    for ref in (p for p in PINNED if p[0] != 'honeycomb'):
+        got = pd.get_f_abc_batch(OracleLogAdapter(), LOG_PARAMS, ref[0], CELL, ANSATZ, RELAX,
+                                 [ref[1:4], (ref[1], ref[2], ref[3] * 1.01)])
+        _check_pinned(got[0], ref)
+        assert got[1].stop == pd.STOP_CONVERGED
