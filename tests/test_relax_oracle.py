@@ -123,3 +123,17 @@ def test_oracle_batch_driver_returns_the_pins():
                                  [ref[1:4], (ref[1], ref[2], ref[3] * 1.01)])
         _check_pinned(got[0], ref)
         assert got[1].stop == pd.STOP_CONVERGED
+
+
+def test_oracle_find_q0star_reproduces_the_reference_pin():
+    """Find_q0Star at (eps -0.9, phi 0.63) on the oracle's stepper through
+    `find_q0star`: q0* within 1e-8 and fmin within 1e-13 of the reference test's values
+    (tests/test_phase_diagram_q0star.py:53, 529-539), in the 392,000 steps the reference
+    test records for it (:531-533). About 40 s of one CPU core."""
+    from test_relax import QSCAN
+    recs = []
+    q, f = pd.find_q0star(OracleLogAdapter(), LOG_PARAMS, 'triangle', CELL, ANSATZ, RELAX, QSCAN, -0.9, 0.63,
+                          record=recs.append)
+    assert abs(q - 0.9638831589507376) < 1e-8
+    assert abs(f - (-0.5535949848941145)) < 1e-13
+    assert sum(r['steps'] for r in recs) == 392000
