@@ -325,6 +325,19 @@ class StdAdapter(_Adapter):
         return _diag.Diagnostics(d.fitness, d.amplitudes, {'maxima_per_cell': d.details['maxima_per_cell']})
 
 
+def scaled_fitness(fit_plus, fit_minus, e, s):
+    """1 - |mean((d - s e)^2)| for a field deviation d (field minus its mean) and a rebuilt
+    deviation e, from the fitnesses against the rebuilt field and its mirror about the
+    mean, 1 - D+ and 1 - D- with D+- = mean((d -+ e)^2) = V -+ 2 X + E (V = mean(d^2),
+    X = mean(d e), E = mean(e^2), taken from `e` on the host): the log adapter's fitness
+    against its 3-mode field rescaled by s (logpfc_cpu/phase_diagram.py:196-199, 220-222)."""
+    d_plus, d_minus = 1.0 - fit_plus, 1.0 - fit_minus
+    E = float(np.mean(e * e))
+    X = (d_minus - d_plus) / 4.0
+    V = (d_plus + d_minus) / 2.0 - E
+    return 1.0 - abs(V - 2.0 * s * X + s * s * E)
+
+
 class LogAdapter(_Adapter):
     """logPFC adapter (models/logpfc_cpu/phase_diagram.py): amplitudes in units of the
     mean density, the 3-mode field rescaled towards the mean where it would go negative."""
@@ -352,9 +365,11 @@ class LogAdapter(_Adapter):
     def diagnose(self, sim, structure, cell):
         """logpfc_cpu/phase_diagram.py:211-223, 309-321: the device's absolute amplitudes
         divided by the mean. Where the rebuilt 3-mode field stays non-negative (its
-        minimum is taken on the host from the four numbers) the fitness is the device's;
-        where the reference would rescale it, the fitness is recomputed from a host copy
-        of the field against the rescaled 3-mode field."""
+        minimum is taken on the host from the four numbers) the fitness is the device's.
+        Where the reference rescales it towards the mean by s = mean / (mean - min), a
+        second device pass with the amplitude sign flipped gives the fitness against the
+        rebuilt field mirrored about the mean, and the rescaled fitness follows from the
+        two (`scaled_fitness`); the field stays on the device."""
         st, c = self._structure(structure), self.validate_cell(cell)
         d = _diag.diagnose(sim, st, c)
         mean = d.details['mean']
@@ -362,10 +377,10 @@ class LogAdapter(_Adapter):
         sign = st.amplitudeSign
         rebuilt = self.three_mode(st, c, mean, *(sign * a * mean for a in amps))
         fitness = d.fitness
-        if rebuilt.min() < 0:
-            field = sim.plan.get_state().cpu().numpy()
-            rebuilt = self._positive(rebuilt, mean)
-            fitness = 1 - float(np.abs(np.power(field - rebuilt, 2).mean()))
+        low = rebuilt.min()
+        if low < 0:
+            mirrored = _diag.diagnose(sim, replace(st, amplitudeSign=-sign), c)
+            fitness = scaled_fitness(d.fitness, mirrored.fitness, rebuilt - mean, mean / (mean - low))
         return _diag.Diagnostics(fitness, amps, {'maxima_per_cell': d.details['maxima_per_cell']})
 
     def frozen_field(self, state, params, temp, cell):

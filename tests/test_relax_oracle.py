@@ -90,9 +90,14 @@ class OracleLogAdapter(pd.LogAdapter):
         mean = np.fft.rfft2(n)[0, 0].real / n.size
         amps = tuple(abs(a / mean) for a in (A, B, C))
         rebuilt = self.three_mode(st, c, mean, *(st.amplitudeSign * a * mean for a in amps))
-        if rebuilt.min() < 0:   # the reference rescales the rebuilt field towards the mean
+        low = rebuilt.min()
+        if low < 0:   # the reference rescales the rebuilt field towards the mean
             self.rescaled += 1
-            fitness = 1 - float(np.abs(np.power(n - self._positive(rebuilt, mean), 2).mean()))
+            # as the B200 adapter does it: from the fitness against the mirrored field
+            mirrored = orc.diagnose_modes(n, mode_sets, -st.amplitudeSign, c['Mx'] * c['My'])[0]
+            fitness = pd.scaled_fitness(fitness, mirrored, rebuilt - mean, mean / (mean - low))
+            direct = 1 - float(np.abs(np.power(n - self._positive(rebuilt, mean), 2).mean()))
+            assert abs(fitness - direct) < 1e-13
         return diagnostics.Diagnostics(fitness, amps, {})
 
 
