@@ -556,3 +556,19 @@ def test_log_ansatz_equals_the_reference_build(golden):
                           dict(mode='H2L', A1=0.9, A2=0.0, A3=0.0), 0.7)
     assert got.shape == d["dfield_clean"].shape
     assert np.array_equal(got, d["dfield_clean"])
+
+
+def test_scaled_fitness_identity():
+    """The log adapter's rescaled fitness from the fitnesses against the rebuilt field and
+    its mirror: equal to the direct mean of (d - s e)^2."""
+    rng = np.random.default_rng(5)
+    for _ in range(20):
+        d = 0.1 * rng.standard_normal((24, 28))
+        d -= d.mean()
+        e = 0.1 * rng.standard_normal((24, 28))
+        e -= e.mean()
+        s = rng.uniform(0.3, 1.0)
+        plus = 1 - float(np.mean((d - e) ** 2))
+        minus = 1 - float(np.mean((d + e) ** 2))
+        direct = 1 - float(np.mean((d - s * e) ** 2))
+        assert pd.scaled_fitness(plus, minus, e, s) == pytest.approx(direct, abs=1e-14)
