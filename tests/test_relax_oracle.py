@@ -142,3 +142,18 @@ def test_oracle_find_q0star_reproduces_the_reference_pin():
     assert abs(q - 0.9638831589507376) < 1e-8
     assert abs(f - (-0.5535949848941145)) < 1e-13
     assert sum(r['steps'] for r in recs) == 392000
+
+
+def test_oracle_density_scan_reproduces_the_status_points():
+    """tests/test_phase_diagram_q0star.py:542-551: (-0.9, 0.51) and (-0.9, 0.52) end with
+    no local minimum, the reference's message, in the 66,000 and 56,000 steps its comment
+    records; here through `scan_density_batch` (one batched search) on the oracle's
+    stepper. About 10 s of one CPU core."""
+    from test_relax import QSCAN
+    r = pd.scan_density_batch(OracleLogAdapter(), LOG_PARAMS, 'triangle', CELL, ANSATZ, RELAX, QSCAN, -0.9,
+                              [0.51, 0.52])
+    assert [str(x) for x in r['status']] == [pd.STATUS_NO_LOCAL_MINIMUM] * 2
+    assert [str(x) for x in r['message']] == [pd.MSG_NO_LOCAL_MINIMUM] * 2
+    assert np.isnan(r['q0star']).all() and np.isnan(r['fmin']).all()
+    q = r['qscan']
+    assert [int(q['steps'][q['phi_index'] == k].sum()) for k in range(2)] == [66000, 56000]
