@@ -157,3 +157,36 @@ def test_oracle_density_scan_reproduces_the_status_points():
     assert np.isnan(r['q0star']).all() and np.isnan(r['fmin']).all()
     q = r['qscan']
     assert [int(q['steps'][q['phi_index'] == k].sum()) for k in range(2)] == [66000, 56000]
+
+
+class OracleFrozenAdapter(OracleLogAdapter):
+    """Also the frozen field of the oracle (frozen_moments, logpfc_cpu/phase_diagram.py:
+    465-505); no defect screen."""
+    defect_diagnostics = None
+
+    def frozen_field(self, state, params, temp, cell):
+        A, local = orc.frozen_moments(np.asarray(state), temp, params['g'], 1.0, cell)
+        return diagnostics.FrozenField(A, local, params['beta'], params.get('q0', 1.0))
+
+
+def test_oracle_frozen_q_agrees_with_find_q0star_under_adaptive_dt():
+    """tests/test_phase_diagram_frozen_q.py:69-83 on the oracle's stepper: the 14 x 12
+    cell (7 x 12, 2 x 1), an H2L ansatz and adaptive dt (0.01 up to 0.1); the frozen-q
+    search and Find_q0Star agree within the reference test's bounds (q 1e-5, f 1e-9,
+    f_frozen within 1e-10 of f). About 30 s of one CPU core."""
+    small = {'uNx': 7, 'uNy': 12, 'Mx': 2, 'My': 1}
+    h2l = {'mode': 'H2L', 'A1': 0.9, 'A2': 0.0, 'A3': 0.0}
+    relax = pd.RelaxSettings(dt=0.01, dtMax=0.1, dtRate=1e-5, dtGrow=2.0, dtChecks=10, totalT=1e6, stepT=100.0,
+                             divs=10, maxDepth=4, requiredFitness=0.99, minimumA=1e-6)
+    qs = pd.QScanSettings(passes=3, Deltaq=0.02, q00_Steps=21, Deltaq_Refinement=0.05)
+    params = {'beta': 0.5, 'g': -2.0, 'v0': 1.0}
+    recs = []
+    q_f, f_f = pd.find_q0star(OracleFrozenAdapter(), params, 'triangle', small, h2l, relax, qs, -0.9, 0.62,
+                              record=recs.append)
+    assert max(r['dt_max'] for r in recs) == pytest.approx(0.1)     # dt grew to dtMax
+    r = pd.solve_frozen_q_batch(OracleFrozenAdapter(), params, 'triangle', small, h2l, relax, pd.FrozenQSettings(),
+                                -0.9, [0.62])[0]
+    assert r['status'] == pd.STATUS_OK
+    assert abs(r['q'] - q_f) < 1e-5
+    assert abs(r['f'] - f_f) < 1e-9
+    assert abs(r['f_frozen'] - r['f']) < 1e-10
