@@ -45,6 +45,7 @@ from dataclasses import dataclass, replace
 
 import numpy as np
 
+from . import _lib
 from . import diagnostics as _diag
 from . import logpfc as _logpfc
 from . import stdpfc as _stdpfc
@@ -228,6 +229,7 @@ class _Adapter:
 
     def step(self, sim):
         sim.TimeStep()
+        _count_steps(sim, 1)
 
     def free_energy(self, sim):
         return sim.CalculateFreeEnergy()
@@ -236,6 +238,12 @@ class _Adapter:
     def step_many(self, sim, n):
         """n steps in one call (graph replay, no host round trip between steps)."""
         sim.TimeSteps(n)
+        _count_steps(sim, n)
+
+    def lockstep_key(self, sim):
+        """Plans step together only at the same ping-pong parity: the parity of the steps
+        a plan has taken since it was built (setting a state keeps the parity)."""
+        return getattr(sim, '_relax_steps', 0) & 1
 
     def snapshot(self, sim, out=None):
         """The state as a device array (into `out` when given); `set_state` takes it back."""
@@ -248,14 +256,29 @@ class _Adapter:
         return _PlanLockstep(sims)
 
 
+def _count_steps(sim, n):
+    sim._relax_steps = getattr(sim, '_relax_steps', 0) + n
+
+
 class _PlanLockstep:
     """Simulations stepped together through one `Batch`; F of all of them in one copy."""
 
     def __init__(self, sims):
-        self.batch = Batch(sims)
+        self.sims = list(sims)
+        self.batch = Batch(self.sims)
 
     def step(self, n):
-        self.batch.step(n)
+        try:
+            self.batch.step(n)
+        except _lib.PfcError as e:
+            # plans at different ping-pong parities: refused before any launch; the plans
+            # then step one by one (a batch step equals each plan's own steps)
+            if e.code != _lib.PFC_E_STATE:
+                raise
+            for sim in self.sims:
+                sim.TimeSteps(n)
+        for sim in self.sims:
+            _count_steps(sim, n)
 
     def free_energies(self):
         return self.batch.reduce()[:, 0]
@@ -549,6 +572,112 @@ def _single(run, point, state, keep_state):
         _release(ad, sim)
 
 
+# ---------------------------------------------------------------- adaptive dt in lockstep
+# The one-point evaluation again, written as a generator that yields (simulation, steps)
+# wherever it steps and is resumed once those steps are done, so that a scheduler can
+# step the members that ask for the same number of steps together (their dt may differ:
+# each plan steps with its own coefficients). Every adapter call is the one `_single`,
+# `_Run.take_step` and `_Run.rollback` make, in the same order.
+def _take_step_gen(run, sim, point, stepT, depth, counter, f_last=None):
+    ad, r = run.ad, run.relax
+    mini = int(round(stepT / ad.get_dt(sim)))
+    phi_last = _snapshot(ad, sim)
+    t_last = ad.get_time(sim)
+    f_last = ad.free_energy(sim) if f_last is None else f_last
+    yield sim, mini
+    counter[0] += mini
+    f = ad.free_energy(sim)
+    delta_f = f - f_last
+    if np.isnan(f) or delta_f > r.fTol * abs(f_last):
+        ad.set_state(sim, phi_last)
+        ad.set_time(sim, t_last)
+        if depth >= r.maxDepth:
+            raise MaxDepthReached(f'Max recursion depth reached at t={ad.get_time(sim):0.6f}', nan=bool(np.isnan(f)))
+        sub = run.generate(*point, ad.get_dt(sim) / r.divs, state=phi_last)
+        try:
+            ad.set_time(sub, ad.get_time(sim))
+            for _ in range(r.divs):
+                yield from _take_step_gen(run, sub, point, stepT / r.divs, depth + 1, counter)
+                ad.set_state(sim, _snapshot(ad, sub))
+                ad.set_time(sim, ad.get_time(sub))
+        finally:
+            _release(ad, sub)
+        return ad.free_energy(sim) - f_last
+    return delta_f
+
+
+def _single_gen(run, point, state, keep_state):
+    """`_single` with adaptive dt as a generator; returns the RelaxResult."""
+    ad, r = run.ad, run.relax
+    sim = run.generate(*point, run.first_dt(), state=state)
+    try:
+        f_last = ad.free_energy(sim)
+        A_last = run.amplitude(sim)
+        stop, counter, dt_max = STOP_TOTALT, [0], ad.get_dt(sim)
+        for _ in range(int(r.totalT / r.stepT)):
+            try:
+                f0, sub_t = f_last, r.stepT / r.dtChecks
+                As = A_last
+                for k in range(r.dtChecks):
+                    d_sub = yield from _take_step_gen(run, sim, point, sub_t, 0, counter)
+                    fs_new = ad.free_energy(sim)
+                    As_new = run.amplitude(sim)
+                    if k < r.dtChecks - 1:
+                        sim, dt_max = run.adapt_dt(sim, point, sub_t, d_sub, fs_new, As_new, As, dt_max)
+                    As = As_new
+                delta_f = ad.free_energy(sim) - f0
+            except MaxDepthReached as e:
+                stop = STOP_NAN if e.nan else STOP_MAX_DEPTH
+                break
+            f_last = ad.free_energy(sim)
+            reason, A = run.check(sim, delta_f, f_last, A_last)
+            if reason is not None:
+                stop = reason
+                break
+            sim, dt_max = run.adapt_dt(sim, point, r.stepT / r.dtChecks, delta_f / r.dtChecks, f_last, A, A_last,
+                                       dt_max)
+            A_last = A
+        return run.finish(sim, stop, counter[0], dt_max, keep_state)
+    finally:
+        _release(ad, sim)
+
+
+def _adaptive_batch(run, points, states, keep_state):
+    """Adaptive-dt evaluations in lockstep: each round, the members' pending step
+    requests are grouped by step count and each group is stepped as one batch."""
+    ad = run.ad
+    gens = [_single_gen(run, p, s, keep_state) for p, s in zip(points, states)]
+    results = [None] * len(gens)
+    pending = {}
+    try:
+        for i, g in enumerate(gens):
+            try:
+                pending[i] = next(g)
+            except StopIteration as e:
+                results[i] = e.value
+        while pending:
+            groups = {}
+            for i, (sim, n) in pending.items():
+                key = (n, ad.lockstep_key(sim) if hasattr(ad, 'lockstep_key') else None)
+                groups.setdefault(key, []).append(i)
+            for (n, _), idx in groups.items():
+                lock = _lockstep(ad, [pending[i][0] for i in idx])
+                try:
+                    lock.step(n)
+                finally:
+                    lock.close()
+            for i in sorted(pending):
+                try:
+                    pending[i] = gens[i].send(None)
+                except StopIteration as e:
+                    results[i] = e.value
+                    del pending[i]
+        return results
+    finally:
+        for g in gens:
+            g.close()
+
+
 # ---------------------------------------------------------------- many evaluations
 class _Member:
     def __init__(self, index, point, sim, f_last, A_last):
@@ -563,15 +692,15 @@ def get_f_abc_batch(adapter, params, structure, cell, ansatz, relax, points, sta
     """`Get_f_ABC` for every (temp, meanDensity, q00) of `points`, the members stepped
     together (see the module docstring). Returns RelaxResults in the order of `points`,
     each equal to what `get_f_abc` returns for that point. With adaptive dt
-    (relax.dtMax set) every member has its own dt schedule, so the points run one after
-    another through `get_f_abc`."""
+    (relax.dtMax set) every member has its own dt schedule: the members that ask for the
+    same number of steps next are stepped together (`_adaptive_batch`)."""
     run = _Run(adapter, params, structure, cell, ansatz, relax)
     points = [tuple(float(v) for v in p) for p in points]
     states = [None] * len(points) if states is None else list(states)
     if len(states) != len(points):
         raise ValueError('states must match points')
     if relax.dtMax is not None:
-        return [_single(run, p, s, keep_state) for p, s in zip(points, states)]
+        return _adaptive_batch(run, points, states, keep_state)
     ad, r = run.ad, run.relax
     dt = run.first_dt()
     mini = int(round(r.stepT / dt))

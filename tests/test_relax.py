@@ -572,3 +572,23 @@ def test_scaled_fitness_identity():
         minus = 1 - float(np.mean((d + e) ** 2))
         direct = 1 - float(np.mean((d - s * e) ** 2))
         assert pd.scaled_fitness(plus, minus, e, s) == pytest.approx(direct, abs=1e-14)
+
+
+def test_adaptive_dt_batch_equals_one_point_runs():
+    """With adaptive dt the members ask for different step counts; the batch steps the
+    members that ask for the same count together and returns the one-point results."""
+    relax = pd.RelaxSettings(dt=0.1, totalT=1e4, stepT=10.0, divs=10, maxDepth=4, requiredFitness=0.99,
+                             minimumA=1e-6, dtMax=1.0)
+    points = [(0.1, 0.5, 1.0), (0.1, 0.75, 1.0), (0.1, 0.9, 1.0), (0.1, 0.6, 1.0), (0.1, 0.5, 1.3),
+              (0.2, 0.55, 0.98)]
+    ad = ToyAdapter()
+    got = pd.get_f_abc_batch(ad, {}, 'blob', {}, {}, relax, points)
+    total = 0
+    for g, p in zip(got, points):
+        one = ToyAdapter()
+        w = pd.get_f_abc(one, {}, 'blob', {}, {}, relax, *p)
+        total += one.steps
+        assert (g.values(), g.stop, g.steps, g.dt_max) == (w.values(), w.stop, w.steps, w.dt_max), p
+    assert ad.steps == total
+    assert {g.stop for g in got} == {pd.STOP_CONVERGED, pd.STOP_NAN, pd.STOP_POOR_FIT}
+    assert max(g.dt_max for g in got) > 0.1

@@ -230,3 +230,19 @@ def test_oracle_std_relaxation_reproduces_the_recorded_mirror_values():
     assert hc.values() == pytest.approx(tri.values(), abs=1e-14)
     liquid = (1.0 - 0.25) / 2 * 0.25 ** 2 + 0.25 ** 4 / 4
     assert tri.f < liquid
+
+
+def test_oracle_adaptive_dt_batch_equals_one_point_runs():
+    """Adaptive dt (0.01 up to 0.1) on the oracle's logPFC stepper, the 14 x 12 cell: three
+    q00 points as one batch equal the one-point runs bit for bit."""
+    small = {'uNx': 7, 'uNy': 12, 'Mx': 2, 'My': 1}
+    h2l = {'mode': 'H2L', 'A1': 0.9, 'A2': 0.0, 'A3': 0.0}
+    relax = pd.RelaxSettings(dt=0.01, dtMax=0.1, dtRate=1e-5, dtGrow=2.0, dtChecks=10, totalT=1e6, stepT=100.0,
+                             divs=10, maxDepth=4, requiredFitness=0.99, minimumA=1e-6)
+    params = {'beta': 0.5, 'g': -2.0, 'v0': 1.0}
+    points = [(-0.9, 0.62, 0.94), (-0.9, 0.62, 0.96), (-0.9, 0.62, 1.0)]
+    got = pd.get_f_abc_batch(OracleLogAdapter(), params, 'triangle', small, h2l, relax, points)
+    for g, p in zip(got, points):
+        w = pd.get_f_abc(OracleLogAdapter(), params, 'triangle', small, h2l, relax, *p)
+        assert (g.values(), g.stop, g.steps, g.dt_max) == (w.values(), w.stop, w.steps, w.dt_max), p
+    assert all(g.dt_max == pytest.approx(0.1) for g in got)
