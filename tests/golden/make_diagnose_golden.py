@@ -3,8 +3,8 @@
 Run in a container where the reference checkout exists (it is not needed, and not
 present, where the tests run):
 
-    NUMBA_CACHE_DIR=/tmp/numba_cache PYTHONPYCACHEPREFIX=/tmp/pycache \
-        python tests/golden/make_diagnose_golden.py /root/reference
+    NUMBA_CACHE_DIR=<scratch dir> PYTHONPYCACHEPREFIX=<scratch dir> \
+        python tests/golden/make_diagnose_golden.py <reference checkout>
 
 `diagnose(sim, structure, cell)` (src/pfc_models/models/stdpfc_cpu/phase_diagram.py:
 178-215) needs from `sim` only `n`, `State.n`, `State.n_hat`, `fft_fwd` and `Geometry`;
@@ -74,4 +74,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PFC_REFERENCE", "."))
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <reference checkout>")
+    main(sys.argv[1])

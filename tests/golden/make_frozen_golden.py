@@ -3,8 +3,8 @@
 Run in a container where the reference checkout exists (it is not needed, and not
 present, where the tests run):
 
-    NUMBA_CACHE_DIR=/tmp/numba_cache PYTHONPYCACHEPREFIX=/tmp/pycache \
-        python tests/golden/make_frozen_golden.py /root/reference
+    NUMBA_CACHE_DIR=<scratch dir> PYTHONPYCACHEPREFIX=<scratch dir> \
+        python tests/golden/make_frozen_golden.py <reference checkout>
 
 For the three parameter sets of the reference's own test
 (tests/test_phase_diagram_frozen_q.py:22-37: a 'triangle' H2L ansatz in the
@@ -73,4 +73,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PFC_REFERENCE", "."))
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <reference checkout>")
+    main(sys.argv[1])

@@ -3,8 +3,8 @@
 Run in a container where the reference checkout exists (it is not needed, and
 not present, where the tests run):
 
-    NUMBA_CACHE_DIR=/tmp/numba_cache PYTHONPYCACHEPREFIX=/tmp/pycache \
-        python tests/golden/make_golden.py /root/reference
+    NUMBA_CACHE_DIR=<scratch dir> PYTHONPYCACHEPREFIX=<scratch dir> \
+        python tests/golden/make_golden.py <reference checkout>
 
 The reference's CPU models (``pfc_models.models.stdpfc_cpu`` and
 ``logpfc_cpu``) import pyFFTW, which is absent here; ``pyfftw_standin/`` puts a
@@ -229,4 +229,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <reference checkout>")
+    main(sys.argv[1])

@@ -2,14 +2,16 @@
 test (tests/test_phase_diagram_common_tangent.py:43-77): the eps = -0.9 logPFC
 triangle table (phi, fmin, q0*) and the coexistence densities it pins.
 
-    python tests/golden/make_tangent_golden.py /root/reference
+    python tests/golden/make_tangent_golden.py <reference checkout>
 """
 import ast
 import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(f"usage: python {sys.argv[0]} <reference checkout>")
+ref = sys.argv[1]
 src = open(os.path.join(ref, "tests", "test_phase_diagram_common_tangent.py")).read()
 tree = ast.parse(src)
 vals = {}

@@ -3,7 +3,7 @@
 Run in a container where the reference checkout exists (it is not needed, and not
 present, where the tests run):
 
-    PYTHONPYCACHEPREFIX=/tmp/pycache python tests/golden/make_vacancy_golden.py /root/reference
+    PYTHONPYCACHEPREFIX=<scratch dir> python tests/golden/make_vacancy_golden.py <reference checkout>
 
 `_VacancyTracker` (src/pfc_models/analysis/vacancy_tracker.py) is plain NumPy, so its
 module is loaded by file path and run unmodified. The fields are seeded synthetic
@@ -150,4 +150,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PFC_REFERENCE", "."))
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <reference checkout>")
+    main(sys.argv[1])
