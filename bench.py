@@ -2,26 +2,40 @@
 """PFC site-steps/s on B200: the fused ETD1 stepper on the 2048^2 stdPFC polycrystal.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --kernel-case --nx 2048 --ny 2048 --precision fp32 --steps 4 [--batch K]
 
 Workload (stdPFC polycrystal, 2048^2): dx = dy = pi/4, dt = 0.5, r = epsilon = -0.3,
 Gamma = beta = q0 = 1, g = 0; mean psi = -0.3 plus 0.01 U[-1,1] noise (seed 0) and
 64 seeds of radius 12 dx with the rotated one-mode profile (seed 1). Synthetic,
 seeded; no dataset is involved.
 
-One bench step = one ETD1 time step (row kernel + column kernel). `value` is the
-FP32-mixed form with the state resident in HBM, each step timed with a pair of CUDA
-events on the launching stream and L2 flushed (a 256 MiB write) between steps, so
-every step starts from HBM. The per-kernel durations behind `roofline` come from a
-second pass of the same number of steps with events around each launch. The FP64 plain form is timed the same way (`fp64_plain`).
-`e2e` is the same metric through the public Python API (`State.n[...] = host`,
-`TimeStep()` x 100, `CalculateFreeEnergy()`), the host field pinned, both copies
-(the field in, F/mu/mean out) inside the timed region. Under torchrun with N > 1 every rank runs an
-independent replica (a single simulation does not shard profitably over NVLink);
-timings are the max over ranks.
+One bench step = one block of 16 ETD1 time steps (32 kernel launches), replayed from the
+plan's 16-step CUDA graph: the unit in which the 20000-step run advances. `value` is the
+FP32-mixed form with the state resident in HBM; each bench step is timed with a pair of
+CUDA events on the launching stream and L2 is flushed (a 256 MiB write, outside the
+events) between bench steps, so every block starts from HBM; inside a block the 60 MB
+working set stays in L2 from one time step to the next, as it does in the long run. The
+per-kernel durations behind `roofline` come from a second pass of the same blocks with
+events around each launch. The FP64 plain form is timed the same way (`fp64_plain`).
+`single_step` repeats the measurement with one time step per bench step (L2 flushed
+between time steps); `solidify8192` times the 8192^2 workload, whose 1.6 GB working set
+does not fit in L2 (the HBM-bound case).
+`accuracy` steps both forms 20000 steps in lockstep from the same field (outside every
+timed region) and states the FP32-mixed error against FP64: F per site, mu per site,
+psi in relative L2, and the mass drift.
+`e2e` is the same metric through the public Python API: per frame of 8 bench steps,
+`State.n[...] = host field` (pinned, FP64), 128 `TimeStep()` calls and
+`CalculateFreeEnergy()` (F, mu and mean to the host), all inside the timed region.
+Under torchrun with N > 1 every rank runs an independent replica (a single simulation
+does not shard profitably over NVLink); timings are the max over ranks.
 
 `--impl reference` times the reference's CPU algorithm (the oracle port of
 stdpfc_cpu, threaded pocketfft through scipy.fft with every host core) on the
 same workload and metric.
+
+`--kernel-case` runs a short fixed stepper workload (a noisy liquid of the given size,
+or `--batch K` such plans stepped together) and prints per-kernel device times: the
+small case for ncu captures.
 """
 from __future__ import annotations
 
@@ -44,24 +58,29 @@ UNIT = "site-steps/s"
 NX = NY = 2048
 DX = math.pi / 4
 PARAMS = dict(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.3, g=0.0, dt=0.5)
-E2E_STEPS = 100
+BLOCK = 16                 # ETD1 time steps per bench step (one graph replay)
+E2E_BLOCKS = 8             # bench steps per e2e frame (one upload, one F read-back)
+ACCURACY_STEPS = 20000     # the workload's full length
 FLUSH_BYTES = 256 << 20
 
 
 def workload_config(extra=None):
     c = {"workload": "stdPFC polycrystal 2048x2048, dx=pi/4, dt=0.5, r=-0.3, 64 seeds r=12dx, FP32-mixed",
          "nx": NX, "ny": NY, "model": "stdPFC", "precision": "fp32_mixed",
-         "l2": "flushed between steps (256 MiB write)"}
+         "step": f"{BLOCK} ETD1 time steps (one CUDA graph replay, {2 * BLOCK} kernel launches)",
+         "l2": "flushed (256 MiB write) between bench steps; the 60 MB working set stays in L2 between "
+               "the time steps of a block, as in the 20000-step run"}
     if extra:
         c.update(extra)
     return c
 
 
 def initial_field():
-    from pfc_models_b200 import fields, spectral
-    g = spectral.Build2DGeometry(NX, NY, NX * DX, NY * DX)
-    return g, fields.GeneratePolycrystalInitialConditions(g, -0.3, 0.01, nSeeds=64, radius=12 * DX,
-                                                          A=0.5, q=math.sqrt(3) / 2, noise_seed=0, seed=1)
+    from pfc_models_b200 import workloads
+    from pfc_models_b200 import spectral
+    p = workloads.parameters("polycrystal2048")
+    g = spectral.Build2DGeometry(p["Nx"], p["Ny"], p["Lx"], p["Ly"])
+    return g, workloads.initial_field("polycrystal2048", g)
 
 
 def peaks():
@@ -75,17 +94,23 @@ def peaks():
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """Samples SM clock and clock-event reasons of one GPU during the timed region
-    through NVML (read-only queries), polled every 2 ms from a thread."""
+    """Samples SM clock and clock-event reasons of one GPU through NVML (read-only
+    queries), polled every 2 ms from a thread while the GPU work of the bench runs.
+    `mark(True/False)` brackets the timed regions; samples inside them are reported
+    apart from the whole run's."""
 
     REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
                0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
-        self.samples = []
+        self.samples = []      # (clock MHz, in a timed region)
         self.reasons = 0
         self.thread = None
+        self.timed = False
+
+    def mark(self, timed):
+        self.timed = bool(timed)
 
     def start(self):
         import threading
@@ -118,7 +143,7 @@ class ClockSampler:
         def loop():
             while not self.stop_flag:
                 try:
-                    self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                    self.samples.append((self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM), self.timed))
                     self.reasons |= int(get_r(self.h))
                 except Exception:
                     pass
@@ -135,8 +160,14 @@ class ClockSampler:
         if not self.samples:
             return None
         names = sorted(n for bit, n in self.REASONS.items() if self.reasons & bit)
-        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz, "reasons": names,
-                "samples": len(self.samples), "source": "nvml"}
+        allc = [c for c, _ in self.samples]
+        timed = [c for c, t in self.samples if t]
+        under = timed if len(timed) >= 5 else allc
+        return {"sm_mhz": statistics.median(under), "sm_max_mhz": self.max_mhz, "reasons": names,
+                "samples": len(under), "sm_mhz_min": min(under), "all_samples": len(allc),
+                "all_sm_mhz": statistics.median(allc),
+                "source": "nvml every 2 ms; sm_mhz and samples cover the timed regions (2048^2 blocks and "
+                          "single steps, e2e, 8192^2), all_* the whole run from the first warm-up"}
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle port)
@@ -173,6 +204,8 @@ def run_reference(args):
     sim.set_field(f0)
     for _ in range(max(args.warmup, 1)):
         sim.step()
+    # each bench step is a bounded sample of one block: 1 ETD1 step of the CPU stepper
+    # stands for the block's 16 (the metric is per site-step, so the rate is the same)
     budget_s = 150.0
     times = []
     t_all = time.perf_counter()
@@ -186,16 +219,72 @@ def run_reference(args):
     value = NX * NY * len(times) / total
     sample = (f"{len(times)} of {args.steps} requested ETD1 steps at 2048^2 "
               f"(stopped at the {budget_s:.0f} s budget)" if len(times) < args.steps else
-              f"{len(times)} ETD1 steps at 2048^2")
+              f"{len(times)} ETD1 steps at 2048^2, one per bench step")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded polycrystal)",
-            "config": workload_config({"precision": "fp64 (reference CPU algorithm)", "l2": "n/a (CPU)"}),
+            "config": workload_config({"precision": "fp64 (reference CPU algorithm)", "l2": "n/a (CPU)",
+                                       "step": "1 ETD1 time step (a bounded sample of a 16-step block)"}),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": sample + f", numpy/scipy pocketfft, {cores} threads"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ kernel case (ncu)
+def run_kernel_case(a):
+    """A short fixed stepper workload: a noisy liquid of nx x ny (stdPFC r = -0.3 at mean
+    -0.3, or logPFC with the eps = -0.9 parameter set at mean 0.55), `steps` ETD1 steps
+    with CUDA events around each launch; or `batch` such plans stepped together. Keeps the
+    device footprint to the plans' buffers so that an ncu capture of a few launches ends
+    quickly."""
+    import torch
+
+    from pfc_models_b200 import fields, logpfc, stdpfc
+    mod = stdpfc if a.model == "std" else logpfc
+    geom = mod.Build2DGeometry(a.nx, a.ny, a.nx * math.pi / 4, a.ny * math.pi / 4)
+    if a.model == "std":
+        prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.3, g=0.0, dt=0.5)
+        mean = -0.3
+    else:
+        prm = logpfc.BuildLogPFCModelParameters(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=0.1)
+        mean = 0.55
+    if a.batch > 0:
+        from pfc_models_b200.simulation import Batch
+        sims = []
+        for k in range(a.batch):
+            s = mod.BuildB200_Simulation(prm, geom, precision=a.precision)
+            (s.State.n if a.model == "std" else s.State.phi)[...] = fields.GenerateNoisyLiquid(geom, mean, 0.01,
+                                                                                                 seed=k)
+            sims.append(s)
+        b = Batch(sims)
+        b.step(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        b.step(a.steps)
+        e1.record()
+        e1.synchronize()
+        F = b.reduce()[:, 0]
+        us = 1e3 * e0.elapsed_time(e1) / a.steps
+        print(json.dumps({"nx": a.nx, "ny": a.ny, "precision": a.precision, "model": a.model, "steps": a.steps,
+                          "batch": a.batch, "path": sims[0].plan.path(), "classes": b.classes,
+                          "us_per_step": us, "site_steps_per_s": a.batch * a.nx * a.ny / (us * 1e-6),
+                          "finite": bool(np.isfinite(F).all())}))
+        b.close()
+        return 0
+    sim = mod.BuildB200_Simulation(prm, geom, precision=a.precision)
+    field = sim.State.n if a.model == "std" else sim.State.phi
+    field[...] = fields.GenerateNoisyLiquid(geom, mean, 0.01, seed=0)
+    ms_r, ms_c = sim.plan.step_timed(a.steps)
+    torch.cuda.synchronize()
+    F = float(sim.CalculateFreeEnergy())
+    print(json.dumps({"nx": a.nx, "ny": a.ny, "precision": a.precision, "model": a.model, "steps": a.steps,
+                      "row_us": 1e3 * ms_r / a.steps, "col_us": 1e3 * ms_c / a.steps, "F": F,
+                      "finite": bool(np.isfinite(F)), "plan": sim.plan.info(), "variant": sim.plan.variant()}))
+    sim.plan.close()
     return 0
 
 
@@ -227,10 +316,12 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    from pfc_models_b200 import stdpfc
+    from pfc_models_b200 import stdpfc, workloads
 
     geom, f0 = initial_field()
     flush_buf = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    clocks = ClockSampler(local)
+    clocks.start()
 
     def flush():
         flush_buf.zero_()
@@ -240,93 +331,126 @@ def run_ours(args):
         sim.State.n[...] = f0
         return sim
 
-    def time_steps(sim, k, sampler=None):
-        """The timed region: k steps, each bracketed by its own pair of CUDA events on the
-        launching stream (nothing recorded between the two kernels of a step), L2 flushed
-        between steps outside the events."""
+    def time_blocks(plan, k, block):
+        """The timed region: k bench steps of `block` time steps each, every one bracketed by
+        its own pair of CUDA events on the launching stream (nothing recorded between the
+        kernels of a block), L2 flushed between bench steps outside the events."""
         s = torch.cuda.current_stream(dev)
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
-        launches0 = sim.plan.launches()
+        launches0 = plan.launches()
         barrier()
-        if sampler:
-            sampler.start()
+        clocks.mark(True)
         for a, b in evs:
             a.record(s)
-            sim.plan.step(1)
+            plan.step(block)
             b.record(s)
             flush()
         barrier()
-        clocks = sampler.stop() if sampler else None
-        return [a.elapsed_time(b) for a, b in evs], sim.plan.launches() - launches0, clocks
+        clocks.mark(False)
+        return [a.elapsed_time(b) for a, b in evs], plan.launches() - launches0
 
-    def time_kernels(sim, k):
-        """Per-kernel durations for the roofline: k more steps with events around each of
-        the two launches (an event between the kernels adds a few us, so this pass is kept
-        apart from the timed region above), L2 flushed between steps."""
-        ms_r, ms_c = [], []
+    def time_kernels(plan, k, block):
+        """Per-kernel durations for the roofline: k more bench steps with events around each
+        launch (an event between the kernels adds a few us, so this pass is kept apart from
+        the timed region above), L2 flushed between bench steps."""
+        ms_r, ms_c = 0.0, 0.0
         barrier()
         for _ in range(k):
-            r, c = sim.plan.step_timed(1)
-            ms_r.append(r)
-            ms_c.append(c)
+            r, c = plan.step_timed(block)
+            ms_r += r
+            ms_c += c
             flush()
         barrier()
-        return ms_r, ms_c
+        return ms_r / (k * block), ms_c / (k * block)
+
+    def measure(sim, block, k, warmup):
+        for _ in range(max(warmup, 3)):
+            sim.plan.step(block)
+            flush()
+        ms, launches = time_blocks(sim.plan, k, block)
+        total_ms = max_over_ranks(sum(ms))
+        row_ms, col_ms = time_kernels(sim.plan, k, block)
+        return dict(total_ms=total_ms, launches=launches, row_ms=row_ms, col_ms=col_ms,
+                    ms_per_timestep=total_ms / (k * block))
 
     sites = NX * NY
-    results = {}
+    res = {}
+    sims = {}
     for precision in ("fp32", "fp64"):
-        sim = build(precision)
-        # warm-up through the timed path: records the one-step graph of each parity
-        for _ in range(max(args.warmup, 3)):
-            sim.plan.step(1)
-            flush()
-        sampler = ClockSampler(local) if precision == "fp32" else None
-        ms_step, launches, clocks = time_steps(sim, args.steps, sampler)
-        total_ms = max_over_ranks(sum(ms_step))
-        ms_r, ms_c = time_kernels(sim, args.steps)
-        results[precision] = dict(sim=sim, ms_r=ms_r, ms_c=ms_c, total_ms=total_ms, launches=launches,
-                                  clocks=clocks, value=world * sites * args.steps / (total_ms / 1e3))
-    # F agreement of the two forms after the same number of steps from the same field
-    F32 = results["fp32"]["sim"].Reduce()
-    F64 = results["fp64"]["sim"].Reduce()
-    dF = abs(F32[0] / F64[0] - 1)
-    mass_drift = abs(F32[2] - float(np.mean(f0)))
+        sims[precision] = build(precision)
+        res[precision] = measure(sims[precision], BLOCK, args.steps, args.warmup)
+        res[precision]["value"] = world * sites * BLOCK * args.steps / (res[precision]["total_ms"] / 1e3)
+    single = {}
+    for precision in ("fp32", "fp64"):
+        r = measure(sims[precision], 1, args.steps, args.warmup)
+        single[precision] = dict(value=world * sites * args.steps / (r["total_ms"] / 1e3),
+                                 us_per_step=1e3 * r["ms_per_timestep"], row_us=1e3 * r["row_ms"],
+                                 col_us=1e3 * r["col_ms"])
 
     # ---- end to end through the public API, host buffers pinned
-    sim = results["fp32"]["sim"]
+    sim = sims["fp32"]
     host_in = torch.from_numpy(f0).pin_memory()
-    e2e_frames = max(2, min(args.steps // 20, 10))
+    e2e_frames = max(2, min(args.steps // E2E_BLOCKS, 5))
     sim.State.n[...] = host_in
-    sim.TimeSteps(E2E_STEPS)
+    sim.TimeSteps(BLOCK * E2E_BLOCKS)
     sim.CalculateFreeEnergy()
     barrier()
     s = torch.cuda.current_stream(dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.mark(True)
     ev0.record(s)
     for _ in range(e2e_frames):
         sim.State.n[...] = host_in
-        for _ in range(E2E_STEPS):
+        for _ in range(BLOCK * E2E_BLOCKS):
             sim.TimeStep()
         sim.CalculateFreeEnergy()
     ev1.record(s)
     barrier()
+    clocks.mark(False)
     e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    e2e_value = world * sites * E2E_STEPS * e2e_frames / (e2e_ms / 1e3)
+    e2e_value = world * sites * BLOCK * E2E_BLOCKS * e2e_frames / (e2e_ms / 1e3)
+    for p in sims.values():
+        p.plan.close()
 
-    # ---- roofline of the dominant kernel (column pass: reads V and n_hat, writes n_hat' and W)
+    # ---- the HBM-bound case: 8192^2 solidification, same bench step
+    big = {}
+    if not args.no_8192:
+        kb = max(2, min(args.steps // 4, 5))
+        bic = None
+        for precision in ("fp32", "fp64"):
+            bsim, bic = workloads.build("solidify8192", precision, field=bic)
+            bsim.State.n[...] = bic
+            r = measure(bsim, BLOCK, kb, 3)
+            big[precision] = dict(value=world * 8192 * 8192 * BLOCK * kb / (r["total_ms"] / 1e3),
+                                  us_per_step=1e3 * r["ms_per_timestep"], row_us=1e3 * r["row_ms"],
+                                  col_us=1e3 * r["col_ms"], bench_steps=kb)
+            bsim.plan.close()
+            del bsim
+        del bic
+        torch.cuda.empty_cache()
+    clk = clocks.stop()
+
+    # ---- accuracy over the workload's full length (outside every timed region)
+    acc = None
+    if not args.no_accuracy:
+        err = workloads.lockstep_error("polycrystal2048", steps=ACCURACY_STEPS, every=1000)
+        acc = {"after_steps": ACCURACY_STEPS, "every": 1000,
+               "max_rel_F_fp32_vs_fp64": err["max_rel_F"], "max_abs_mu_fp32_vs_fp64": err["max_abs_mu"],
+               "max_psi_rel_l2_fp32_vs_fp64": err["max_psi_rel_l2"],
+               "max_deviation_rel_l2_fp32_vs_fp64": err["max_dev_rel_l2"],
+               "mass_drift_fp32": err["max_drift32"], "mass_drift_fp64": err["max_drift64"],
+               "F_final": {"fp32": err["records"]["F32"][-1], "fp64": err["records"]["F64"][-1]}}
+
+    # ---- roofline of the dominant kernel and of the whole step
     hbm, peak_kind = peaks()
-    r32 = results["fp32"]
-    col_ms = statistics.mean(r32["ms_c"])
-    row_ms = statistics.mean(r32["ms_r"])
+    r32 = res["fp32"]
     elt = 8  # complex64
     spec = (NX // 2) * NY * elt
     col_bytes, row_bytes = 4 * spec, 2 * spec
-    dominant = "column" if col_ms >= row_ms else "row"
-    dom_bytes, dom_ms = (col_bytes, col_ms) if dominant == "column" else (row_bytes, row_ms)
+    dominant = "column" if r32["col_ms"] >= r32["row_ms"] else "row"
+    dom_bytes, dom_ms = (col_bytes, r32["col_ms"]) if dominant == "column" else (row_bytes, r32["row_ms"])
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    # the whole step from the timed region (whole-step events), the kernels from their pass
-    step_achieved = (col_bytes + row_bytes) / ((r32["total_ms"] / args.steps) / 1e3) / 1e9
+    step_achieved = (col_bytes + row_bytes) / (r32["ms_per_timestep"] / 1e3) / 1e9
     traffic = None
     prof = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(prof):
@@ -336,38 +460,51 @@ def run_ours(args):
             traffic = None
 
     if rank == 0:
-        ms_per_step = r32["total_ms"] / args.steps
         line = {
             "metric": METRIC, "value": r32["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (FP64 mean, ETD coefficients and reductions)",
+            "warmup": args.warmup, "ms_per_step": r32["total_ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (FP64 mean, ETD coefficients and reductions)",
             "data": "synthetic (seeded polycrystal)",
             "config": workload_config({"parallelism": "replicas" if world > 1 else "single GPU"}),
             "gpu_launches": r32["launches"],
-            "fp64_plain": {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["total_ms"] / args.steps,
-                           "fp32_over_fp64": r32["value"] / results["fp64"]["value"]},
-            "accuracy": {"dF_over_F_fp32_vs_fp64": dF, "mass_drift_fp32": mass_drift,
-                         "after_steps": max(args.warmup, 3) + 2 * args.steps},
+            "us_per_time_step": 1e3 * r32["ms_per_timestep"],
+            "fp64_plain": {"value": res["fp64"]["value"], "us_per_time_step": 1e3 * res["fp64"]["ms_per_timestep"],
+                           "fp32_over_fp64": r32["value"] / res["fp64"]["value"]},
+            "single_step": {"note": "one ETD1 time step per bench step, L2 flushed between time steps",
+                            **{k: v for k, v in single.items()},
+                            "fp32_over_fp64": single["fp32"]["value"] / single["fp64"]["value"],
+                            "step_frac": 24 * sites / (single["fp32"]["us_per_step"] * 1e-6) / 1e9 / hbm},
             "roofline": {"bound": "hbm", "kernel": f"{dominant} pass (FP32)", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": dom_bytes,
                          "step": {"achieved": step_achieved, "frac": step_achieved / hbm,
                                   "bytes_per_site": (col_bytes + row_bytes) / sites,
-                                  "row_ms": row_ms, "col_ms": col_ms,
-                                  "kernel_timing": "separate pass of the same number of steps, CUDA events "
+                                  "row_us": 1e3 * r32["row_ms"], "col_us": 1e3 * r32["col_ms"],
+                                  "kernel_timing": "separate pass of the same bench steps, CUDA events "
                                                    "around each launch"}},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": sites * 8,
-                    "d2h_bytes_per_step": 24,
-                    "note": f"one e2e step = State.n[...] = pinned host field (FP64), {E2E_STEPS} "
-                            "TimeStep() calls, CalculateFreeEnergy() (F, mu, mean to the host)"},
-            "clocks": r32["clocks"],
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": sites * 8 // E2E_BLOCKS,
+                    "d2h_bytes_per_step": 24 // E2E_BLOCKS,
+                    "note": f"one e2e frame = {E2E_BLOCKS} bench steps: State.n[...] = pinned host field "
+                            f"(FP64, {sites * 8} B), {BLOCK * E2E_BLOCKS} TimeStep() calls, "
+                            "CalculateFreeEnergy() (F, mu, mean: 24 B to the host); bytes per bench step = "
+                            f"frame bytes / {E2E_BLOCKS}"},
+            "clocks": clk,
         }
+        if big:
+            b32 = big["fp32"]
+            line["solidify8192"] = {
+                "workload": "stdPFC 8192^2, dx=pi/4, dt=0.5, r=-0.25, mean -0.28, 256 seeds; 16-step bench steps, "
+                            "L2 flushed between them (the 1.6 GB working set exceeds L2)",
+                "fp32": b32, "fp64": big["fp64"], "fp32_over_fp64": b32["value"] / big["fp64"]["value"],
+                "step_achieved_gbs": 24 * 8192 * 8192 / (b32["us_per_step"] * 1e-6) / 1e9,
+                "step_frac": 24 * 8192 * 8192 / (b32["us_per_step"] * 1e-6) / 1e9 / hbm}
+        if acc:
+            line["accuracy"] = acc
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line))
-    for r in results.values():
-        r["sim"].plan.close()
     if distributed:
         dist.barrier()
         dist.destroy_process_group()
@@ -377,13 +514,24 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-8192", action="store_true", help="skip the 8192^2 HBM-bound key")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the 20000-step FP32 vs FP64 record")
+    kc = ap.add_argument_group("kernel case (short fixed workload for profiling)")
+    kc.add_argument("--kernel-case", action="store_true")
+    kc.add_argument("--nx", type=int, default=2048)
+    kc.add_argument("--ny", type=int, default=2048)
+    kc.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    kc.add_argument("--model", default="std", choices=["std", "log"])
+    kc.add_argument("--batch", type=int, default=0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.kernel_case:
+        return run_kernel_case(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -10,7 +10,8 @@ from pfc_models_b200 import workloads
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name,steps,every", [("solidify8192", 200, 50), ("logpfc1024", 1000, 250)])
+@pytest.mark.parametrize("name,steps,every", [("solidify8192", 200, 50), ("logpfc1024", 1000, 250),
+                                             ("polycrystal2048", 2000, 500)])
 def test_fp32_mixed_tracks_fp64_at_full_size(name, steps, every):
     r32 = workloads.run(name, "fp32", steps, every)
     r64 = workloads.run(name, "fp64", steps, every)
