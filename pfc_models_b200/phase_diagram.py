@@ -41,11 +41,11 @@ from __future__ import annotations
 
 import os
 import time
+import warnings
 from dataclasses import dataclass, replace
 
 import numpy as np
 
-from . import _lib
 from . import diagnostics as _diag
 from . import logpfc as _logpfc
 from . import stdpfc as _stdpfc
@@ -260,6 +260,12 @@ def _count_steps(sim, n):
     sim._relax_steps = getattr(sim, '_relax_steps', 0) + n
 
 
+# Times a lockstep group held plans at different ping-pong parities and stepped them one
+# by one instead of as one batch launch (the schedulers group by parity, so this stays 0
+# unless a step path bypasses _count_steps; the GPU tests assert it).
+LOCKSTEP_FALLBACKS = {"parity": 0}
+
+
 class _PlanLockstep:
     """Simulations stepped together through one `Batch`; F of all of them in one copy."""
 
@@ -268,15 +274,18 @@ class _PlanLockstep:
         self.batch = Batch(self.sims)
 
     def step(self, n):
-        try:
-            self.batch.step(n)
-        except _lib.PfcError as e:
-            # plans at different ping-pong parities: refused before any launch; the plans
-            # then step one by one (a batch step equals each plan's own steps)
-            if e.code != _lib.PFC_E_STATE:
-                raise
+        if len({getattr(s, '_relax_steps', 0) & 1 for s in self.sims}) > 1:
+            # plans at different ping-pong parities cannot share a launch: step them one by
+            # one (a batch step equals each plan's own steps), and say so
+            LOCKSTEP_FALLBACKS["parity"] += 1
+            warnings.warn("lockstep group at mixed ping-pong parities: stepping its plans one by one",
+                          RuntimeWarning, stacklevel=2)
             for sim in self.sims:
                 sim.TimeSteps(n)
+        else:
+            # any refusal here (a plan without a state, parities the host count missed) is a
+            # fault of the caller and raises
+            self.batch.step(n)
         for sim in self.sims:
             _count_steps(sim, n)
 

@@ -202,3 +202,26 @@ def test_auto_kernels_use_the_packaged_table():
             {k: int(table[key].get(k) or 0) for k in tune.VARIANT_KEYS}:
         assert (v["ee_row"], v["ee_col"]) == (table[key]["ee_row"], table[key]["ee_col"])
     assert v["fast"] == 1
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_nonfinite_member_is_flagged_alone(precision):
+    """A NaN seeded on the host into one member's field: after a batch run that member's
+    device status word reads PFC_STATUS_NONFINITE (set by the compensated reduction that
+    met it) while every other member's reads 0, and their fields equal the same plans
+    stepped alone bit for bit. The reference leaves such a NaN for its caller to find in
+    f (phase_diagram/q0star.py:277-281)."""
+    ref = [_std_sim(128, 128, -0.25, -0.2, precision, seed=i, graphs=False, pdl=False) for i in range(4)]
+    sims = [_std_sim(128, 128, -0.25, -0.2, precision, seed=i) for i in range(4)]
+    f = sims[2].State.n.get()
+    f[5, 7] = np.nan
+    sims[2].State.n[...] = f
+    b = Batch(sims)
+    b.step(37)
+    red = b.reduce()
+    assert [s.plan.status() for s in sims] == [0, 0, _lib.STATUS_NONFINITE, 0]
+    assert np.isnan(red[2, 0]) and np.all(np.isfinite(np.delete(red, 2, axis=0)))
+    for i in (0, 1, 3):
+        ref[i].TimeSteps(37)
+        assert np.array_equal(_field(sims[i]), _field(ref[i])), i
+    b.close()

@@ -592,3 +592,24 @@ def test_adaptive_dt_batch_equals_one_point_runs():
     assert ad.steps == total
     assert {g.stop for g in got} == {pd.STOP_CONVERGED, pd.STOP_NAN, pd.STOP_POOR_FIT}
     assert max(g.dt_max for g in got) > 0.1
+
+
+@pytest.mark.gpu
+def test_log_adaptive_dt_batch_on_b200_plans():
+    """Adaptive dt on B200 plans: the members ask for different step counts at different
+    ping-pong parities, plans rebuilt by a rollback or a dt change join the lockstep
+    mid-run, and plans of different dt share a batch launch. The batch returns each
+    point's one-point result bit for bit, and no lockstep group ever had to fall back to
+    stepping its plans one by one."""
+    relax = pd.RelaxSettings(dt=0.1, totalT=2e4, stepT=1e2, divs=10, maxDepth=4, requiredFitness=0.99,
+                             minimumA=1e-6, dtMax=0.4)
+    ad = pd.LogAdapter()
+    points = [(-0.9, 0.63, 0.9638831589013295), (-0.9, 0.63, 0.98), (-0.9, 0.88, 1.0)]
+    fallbacks = pd.LOCKSTEP_FALLBACKS["parity"]
+    got = pd.get_f_abc_batch(ad, LOG_PARAMS, 'triangle', CELL, ANSATZ, relax, points)
+    got += pd.get_f_abc_batch(ad, LOG_PARAMS, 'honeycomb', CELL, ANSATZ, relax, [(-0.9, 1.2, 1.0)])
+    assert pd.LOCKSTEP_FALLBACKS["parity"] == fallbacks
+    for g, (structure, p) in zip(got, [('triangle', p) for p in points] + [('honeycomb', (-0.9, 1.2, 1.0))]):
+        w = pd.get_f_abc(ad, LOG_PARAMS, structure, CELL, ANSATZ, relax, *p)
+        assert (g.values(), g.stop, g.steps, g.dt_max) == (w.values(), w.stop, w.steps, w.dt_max), (structure, p)
+    assert max(g.dt_max for g in got) > 0.1
