@@ -23,6 +23,7 @@ SPEC_N_HAT, SPEC_N_HAT_NOW = 0, 1
 FLAG_GENERIC_ONLY, FLAG_NO_GRAPHS, FLAG_PDL = 1, 2, 4
 FLAG_NO_ONE_CTA = 8
 PATH_MIXED_RADIX, PATH_POW2, PATH_ONE_CTA = 0, 1, 2
+STATUS_NONFINITE = 1
 
 
 def flag_variant(ee_row=0, ee_col=0, row_tile=0, col_cta=0, pdl=0):
