@@ -146,6 +146,11 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
                                      state towards L2) while the kernel before it drains */
 #define PFC_FLAG_NO_ONE_CTA 8     /* step small FP64 mixed-radix grids with the two-kernel
                                      step instead of the one-CTA whole-grid kernel */
+#define PFC_FLAG_PACKED 16        /* FP32-mixed power-of-two grids: the two-lane packed step
+                                     kernels (two rows / two columns per thread in packed
+                                     f32x2 arithmetic); PFC_FLAG_ROW_EE / COL_EE then give the
+                                     values per lane (8 or 16), PFC_FLAG_ROW_TILE the rows per
+                                     CTA (even) and PFC_FLAG_COL_CTA the column pairs per CTA */
 /* Variant of the power-of-two step kernels (0 in a field = the precision's default):
  * complex values per thread of the row and of the column kernel (FP32: 8, 16 or 32,
  * default 32; FP64: 8 or 16, default 16) and rows per CTA of the row kernel

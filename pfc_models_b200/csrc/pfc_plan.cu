@@ -167,7 +167,9 @@ struct pfc_plan {
   void* fast_row_fn = nullptr;
   void* fast_col_fn = nullptr;
   int fr_rows = 0, fr_threads = 0, fr_ld = 0, fr_grid = 0;
-  int ee_row = 0, ee_col = 0;  // elements per thread of the fast kernels
+  int ee_row = 0, ee_col = 0;  // elements per thread of the fast kernels (per lane when packed)
+  bool packed = false;         // two-lane packed FP32 step kernels (pfc_pack_step.cuh)
+  int rt4_off = 0;             // packed kernels: offset of the float4 real-packing table in tw
   int fc_threads = 0, fc_grid = 0;
   size_t fr_smem = 0, fc_smem = 0;
   int tw_ra = 0, tw_rb = 0, tw_ca = 0, tw_cb = 0;  // table offsets (complex elements)
@@ -331,11 +333,68 @@ bool fast_seq_tables(int lg, int ee, std::vector<long double>& tw, int& a, int& 
   return ee == 8 ? FastInst<double, 8>::tables(lg, tw, a, b) : FastInst<double, 16>::tables(lg, tw, a, b);
 }
 
+// The two-lane packed FP32 step kernels (PFC_FLAG_PACKED): row tiles of `rows` rows
+// (rows / 2 groups of one row pair), ngc column pairs per CTA; float4 pass tables.
+int setup_pack(pfc_plan* h, std::vector<long double>& tw) {
+  const int flags = h->prob.flags;
+  const int ee_r = PFC_FLAG_ROW_EE_OF(flags) ? PFC_FLAG_ROW_EE_OF(flags) : 16;
+  const int ee_c = PFC_FLAG_COL_EE_OF(flags) ? PFC_FLAG_COL_EE_OF(flags) : 16;
+  if ((ee_r != 8 && ee_r != 16) || (ee_c != 8 && ee_c != 16))
+    return fail(PFC_E_ARG, "pfc_plan_create: packed kernels take 8 or 16 values per lane (got %d, %d)", ee_r, ee_c);
+  const int tile = PFC_FLAG_ROW_TILE_OF(flags);
+  if (tile && (tile < 2 || tile > 16 || (tile & (tile - 1))))
+    return fail(PFC_E_ARG, "pfc_plan_create: packed row tile %d is not a power of two in [2, 16]", tile);
+  const int lm = ilog2_exact(h->m), ly = ilog2_exact(h->ny);
+  if ((flags & PFC_FLAG_GENERIC_ONLY) || lm < kPackMinLog || lm > kPackMaxLogRow || ly < kPackMinLog ||
+      ly > kPackMaxLogCol)
+    return PFC_OK;
+  FastKernel kr, kc;
+  if (!pack_row(lm, ee_r, h->prob.model, &kr) || !pack_col(ly, ee_c, &kc)) return PFC_OK;
+  const size_t slot = 16;   // one pc (two complex floats)
+  const size_t ld = (size_t)h->m + (h->m >> 4);
+  int rows = tile ? tile : 8;
+  // the kernels are built for max(256, threads per transform) threads per CTA; at most
+  // about half the shared memory of an SM per CTA
+  const int max_threads = std::max(256, kr.tpf);
+  while (rows > 2 && ((size_t)(rows / 2) * ld * slot > 110 * 1024 || (rows / 2) * kr.tpf > max_threads)) rows /= 2;
+  if (h->ny % rows || (rows / 2) * kr.tpf > max_threads || (size_t)(rows / 2) * ld * slot > 200 * 1024)
+    return PFC_OK;
+  const int col_cta = PFC_FLAG_COL_CTA_OF(flags), ngc_max = std::max(1, 256 / kc.tpf);
+  const int npairs = h->m / 2;
+  int ngc = std::min(col_cta ? std::min(col_cta, ngc_max) : ngc_max, npairs);
+  while (npairs % ngc) ngc /= 2;
+  const size_t padn = (size_t)h->ny + (h->ny >> 4) + 2;
+  const size_t fc_smem = (size_t)ngc * padn * slot;
+  const size_t fr_smem = (size_t)(rows / 2) * ld * slot;
+  if (ngc * kc.tpf > std::max(256, kc.tpf) || fc_smem > 200 * 1024) return PFC_OK;
+  h->fr_rows = rows;
+  h->fr_threads = (rows / 2) * kr.tpf;
+  h->fr_ld = (int)ld;
+  h->fr_grid = h->ny / rows;
+  h->fr_smem = fr_smem;
+  h->fc_threads = ngc * kc.tpf;
+  h->fc_grid = npairs / ngc;
+  h->fc_smem = fc_smem;
+  h->fast_row_fn = kr.fn;
+  h->fast_col_fn = kc.fn;
+  h->ee_row = ee_r;
+  h->ee_col = ee_c;
+  pack_tables(lm, ee_r, tw, h->tw_ra, h->tw_rb);
+  pack_tables(ly, ee_c, tw, h->tw_ca, h->tw_cb);
+  pack_real_table(h->nx, tw, h->rt4_off);
+  if (int rc = raise_smem_limit(h->fast_row_fn, h->fr_smem)) return rc;
+  if (int rc = raise_smem_limit(h->fast_col_fn, h->fc_smem)) return rc;
+  h->fast = true;
+  h->packed = true;
+  return PFC_OK;
+}
+
 // Chooses the fast kernels and their launch shapes; appends their twiddle tables to tw.
 // problem.flags may pick the elements per thread of each kernel and the row tile.
 template <class T>
 int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
   const int flags = h->prob.flags;
+  if (sizeof(T) == 4 && (flags & PFC_FLAG_PACKED)) return setup_pack(h, tw);
   const int ee_r = PFC_FLAG_ROW_EE_OF(flags) ? PFC_FLAG_ROW_EE_OF(flags) : fast_ee_default<T>();
   const int ee_c = PFC_FLAG_COL_EE_OF(flags) ? PFC_FLAG_COL_EE_OF(flags) : fast_ee_default<T>();
   const int tile = PFC_FLAG_ROW_TILE_OF(flags);
@@ -429,7 +488,7 @@ int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
     a.in = reinterpret_cast<const cplx<T>*>(h->W);
     a.out = reinterpret_cast<cplx<T>*>(h->V);
     const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(h->tw);
-    a.twA = tw + h->tw_ra; a.twB = tw + h->tw_rb; a.rtw = tw + h->rt_off;
+    a.twA = tw + h->tw_ra; a.twB = tw + h->tw_rb; a.rtw = tw + (h->packed ? h->rt4_off : h->rt_off);
     a.scal = h->scal;
     a.clamp = h->prob.clamp_log;
     a.g = h->prob.g; a.min_phi = h->prob.min_phi;
@@ -1229,7 +1288,7 @@ int pfc_plan_variant(pfc_plan* h, int32_t* o) {
   o[0] = h->fast ? h->ee_row : 0;
   o[1] = h->fast ? h->ee_col : 0;
   o[2] = h->fast ? h->fr_rows : 0;
-  o[3] = h->fast ? 1 : 0;
+  o[3] = h->packed ? 2 : h->fast ? 1 : 0;
   return PFC_OK;
 }
 
@@ -1261,7 +1320,8 @@ int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out) {
       // (mixed-radix plans of one size and precision share the FFT description, twiddle
       // tables and launch shape, all of which come from plans[0] of the class)
       if (r->fast == h->fast && r->onecta == h->onecta && r->fast_row_fn == h->fast_row_fn &&
-          r->fast_col_fn == h->fast_col_fn &&
+          r->fast_col_fn == h->fast_col_fn && r->packed == h->packed && r->fr_rows == h->fr_rows &&
+          r->fc_threads == h->fc_threads &&
           r->row_rset == h->row_rset && r->col_rset == h->col_rset && r->prob.model == h->prob.model &&
           r->nx == h->nx && r->ny == h->ny && r->prob.g == h->prob.g && r->prob.clamp_log == h->prob.clamp_log &&
           r->prob.min_phi == h->prob.min_phi) {

@@ -40,6 +40,17 @@ struct FastInst {
   static bool tables(int lg, std::vector<long double>& tw, int& offA, int& offB);
 };
 
+// Two-lane packed FP32 step kernels (pfc_pack_step.cuh), `ee` = 8 or 16 complex values
+// per lane and thread: row transforms of 2^lg points (M = nx/2), column transforms of
+// 2^lg points (ny). Their pass tables are float4 entries (c, c, s, s), appended to `tw`
+// as two complex slots each, at even (16-byte aligned) offsets; pack_real_table appends
+// the real-packing table exp(-2 pi i k / nx), k < nx/2, in the same form.
+constexpr int kPackMinLog = 6, kPackMaxLogRow = 12, kPackMaxLogCol = 13;
+bool pack_row(int lg, int ee, int model, FastKernel* out);
+bool pack_col(int lg, int ee, FastKernel* out);
+bool pack_tables(int lg, int ee, std::vector<long double>& tw, int& offA, int& offB);
+void pack_real_table(int nx, std::vector<long double>& tw, int& off);
+
 // Mixed-radix kernels (pfc_kernels.cuh), by mode (kRow* / kCol*) and radix set.
 template <class T>
 struct GenericInst {

@@ -363,10 +363,11 @@ def _kernel_flags(kernels, prob):
     """problem.flags bits for the `kernels` choice of a Simulation: "auto" (the variant
     the autotuner cached for this grid, else the defaults), "default", "generic" (the
     mixed-radix kernels everywhere), or a dict with any of "ee_row", "ee_col",
-    "row_tile", "col_cta" (columns per CTA of the column kernel) and "pdl"."""
+    "row_tile", "col_cta" (columns per CTA of the column kernel), "pdl" and "packed"
+    (the two-lane packed FP32 kernels; then ee_* count values per lane)."""
     if isinstance(kernels, dict):
         return _lib.flag_variant(**{k: kernels.get(k, 0) for k in ("ee_row", "ee_col", "row_tile", "col_cta",
-                                                                    "pdl")})
+                                                                    "pdl", "packed")})
     if kernels == "generic":
         return _lib.FLAG_GENERIC_ONLY
     if kernels == "default":
