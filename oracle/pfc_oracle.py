@@ -200,6 +200,77 @@ def run(model, params: Params, geom: Geometry, field0, steps, record_every=None)
     return sim.n, rec
 
 
+# ---------------------------------------------------------------- log PFC with an external potential
+class OracleExtv:
+    """The reference's logpfc_extv stepper (models/logpfc_extv/simulation.py), restated.
+
+    Per TimeStep (:301-330): ValidatePhiRange (:375-405) re-optimises the shift M when the
+    field's range leaves the last optimised range by more than 10 % (relative, floor and
+    ceiling); OptimizeM (:332-373) sets M = (N(max) - N(min)) / (max - min) with
+    N(x) = g x^2 + x^3 + ln x (min replaced by minPhi when the field's minimum is <= 0) and
+    rebuilds the linear mu kernel beta (q0^2 + lap)^2 + eps + M and the ETD1 coefficients
+    (kernel_etd, smallZTol 1e-8 by default, :69-117); the nonlinearity is the clamped log
+    where(phi > minPhi, ln phi, ln minPhi) + g phi^2 + phi^3 - M phi (:524-539); the update
+    phi_next_hat = A phi_hat + B (Gamma lap N_hat + lap V_hat), with the k = 0 mode kept
+    (:557-577). F is the logPFC free energy (:427-451). V is a real field (the reference's
+    _ExternalPotential.V, zero unless set)."""
+
+    def __init__(self, params: Params, geom: Geometry, min_phi=1e-6, V=None):
+        self.p, self.geom = params, geom
+        self.min_phi, self.min_log = min_phi, np.log(min_phi)
+        self.lap = laplacian(geom)
+        self.M = 0.0
+        self.phi_min = self.phi_max = None
+        self.floor_tol = self.ceiling_tol = 0.1
+        self.optimizations = 0
+        self.n = np.zeros((geom.Ny, geom.Nx))
+        self.V_hat = np.fft.rfft2(np.zeros((geom.Ny, geom.Nx)) if V is None else np.asarray(V, dtype=np.float64))
+        self._coefficients(0.0)
+
+    def _coefficients(self, M):
+        p = self.p
+        kl = p.Gamma * self.lap * (p.beta * (p.q0**2 + self.lap) ** 2 + p.epsilon + M)
+        self.A, self.B = etd1(kl, p.dt, p.smallZTol)
+
+    def set_field(self, phi):
+        self.n = np.array(phi, dtype=np.float64, copy=True)
+
+    def optimize_m(self):
+        g = self.p.g
+        lo = float(np.min(self.n)) if self.n.min() > 0 else self.min_phi
+        hi = float(np.max(self.n))
+        nmu = lambda x: g * x**2 + x**3 + np.log(x)  # noqa: E731
+        self.M = (nmu(hi) - nmu(lo)) / (hi - lo)
+        self._coefficients(self.M)
+        self.phi_min, self.phi_max = lo, hi
+        self.optimizations += 1
+
+    def validate_phi_range(self):
+        lo, hi = float(self.n.min()), float(self.n.max())
+        if self.phi_min is None or self.phi_max is None:
+            self.optimize_m()
+            return
+        if (self.phi_min - lo) / self.phi_min > self.floor_tol or (hi - self.phi_max) / self.phi_max > self.ceiling_tol:
+            self.optimize_m()
+
+    def step(self):
+        self.validate_phi_range()
+        p, phi = self.p, self.n
+        with np.errstate(divide="ignore", invalid="ignore"):
+            N = np.where(phi > self.min_phi, np.log(phi), self.min_log) + p.g * phi**2 + phi**3 - self.M * phi
+        phi_hat = np.fft.rfft2(phi)
+        nxt = self.A * phi_hat + self.B * (p.Gamma * self.lap * np.fft.rfft2(N) + self.lap * self.V_hat)
+        nxt.flat[0] = phi_hat.flat[0]
+        self.n = np.fft.irfft2(nxt, s=phi.shape)
+
+    def free_energy(self):
+        p, phi = self.p, self.n
+        lin_f = np.fft.irfft2((p.beta / 2.0) * (p.q0**2 + self.lap) ** 2 * np.fft.rfft2(phi), s=phi.shape)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            nonlin_f = phi * np.log(phi) + (p.epsilon / 2.0) * phi**2 + (p.g / 3.0) * phi**3 + phi**4 / 4.0
+        return float((phi * lin_f + nonlin_f).mean())
+
+
 # ---------------------------------------------------------------- vacancy tracking
 def _np_index(i: int, n: int) -> int:
     """An integer index on an axis of length n as NumPy reads it: negative counts from

@@ -121,3 +121,35 @@ def test_substrate(golden):
     np.testing.assert_array_equal(B, d["B"])
     assert B.flat[0] == c["dt"]
     np.testing.assert_array_equal(orc.gaussian(geom, 2 * np.pi), d["gauss"])
+
+
+@pytest.mark.parametrize("case", ["smoke", "dipole", "tanh"])
+def test_extv_oracle_reproduces_the_reference(golden, case):
+    """The logpfc_extv restatement against the reference model run unmodified
+    (tests/golden/make_extv_golden.py): the M it chose for every step, the field's range
+    it saw, F and the mean at the recorded steps, and the fields."""
+    d = golden("extv")
+    g = lambda k: d[f"{case}/{k}"]  # noqa: E731
+    nx, ny, lx, ly, dt, steps = g("config")
+    nx, ny, steps = int(nx), int(ny), int(steps)
+    geom = orc.build_geometry(nx, ny, lx, ly)
+    prm = orc.Params(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=dt, smallZTol=1e-8)
+    sim = orc.OracleExtv(prm, geom, V=g("V"))
+    sim.set_field(g("phi0"))
+    F_steps = list(g("F_step"))
+    rec = list(g("record"))
+    M = []
+    for s in range(1, steps + 1):
+        assert sim.n.min() == pytest.approx(g("phi_min")[s - 1], rel=1e-12)
+        assert sim.n.max() == pytest.approx(g("phi_max")[s - 1], rel=1e-12)
+        sim.step()
+        M.append(sim.M)
+        if s in F_steps:
+            i = F_steps.index(s)
+            assert sim.free_energy() == pytest.approx(g("F")[i], rel=1e-12), s
+            assert float(sim.n.mean()) == pytest.approx(g("mean")[i], abs=1e-13), s
+        if s in rec:
+            f = g("fields")[rec.index(s)]
+            assert np.linalg.norm(sim.n - f) / np.linalg.norm(f) < 1e-12, s
+    np.testing.assert_allclose(M, g("M"), rtol=1e-12)
+    assert sim.optimizations >= 2
