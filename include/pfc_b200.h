@@ -146,6 +146,11 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
                                      state towards L2) while the kernel before it drains */
 #define PFC_FLAG_NO_ONE_CTA 8     /* step small FP64 mixed-radix grids with the two-kernel
                                      step instead of the one-CTA whole-grid kernel */
+#define PFC_FLAG_EXTV 32          /* log PFC with an external potential and the re-optimised
+                                     linear shift M (models/logpfc_extv/simulation.py): needs
+                                     FP64 plain, the log model and clamp_log = 1 with
+                                     min_phi > 0; steps with the mixed-radix two-kernel step
+                                     plus two small kernels, alone (not in a batch) */
 #define PFC_FLAG_PACKED 16        /* FP32-mixed power-of-two grids: the two-lane packed step
                                      kernels (two rows / two columns per thread in packed
                                      f32x2 arithmetic); PFC_FLAG_ROW_EE / COL_EE then give the
@@ -287,6 +292,31 @@ int pfc_locate_vacancies(const double* dev_field, int32_t nx, int32_t ny, double
 int pfc_last_error(char* buf, size_t len);
 
 int pfc_abi_version(void);
+
+/* ---- log PFC with an external potential (plans created with PFC_FLAG_EXTV) ----
+ * The reference's logpfc_extv model (models/logpfc_extv/simulation.py) on the log stepper:
+ * every pfc_step step does what its TimeStep (:301-330) does. ValidatePhiRange (:375-405)
+ * reads the field's range and, on the first step or when the range leaves the last
+ * optimised one by more than the floor / ceiling tolerances (relative, 0.1 by default),
+ * OptimizeM (:332-373) sets M = (N(max) - N(min)) / (max - min), N(x) = g x^2 + x^3 + ln x,
+ * and rebuilds the ETD1 coefficients of beta (q0^2 + lap)^2 + eps + M; the update is
+ * phi_hat' = A_M phi_hat + B_M (Gamma lap (N_hat - M phi_hat) + lap V_hat) with the clamped
+ * log (:524-577). The decision, M and the rebuild run on the device, stream-ordered. */
+
+/* Replaces _ExternalPotential.SetPotential / SetGaussianDipolePotential /
+ * SetPotential_alongX / SetDoubleVacancyAlongX_TanhPotential (models/logpfc_extv/
+ * external_potentials.py:109-131): V as a real FP64 (ny, nx) device field; its rfft2 is
+ * taken on the device and the next step rebuilds the forcing B lap V_hat. */
+int pfc_set_potential(pfc_plan* plan, const double* dev_v, void* stream);
+
+/* Reads the M-shift state (State.M, State.phi_min, State.phi_max of
+ * models/logpfc_extv/simulation.py:130-144) after synchronising: out6 = {M, phi_min,
+ * phi_max of the last optimisation (NaN before the first step), the field's min and max
+ * seen by the last step, number of optimisations}. */
+int pfc_extv_state(pfc_plan* plan, double* host_out6);
+
+/* Sets State.phi_floor_tol / State.phi_ceiling_tol (models/logpfc_extv/simulation.py:143-144). */
+int pfc_extv_set_tolerances(pfc_plan* plan, double floor_tol, double ceiling_tol);
 
 #ifdef __cplusplus
 }

@@ -23,6 +23,7 @@ SPEC_N_HAT, SPEC_N_HAT_NOW = 0, 1
 FLAG_GENERIC_ONLY, FLAG_NO_GRAPHS, FLAG_PDL = 1, 2, 4
 FLAG_NO_ONE_CTA = 8
 FLAG_PACKED = 16
+FLAG_EXTV = 32
 PATH_MIXED_RADIX, PATH_POW2, PATH_ONE_CTA = 0, 1, 2
 STATUS_NONFINITE = 1
 
@@ -63,6 +64,9 @@ SIGNATURES = {
     "pfc_diagnose_modes": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _dbl, _vp, _vp]),
     "pfc_frozen_moments": (ctypes.c_int, [_vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _dbl, _vp, _vp]),
     "pfc_defect_screen": (ctypes.c_int, [_vp, _vp, _vp, _dbl, _dbl, _vp, _vp]),
+    "pfc_set_potential": (ctypes.c_int, [_vp, _vp, _vp]),
+    "pfc_extv_state": (ctypes.c_int, [_vp, ctypes.POINTER(_dbl)]),
+    "pfc_extv_set_tolerances": (ctypes.c_int, [_vp, _dbl, _dbl]),
 }
 
 

@@ -92,6 +92,32 @@ __device__ void block_reduce_store(KSum* v, double* out) {
   }
 }
 
+// Block minimum and maximum; thread 0 writes (min, max) to out[0..1]. Every thread of the
+// block calls it.
+__device__ inline void block_minmax_store(double lo, double hi, double* out) {
+  __shared__ double rmin[32], rmax[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    lo = fmin(lo, __shfl_down_sync(0xffffffffu, lo, off));
+    hi = fmax(hi, __shfl_down_sync(0xffffffffu, hi, off));
+  }
+  if (lane == 0) {
+    rmin[warp] = lo;
+    rmax[warp] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int w = 1; w < nw; ++w) {
+      lo = fmin(lo, rmin[w]);
+      hi = fmax(hi, rmax[w]);
+    }
+    out[0] = lo;
+    out[1] = hi;
+  }
+}
+
 // ---------------------------------------------------------------- nonlinearity
 // Plain FP64 form: the reference's expressions
 // (models/stdpfc/simulation.py:297, models/logpfc/simulation.py:296).
@@ -151,6 +177,7 @@ struct RowArgs {
   const double* scal;       // device scalar block
   const double* add;        // materialise: constant added (device pointer), may be null
   double* partials;         // per-CTA compensated sums
+  double* minmax;           // step mode, FP64 form: per-CTA (min, max) of the field, or null
   int clamp;
   double g, min_phi, min_log, epsilon;
   const BatchBufs* batch;   // step mode of a batch: per-plan W, V and scalars at [blockIdx.y]
@@ -178,6 +205,7 @@ struct ColArgs {
   cplx<T>* wout;                // W' (step/init/combine)
   const cplx<T>* coef;          // (A - 1, Bg) [kx][ky], kx <= m, ky <= ny/2, working precision
   const cplx<double>* coef64;   // FP32 form: the same in FP64, read for the slow modes
+  const cplx<double>* forcing;  // step mode, FP64 form: added to n_hat', [kx][ky] (kx <= m), or null
   float slow_tau;
   double* partials;
   double* out_c128;             // export: (ny, m+1) complex128
@@ -322,11 +350,17 @@ __global__ void __launch_bounds__(LB, MINB) row_kernel(RowArgs<T> a) {
                     (T)nonlin_dev<MODEL>((float)z.y, c1, c2, inv, inv_d, a.clamp, mphi_rel, lmin));
       }
     } else {
+      double lo = INFINITY, hi = -INFINITY;
       for (int j = lt; j < m; j += tpf) {
         const cplx<T> z = buf[j];
+        if (valid) {
+          lo = fmin(lo, fmin((double)z.x, (double)z.y));
+          hi = fmax(hi, fmax((double)z.x, (double)z.y));
+        }
         buf[j] = mk((T)nonlin_plain<MODEL>((double)z.x, a.g, a.clamp, a.min_phi, a.min_log),
                     (T)nonlin_plain<MODEL>((double)z.y, a.g, a.clamp, a.min_phi, a.min_log));
       }
+      if (a.minmax) block_minmax_store(lo, hi, a.minmax + 2 * blockIdx.x);
     }
     __syncthreads();
   }
@@ -520,8 +554,12 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
         cplx<double> h0, hm, g0, gm;
         unpack_pair(pk, pkp, h0, hm);
         unpack_pair(qk, qkp, g0, gm);
-        const cplx<double> h0n = h0 + c0v.x * h0 + c0v.y * g0;
-        const cplx<double> hmn = hm + cMv.x * hm + cMv.y * gm;
+        cplx<double> h0n = h0 + c0v.x * h0 + c0v.y * g0;
+        cplx<double> hmn = hm + cMv.x * hm + cMv.y * gm;
+        if (a.forcing) {
+          h0n = h0n + a.forcing[ky];
+          hmn = hmn + a.forcing[(size_t)m * ny + ky];
+        }
         const cplx<double> ok = h0n + mul_i(hmn);
         const cplx<double> okp = conj(h0n) + mul_i(conj(hmn));
         state_st<T>(a_nout, a_nout_lo, cb + ky, ok, true);
@@ -568,8 +606,12 @@ __global__ void __launch_bounds__(LB, MINB) col_kernel(ColArgs<T> a) {
             pkp.x += (double)lp.x;
             pkp.y += (double)lp.y;
           }
-          const cplx<double> ok = pk + c.x * pk + c.y * qk;
-          const cplx<double> okp = pkp + c.x * pkp + c.y * qkp;
+          cplx<double> ok = pk + c.x * pk + c.y * qk;
+          cplx<double> okp = pkp + c.x * pkp + c.y * qkp;
+          if (a.forcing) {
+            ok = ok + a.forcing[cb + ky];
+            okp = okp + a.forcing[cb + kyp];
+          }
           state_st<T>(a_nout, a_nout_lo, cb + ky, ok, slow);
           buf[ky] = mk((T)ok.x, (T)ok.y);
           if (kyp != ky) {

@@ -169,6 +169,13 @@ struct pfc_plan {
   int fr_rows = 0, fr_threads = 0, fr_ld = 0, fr_grid = 0;
   int ee_row = 0, ee_col = 0;  // elements per thread of the fast kernels (per lane when packed)
   bool packed = false;         // two-lane packed FP32 step kernels (pfc_pack_step.cuh)
+  // log PFC with an external potential (PFC_FLAG_EXTV, pfc_extv.cu)
+  bool extv = false;
+  pfc::ExtvState* extv_st = nullptr;   // device
+  double* extv_minmax = nullptr;       // per row-CTA (min, max) of the field
+  double2* vhat = nullptr;             // rfft2 of V, (ny, m + 1)
+  double2* forcing = nullptr;          // B lap V_hat, [kx][ky]
+  void* scratch_state = nullptr;       // a spectral state for transforming V
   int rt4_off = 0;             // packed kernels: offset of the float4 real-packing table in tw
   int fc_threads = 0, fc_grid = 0;
   size_t fr_smem = 0, fc_smem = 0;
@@ -479,6 +486,24 @@ inline cudaError_t launch_step_kernel(const pfc_plan* h, const void* fn, dim3 gr
   return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
+ExtvCoefArgs extv_coef_args(const pfc_plan* h) {
+  ExtvCoefArgs a{};
+  a.nx = h->nx; a.ny = h->ny; a.m = h->m; a.nyh = h->nyh;
+  const double dx = h->prob.lx / h->nx, dy = h->prob.ly / h->ny;
+  a.fx = 1.0 / (h->nx * dx);
+  a.fy = 1.0 / (h->ny * dy);
+  a.gamma = h->prob.gamma; a.beta = h->prob.beta; a.q0 = h->prob.q0; a.epsilon = h->prob.epsilon;
+  a.dt = h->prob.dt; a.small_z_tol = h->prob.small_z_tol;
+  a.coef = static_cast<double2*>(h->coef);
+  a.vhat = h->vhat;
+  a.forcing = h->forcing;
+  return a;
+}
+
+// launches of one step of this plan (row and column kernels, plus the external-potential
+// decision and coefficient kernels)
+int launches_per_step(const pfc_plan* h) { return h->extv ? 4 : 2; }
+
 template <class T>
 int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullptr, int count = 1) {
   if (h->fast) {
@@ -504,7 +529,17 @@ int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
   ra.in = reinterpret_cast<const cplx<T>*>(h->W);
   ra.out = reinterpret_cast<cplx<T>*>(h->V);
   ra.batch = table;
-  return launch_row<T, kRowStep>(h, ra, s, count);
+  if (!h->extv) return launch_row<T, kRowStep>(h, ra, s, count);
+  // external potential: the field's range, the M decision and (when M or V changed) the
+  // coefficients and the forcing, before the column pass
+  ra.minmax = h->extv_minmax;
+  int rc = launch_row<T, kRowStep>(h, ra, s, count);
+  if (rc) return rc;
+  cudaError_t e = launch_extv_decide(h->extv_minmax, h->row_grid, h->extv_st, h->prob.g, s);
+  if (e == cudaSuccess) e = launch_extv_coef(extv_coef_args(h), h->extv_st, s);
+  h->launches += 2;
+  if (e != cudaSuccess) return fail(PFC_E_CUDA, "external-potential step launch failed: %s", cudaGetErrorString(e));
+  return PFC_OK;
 }
 
 // One column pass of a step: V, n_hat[cur] -> n_hat[cur ^ 1], W (batched as above).
@@ -541,6 +576,7 @@ int launch_step_col(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
   ca.nin_lo = static_cast<const cplx<float>*>(h->nhat_lo[h->cur]);
   ca.nout_lo = static_cast<cplx<float>*>(h->nhat_lo[h->cur ^ 1]);
   ca.batch = table;
+  if (h->extv) ca.forcing = reinterpret_cast<const cplx<double>*>(h->forcing);
   return launch_col<T, kColStep>(h, ca, s, count);
 }
 
@@ -714,7 +750,7 @@ int replay_steps(pfc_plan* h, cudaGraphExec_t* slot, int len, long long count, c
     cudaError_t e = cudaGraphLaunch(slot[p], s);
     if (e != cudaSuccess) return fail(PFC_E_CUDA, "cudaGraphLaunch failed: %s", cudaGetErrorString(e));
   }
-  h->launches += 2LL * len * count;
+  h->launches += (long long)launches_per_step(h) * len * count;
   h->steps_since_set += (long long)len * count;
   if ((len * count) & 1) h->cur ^= 1;
   return PFC_OK;
@@ -990,8 +1026,15 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   if (!factorize(p->ny, fp32, rcol))
     return fail(PFC_E_ARG, "pfc_plan_create: ny = %d has a prime factor other than 2,3,5,7,11,13", p->ny);
 
+  if ((p->flags & PFC_FLAG_EXTV) && (fp32 || p->model != PFC_MODEL_LOG || !p->clamp_log || !(p->min_phi > 0)))
+    return fail(PFC_E_ARG, "pfc_plan_create: PFC_FLAG_EXTV needs the FP64 plain log model with the clamped log "
+                "(clamp_log = 1, min_phi > 0)");
+
   pfc_plan* h = new pfc_plan();
   h->prob = *p;
+  // the external-potential step runs on the mixed-radix kernels and the two-kernel step
+  if (p->flags & PFC_FLAG_EXTV) h->prob.flags |= PFC_FLAG_GENERIC_ONLY | PFC_FLAG_NO_ONE_CTA;
+  h->extv = (p->flags & PFC_FLAG_EXTV) != 0;
   h->fp32 = (p->precision == PFC_FP32_MIXED);
   h->nx = p->nx; h->ny = p->ny; h->m = m; h->nyh = p->ny / 2 + 1;
   h->nspec = (size_t)m * p->ny;
@@ -1136,6 +1179,22 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   if (e == cudaSuccess) e = cudaMalloc(&h->partials, h->npartials * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&h->scal, kScalCount * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&h->status, sizeof(int));
+  if (h->extv) {
+    if (e == cudaSuccess) e = cudaMalloc(&h->extv_st, sizeof(ExtvState));
+    if (e == cudaSuccess) e = cudaMalloc(&h->extv_minmax, 2 * (size_t)h->row_grid * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&h->vhat, (size_t)p->ny * (m + 1) * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&h->forcing, (size_t)(m + 1) * p->ny * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMemset(h->vhat, 0, (size_t)p->ny * (m + 1) * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMemset(h->forcing, 0, (size_t)(m + 1) * p->ny * sizeof(double2));
+    if (e == cudaSuccess) {
+      // ValidatePhiRange's state as the reference builds it (logpfc_extv/simulation.py:130-144)
+      ExtvState st{};
+      st.floor_tol = 0.1;
+      st.ceil_tol = 0.1;
+      st.min_phi = p->min_phi;
+      e = cudaMemcpy(h->extv_st, &st, sizeof(st), cudaMemcpyHostToDevice);
+    }
+  }
   if (e != cudaSuccess)
     return cleanup_fail(fail(e == cudaErrorMemoryAllocation ? PFC_E_NOMEM : PFC_E_CUDA,
                              "pfc_plan_create: cudaMalloc failed: %s", cudaGetErrorString(e)));
@@ -1187,6 +1246,8 @@ int pfc_plan_destroy(pfc_plan* h) {
   for (void* p : {h->nhat[0], h->nhat[1], h->nhat_lo[0], h->nhat_lo[1], h->W, h->V, h->W2, h->coef, h->coef64, h->tw})
     if (p) cudaFree(p);
   if (h->partials) cudaFree(h->partials);
+  for (void* q : {(void*)h->extv_st, (void*)h->extv_minmax, (void*)h->vhat, (void*)h->forcing, h->scratch_state})
+    if (q) cudaFree(q);
   if (h->scal) cudaFree(h->scal);
   if (h->status) cudaFree(h->status);
   for (auto* t : h->oc_table)
@@ -1305,6 +1366,7 @@ int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out) {
     if (!plans[i]) return fail(PFC_E_ARG, "pfc_batch_create: null plan %d", i);
     if (plans[i]->fp32 != plans[0]->fp32) return fail(PFC_E_ARG, "pfc_batch_create: plans mix precisions");
     if (plans[i]->device != plans[0]->device) return fail(PFC_E_ARG, "pfc_batch_create: plans on different devices");
+    if (plans[i]->extv) return fail(PFC_E_ARG, "pfc_batch_create: plans with an external potential step alone");
     for (int j = 0; j < i; ++j)
       if (plans[j] == plans[i]) return fail(PFC_E_ARG, "pfc_batch_create: plan %d appears twice", i);
   }
@@ -1583,5 +1645,62 @@ extern "C" int pfc_defect_screen(pfc_plan* h, const double* dev_field, const dou
   cudaError_t e = launch_defect_screen(dev_field, dev_spectrum, h->nx, h->ny, fx, fy, h->partials, dev_out4,
                                        static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return fail(PFC_E_CUDA, "pfc_defect_screen: launch failed: %s", cudaGetErrorString(e));
+  return PFC_OK;
+}
+
+// ---- log PFC with an external potential
+extern "C" int pfc_set_potential(pfc_plan* h, const double* dev_v, void* stream) {
+  if (!h || !dev_v) return fail(PFC_E_ARG, "pfc_set_potential: null argument");
+  if (!h->extv) return fail(PFC_E_ARG, "pfc_set_potential: the plan was not created with PFC_FLAG_EXTV");
+  if (reinterpret_cast<uintptr_t>(dev_v) % 16) return fail(PFC_E_ARG, "pfc_set_potential: V must be 16-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!h->W2) PFC_CUDA(cudaMalloc(&h->W2, h->nspec * h->elt));
+  if (!h->scratch_state) PFC_CUDA(cudaMalloc(&h->scratch_state, h->nspec * sizeof(double2)));
+  // rfft2 of V through the plan's own forward transform: row pass into W2, column pass
+  // into the scratch state, exported unpacked as (ny, m + 1)
+  RowArgs<double> ra = row_args<double>(h);
+  ra.in_real = dev_v;
+  ra.out = reinterpret_cast<cplx<double>*>(h->W2);
+  int rc = launch_row<double, kRowForward>(h, ra, s);
+  if (rc) return rc;
+  ColArgs<double> ca = col_args<double>(h);
+  ca.in = reinterpret_cast<const cplx<double>*>(h->W2);
+  ca.nout = h->scratch_state;
+  ca.wout = reinterpret_cast<cplx<double>*>(h->W2);
+  rc = launch_col<double, kColInit>(h, ca, s);
+  if (rc) return rc;
+  ColArgs<double> ce = col_args<double>(h);
+  ce.sin = h->scratch_state;
+  ce.out_c128 = reinterpret_cast<double*>(h->vhat);
+  rc = launch_col<double, kColExport>(h, ce, s);
+  if (rc) return rc;
+  // the next step rebuilds the forcing B lap V_hat
+  PFC_CUDA(cudaMemsetAsync(&h->extv_st->v_dirty, 0xff, sizeof(int), s));
+  return PFC_OK;
+}
+
+extern "C" int pfc_extv_state(pfc_plan* h, double* out6) {
+  if (!h || !out6) return fail(PFC_E_ARG, "pfc_extv_state: null argument");
+  if (!h->extv) return fail(PFC_E_ARG, "pfc_extv_state: the plan was not created with PFC_FLAG_EXTV");
+  ExtvState st{};
+  PFC_CUDA(cudaMemcpy(&st, h->extv_st, sizeof(st), cudaMemcpyDeviceToHost));
+  out6[0] = st.M;
+  out6[1] = st.init ? st.phi_min : NAN;
+  out6[2] = st.init ? st.phi_max : NAN;
+  out6[3] = st.last_min;
+  out6[4] = st.last_max;
+  out6[5] = (double)st.count;
+  return PFC_OK;
+}
+
+extern "C" int pfc_extv_set_tolerances(pfc_plan* h, double floor_tol, double ceiling_tol) {
+  if (!h) return fail(PFC_E_ARG, "pfc_extv_set_tolerances: null plan");
+  if (!h->extv) return fail(PFC_E_ARG, "pfc_extv_set_tolerances: the plan was not created with PFC_FLAG_EXTV");
+  if (!(floor_tol >= 0) || !(ceiling_tol >= 0)) return fail(PFC_E_ARG, "pfc_extv_set_tolerances: negative tolerance");
+  ExtvState st{};
+  PFC_CUDA(cudaMemcpy(&st, h->extv_st, sizeof(st), cudaMemcpyDeviceToHost));
+  st.floor_tol = floor_tol;
+  st.ceil_tol = ceiling_tol;
+  PFC_CUDA(cudaMemcpy(h->extv_st, &st, sizeof(st), cudaMemcpyHostToDevice));
   return PFC_OK;
 }

@@ -95,6 +95,26 @@ cudaError_t launch_onecta_step(const RowArgs<double>& ra, const ColArgs<double>&
                                int count, long long nsteps, int model, int rset, bool dense, int threads,
                                size_t smem, cudaStream_t stream);
 
+// Log PFC with an external potential (pfc_extv.cu): the state of the M shift, kept in
+// device memory, and the arguments of the coefficient rebuild.
+struct ExtvState {
+  double M, phi_min, phi_max;   // shift and the range it was optimised for
+  double floor_tol, ceil_tol;   // relative tolerances of ValidatePhiRange (0.1, 0.1)
+  double min_phi;               // replaces a non-positive minimum in OptimizeM
+  double last_min, last_max;    // the field's range seen by the last step
+  int init, changed, count;
+  int v_dirty;                  // nonzero: V changed since the forcing was built
+};
+struct ExtvCoefArgs {
+  int nx, ny, m, nyh;
+  double fx, fy, gamma, beta, q0, epsilon, dt, small_z_tol;
+  double2* coef;          // (A - 1 - M Bg, Bg), [kx][ky <= ny/2]
+  const double2* vhat;    // rfft2 of V, (ny, m + 1) row-major
+  double2* forcing;       // B lap V_hat, [kx][ky], kx <= m
+};
+cudaError_t launch_extv_decide(const double* minmax, int nparts, ExtvState* st, double g, cudaStream_t s);
+cudaError_t launch_extv_coef(const ExtvCoefArgs& a, const ExtvState* st, cudaStream_t s);
+
 // Vacancy location on a local density field (pfc_track.cu), count > 0.
 cudaError_t launch_locate_vacancies(const double* field, int nx, int ny, double dx, double dy, double* xy,
                                     int count, int32_t* status, cudaStream_t stream);

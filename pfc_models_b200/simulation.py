@@ -383,7 +383,7 @@ class Simulation:
     """The reference's Simulation (models/stdpfc/simulation.py:166-268) backed by a plan."""
 
     def __init__(self, model: str, modelParameters, geometry, precision="fp64", clamp_log=False, device=None,
-                 kernels="auto", graphs=True, pdl=None, one_cta=True):
+                 kernels="auto", graphs=True, pdl=None, one_cta=True, _flags=0, _state_cls=None):
         if model not in ("std", "log"):
             raise ValueError(f"model must be 'std' or 'log', got {model!r}")
         if precision not in _PRECISIONS:
@@ -408,11 +408,12 @@ class Simulation:
             prob.flags = (prob.flags & ~_lib.FLAG_PDL) | (_lib.FLAG_PDL if pdl else 0)
         if not one_cta:       # small FP64 mixed-radix grids: keep the two-kernel step
             prob.flags |= _lib.FLAG_NO_ONE_CTA
+        prob.flags |= int(_flags)
         self._plan = Plan(prob, device)
         self._version = 0
         self._mu_current = False
         name = "phi" if model == "log" else "n"
-        self.State = _SimulationState(self, name)
+        self.State = (_state_cls or _SimulationState)(self, name)
         setattr(self, name, getattr(self.State, name))
         self.mu = self.State.mu
 
