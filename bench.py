@@ -29,6 +29,10 @@ psi in relative L2, and the mass drift.
 Under torchrun with N > 1 every rank runs an independent replica (a single simulation
 does not shard profitably over NVLink); timings are the max over ranks.
 
+`cupy_baseline` times the reference's own GPU path (models/stdpfc/simulation.py, unmodified,
+installed under baseline/_ref) through a torch-backed `cupy` stand-in on the same GPU and
+workload, FP64, 100 TimeStep() calls between CUDA events (baseline/cupy_reference.py).
+
 `--impl reference` times the reference's CPU algorithm (the oracle port of
 stdpfc_cpu, threaded pocketfft through scipy.fft with every host core) on the
 same workload and metric.
@@ -190,6 +194,23 @@ def cpu_baseline(max_seconds=20.0, max_steps=20):
     return {"value": NX * NY / med, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{len(times)} ETD1 steps of the same 2048^2 workload, median step "
                       f"{med * 1e3:.1f} ms (numpy/scipy pocketfft, {cores} threads)"}
+
+
+def cupy_baseline(steps=100, warmup=5):
+    """The reference's own GPU path (models/stdpfc/simulation.py through the torch-backed cupy
+    stand-in, baseline/cupy_reference.py) on this GPU, same workload, FP64, in a child
+    process so that the stand-in module never enters this one."""
+    import subprocess
+    script = os.path.join(ROOT, "baseline", "cupy_reference.py")
+    try:
+        r = subprocess.run([sys.executable, script, "--steps", str(steps), "--warmup", str(warmup)],
+                           capture_output=True, text=True, timeout=600)
+        lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+        if r.returncode != 0 or not lines:
+            return {"unavailable": f"exit {r.returncode}: {(r.stderr or r.stdout)[-300:]}"}
+        return json.loads(lines[-1])
+    except Exception as e:  # noqa: BLE001
+        return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
 def run_reference(args):
@@ -504,6 +525,12 @@ def run_ours(args):
             line["accuracy"] = acc
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
+        if world == 1 and not args.no_cupy_baseline:
+            cb = cupy_baseline()
+            if "value" in cb:
+                cb["fp32_over_reference_gpu"] = r32["value"] / cb["value"]
+                cb["fp64_over_reference_gpu"] = res["fp64"]["value"] / cb["value"]
+            line["cupy_baseline"] = cb
         print(json.dumps(line))
     if distributed:
         dist.barrier()
@@ -518,6 +545,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cupy-baseline", action="store_true", help="skip the reference GPU path leg")
     ap.add_argument("--no-8192", action="store_true", help="skip the 8192^2 HBM-bound key")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the 20000-step FP32 vs FP64 record")
     kc = ap.add_argument_group("kernel case (short fixed workload for profiling)")
