@@ -56,6 +56,7 @@ extern "C" {
 
 /* status bits (pfc_status) */
 #define PFC_STATUS_NONFINITE 1  /* a reduction met a NaN/Inf */
+#define PFC_STATUS_TIMEOUT 2    /* a bounded device-side wait gave up (the step is void) */
 
 /*
  * Problem description. Field meanings follow
@@ -151,6 +152,10 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
                                      FP64 plain, the log model and clamp_log = 1 with
                                      min_phi > 0; steps with the mixed-radix two-kernel step
                                      plus two small kernels, alone (not in a batch) */
+#define PFC_FLAG_TMA 64           /* with PFC_FLAG_PACKED: the row kernel stages its tile of W
+                                     with the tensor memory accelerator (cp.async.bulk.tensor
+                                     boxes, mbarrier completion) instead of 16-byte copies;
+                                     single plans only (a batch's launch uses the copies) */
 #define PFC_FLAG_PACKED 16        /* FP32-mixed power-of-two grids: the two-lane packed step
                                      kernels (two rows / two columns per thread in packed
                                      f32x2 arithmetic); PFC_FLAG_ROW_EE / COL_EE then give the

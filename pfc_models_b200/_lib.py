@@ -24,15 +24,17 @@ FLAG_GENERIC_ONLY, FLAG_NO_GRAPHS, FLAG_PDL = 1, 2, 4
 FLAG_NO_ONE_CTA = 8
 FLAG_PACKED = 16
 FLAG_EXTV = 32
+FLAG_TMA = 64
 PATH_MIXED_RADIX, PATH_POW2, PATH_ONE_CTA = 0, 1, 2
 STATUS_NONFINITE = 1
+STATUS_TIMEOUT = 2
 
 
-def flag_variant(ee_row=0, ee_col=0, row_tile=0, col_cta=0, pdl=0, packed=0):
+def flag_variant(ee_row=0, ee_col=0, row_tile=0, col_cta=0, pdl=0, packed=0, tma=0):
     """problem.flags bits selecting a step-kernel variant (PFC_FLAG_ROW_EE & co.)."""
     cc = {0: 0, 1: 1, 2: 2, 4: 3}[int(col_cta)]
     return (int(ee_row) << 8) | (int(ee_col) << 16) | (int(row_tile) << 24) | (cc << 29) | \
-        (FLAG_PDL if pdl else 0) | (FLAG_PACKED if packed else 0)
+        (FLAG_PDL if pdl else 0) | (FLAG_PACKED if packed else 0) | (FLAG_TMA if tma else 0)
 
 # every symbol include/pfc_b200.h declares, with (restype, argtypes)
 _vp, _i32, _i64, _dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double

@@ -183,6 +183,8 @@ struct FastRowArgs {
   const double* scal;
   int clamp;
   double g, min_phi, min_log;
+  int tma_box;               // packed row kernel: kx extent of a TMA box (0: asynchronous copies)
+  int* err;                  // status word; a bounded wait that gave up ORs PFC_STATUS_TIMEOUT
 };
 
 template <class T>

@@ -15,6 +15,8 @@
 // Pass twiddles are float4 (c, c, s, s) tables, [q-1][k] per pass, s = sin of the
 // forward angle; inverse passes conjugate them.
 #pragma once
+#include <cuda.h>
+
 #include "pfc_fast.cuh"
 #include "pfc_pack.cuh"
 
@@ -124,21 +126,40 @@ __device__ __forceinline__ float4 pc2raw(pc v) { return make_float4(v.r.x, v.i.x
 template <int TPF> struct PkBound { static constexpr int value = TPF > 256 ? TPF : 256; };
 template <int TPF> struct PkMinB { static constexpr int value = TPF > 256 ? 1 : 2; };
 
+// Byte offset of tile entry (p, kx) in a TMA-staged tile: the box lands as [kx][rows]
+// (8-byte complex per row, ib = rows * 8 bytes per kx) with the hardware swizzle of its
+// inner width, XOR of the 16-byte chunk index (bits 4..) with bits 7.. of the offset
+// (smask = 0, 1, 3, 7 for no swizzle, 32-, 64- and 128-byte swizzle; the tile starts on a
+// 1024-byte boundary, so the offset's bits are the address bits the hardware uses).
+__device__ __forceinline__ unsigned tma_tile_off(int kx, int p, int ib, unsigned smask) {
+  const unsigned o = (unsigned)kx * (unsigned)ib + 16u * (unsigned)p;
+  return o ^ (((o >> 7) & smask) << 4);
+}
+
+constexpr unsigned kStatusTimeout = 2;   // PFC_STATUS_TIMEOUT
+constexpr long long kTmaWaitLimit = 1LL << 22;
+
 // ------------------------------------------------------------------ row kernel
 // CTA: `rows` consecutive rows (a.rows even), `rows / 2` groups of TPF threads, group p
-// owning rows y0 + 2p, y0 + 2p + 1. The tile is staged with 16-byte asynchronous copies:
-// entry (p, kx) holds W[kx][y0 + 2p] and W[kx][y0 + 2p + 1], the 16 contiguous bytes of
-// the column-major array; consecutive threads take consecutive p of one kx (runs of
-// rows * 8 bytes per kx).
+// owning rows y0 + 2p, y0 + 2p + 1. Entry (p, kx) of the tile is W[kx][y0 + 2p] and
+// W[kx][y0 + 2p + 1], the 16 contiguous bytes of the column-major array. The tile is staged
+// either by the tensor memory accelerator (a.tma_box > 0: one thread issues
+// cp.async.bulk.tensor boxes of rows x tma_box from the tensor map of W, completion counted
+// on an mbarrier, swizzled [kx][rows] layout in shared memory), or with 16-byte
+// asynchronous copies into a padded [p][kx] layout (consecutive threads take consecutive p
+// of one kx: runs of rows * 8 bytes per kx).
 template <int M, int EE_REQ, int MODEL>
 __global__ void __launch_bounds__(PkBound<PkSeq<M, EE_REQ>::TPF>::value, PkMinB<PkSeq<M, EE_REQ>::TPF>::value)
-row_step_pk(FastRowArgs<float> a) {
+row_step_pk(FastRowArgs<float> a, const __grid_constant__ CUtensorMap tmap) {
   using S = PkSeq<M, EE_REQ>;
   constexpr int EE = S::EE, TPF = S::TPF, NP = S::NPASS;
   constexpr int P = kPkPad;
   constexpr int LD = M + (M >> P);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float4* sm = reinterpret_cast<float4*>(smem_raw);
+  // 1024-byte aligned start (the plan requests 1 KB more when it stages with TMA)
+  const unsigned raw_s = (unsigned)__cvta_generic_to_shared(smem_raw);
+  const unsigned pad_s = a.tma_box ? ((1024u - (raw_s & 1023u)) & 1023u) : 0u;
+  float4* sm = reinterpret_cast<float4*>(smem_raw + pad_s);
   const int ny = a.ny, rows = a.rows, pairs = rows >> 1;
   const int y0 = blockIdx.x * rows;
   const int g = threadIdx.x / TPF, t = threadIdx.x - g * TPF;
@@ -160,7 +181,46 @@ row_step_pk(FastRowArgs<float> a) {
 
   // ---- tile load: entry (p, kx) <- 16 bytes at W[kx][y0 + 2p]
   const int tp = threadIdx.x % pairs, kx0 = threadIdx.x / pairs, kstep = blockDim.x / pairs;
-  {
+  const bool tma = a.tma_box > 0;
+  const int ib = rows * 8;
+  const unsigned smask = ib >= 128 ? 7u : ib == 64 ? 3u : ib == 32 ? 1u : 0u;
+  if (tma) {
+    __shared__ __align__(8) unsigned long long tbar;
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(&tbar);
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned bytes = (unsigned)M * (unsigned)ib;
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+      const unsigned base = raw_s + pad_s;
+      // x (the innermost coordinate, rows) = y0 is even: 16-byte aligned; kx is the outer one
+      for (int kx = 0; kx < M; kx += a.tma_box) {
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+            ::"r"(base + (unsigned)kx * (unsigned)ib), "l"(reinterpret_cast<unsigned long long>(&tmap)), "r"(y0),
+              "r"(kx), "r"(bar)
+            : "memory");
+      }
+    }
+    unsigned done = 0;
+    for (long long it = 0; !done && it < kTmaWaitLimit; ++it) {
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}"
+          : "=r"(done)
+          : "r"(bar)
+          : "memory");
+    }
+    if (!done) {
+      // the boxes did not arrive within the limit: report and leave (nothing else reads them)
+      if (threadIdx.x == 0 && a.err) atomicOr(a.err, (int)kStatusTimeout);
+      return;
+    }
+  } else {
     float4* drow = sm + tp * LD;
     const float2* src = gin + (size_t)kx0 * ny + (y0 + 2 * tp);
     const size_t gstep = (size_t)kstep * ny;
@@ -168,10 +228,10 @@ row_step_pk(FastRowArgs<float> a) {
       const unsigned sdst = (unsigned)__cvta_generic_to_shared(drow + padi<P>(kx));
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sdst), "l"(src) : "memory");
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
   }
-  asm volatile("cp.async.commit_group;" ::: "memory");
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
-  __syncthreads();
 
   // nonlinearity parameters (deviation form)
   const float c1 = (float)scal[kScalC1], c2 = (float)scal[kScalC2];
@@ -192,11 +252,17 @@ row_step_pk(FastRowArgs<float> a) {
 #pragma unroll
       for (int q = 0; q < S::radA(0); ++q) {
         const int k = t + b * TPF + q * P0::NR;
-        const pc x = raw2pc(row[padi<P>(k)]);
+        const float4* xk = tma ? reinterpret_cast<const float4*>(reinterpret_cast<const char*>(sm) +
+                                                                  tma_tile_off(k, g, ib, smask))
+                               : row + padi<P>(k);
+        const pc x = raw2pc(*xk);
         if (k == 0) {
           v[b * S::radA(0) + q] = mkpc(add2(x.r, x.i), sub2(x.r, x.i));
         } else {
-          const pc y = raw2pc(row[padi<P>(M - k)]);
+          const float4* xm = tma ? reinterpret_cast<const float4*>(reinterpret_cast<const char*>(sm) +
+                                                                    tma_tile_off(M - k, g, ib, smask))
+                                 : row + padi<P>(M - k);
+          const pc y = raw2pc(*xm);
           const float4 r = __ldg(rtw + k);
           const float2 C = make_float2(r.x, r.y), Sn = make_float2(r.z, r.w);
           const pc s = mkpc(add2(x.r, y.r), sub2(x.i, y.i));
@@ -207,7 +273,9 @@ row_step_pk(FastRowArgs<float> a) {
         }
       }
   }
-  group_sync<TPF>(g);   // every partner read of the tile done before the exchange writes
+  // every partner read of the tile done before the exchange writes (a TMA tile interleaves
+  // the groups' rows, so then the whole CTA)
+  if (tma) __syncthreads(); else group_sync<TPF>(g);
   if constexpr (NP == 1) {
     PkPass<M, EE, S::radA(0), 1>::template compute<true>(v, t, twA);
   } else {

@@ -9,6 +9,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include "pfc_b200.h"
@@ -177,6 +179,8 @@ struct pfc_plan {
   double2* forcing = nullptr;          // B lap V_hat, [kx][ky]
   void* scratch_state = nullptr;       // a spectral state for transforming V
   int rt4_off = 0;             // packed kernels: offset of the float4 real-packing table in tw
+  int tma_box = 0;             // packed row kernel staged by TMA: kx extent of a box (0: cp.async)
+  CUtensorMap tmap{};          // its tensor map of W ([kx][y], 8-byte elements)
   int fc_threads = 0, fc_grid = 0;
   size_t fr_smem = 0, fc_smem = 0;
   int tw_ra = 0, tw_rb = 0, tw_ca = 0, tw_cb = 0;  // table offsets (complex elements)
@@ -396,6 +400,38 @@ int setup_pack(pfc_plan* h, std::vector<long double>& tw) {
   return PFC_OK;
 }
 
+// The tensor map through which the packed row kernel stages its tile (PFC_FLAG_TMA):
+// W as a 2-D array of 8-byte elements, y innermost (ny, stride 8 B) and kx outer (m,
+// stride ny * 8 B); boxes of fr_rows x min(m, 256) with the swizzle of the box's inner
+// width. The box's x coordinate is the tile's first row, always even (16-byte aligned).
+int setup_tma(pfc_plan* h) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", reinterpret_cast<void**>(&encode), cudaEnableDefault,
+                                &q) != cudaSuccess || q != cudaDriverEntryPointSuccess || !encode)
+      return fail(PFC_E_CUDA, "pfc_plan_create: cuTensorMapEncodeTiled is not available");
+  }
+  const int ib = h->fr_rows * 8;
+  CUtensorMapSwizzle sw = CU_TENSOR_MAP_SWIZZLE_NONE;
+  if (ib == 32) sw = CU_TENSOR_MAP_SWIZZLE_32B;
+  else if (ib == 64) sw = CU_TENSOR_MAP_SWIZZLE_64B;
+  else if (ib == 128) sw = CU_TENSOR_MAP_SWIZZLE_128B;
+  else if (ib != 16) return fail(PFC_E_ARG, "pfc_plan_create: TMA staging takes row tiles of 2 to 16 rows");
+  const int box = std::min(h->m, 256);
+  cuuint64_t dims[2] = {(cuuint64_t)h->ny, (cuuint64_t)h->m};
+  cuuint64_t strides[1] = {(cuuint64_t)h->ny * 8};
+  cuuint32_t boxd[2] = {(cuuint32_t)h->fr_rows, (cuuint32_t)box};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode(&h->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, h->W, dims, strides, boxd, estr,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(PFC_E_CUDA, "pfc_plan_create: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  h->tma_box = box;
+  h->fr_smem += 1024;   // room to start the tile on a 1024-byte boundary
+  return raise_smem_limit(h->fast_row_fn, h->fr_smem);
+}
+
 // Chooses the fast kernels and their launch shapes; appends their twiddle tables to tw.
 // problem.flags may pick the elements per thread of each kernel and the row tile.
 template <class T>
@@ -518,7 +554,11 @@ int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
     a.clamp = h->prob.clamp_log;
     a.g = h->prob.g; a.min_phi = h->prob.min_phi;
     a.min_log = (h->prob.min_phi > 0) ? std::log(h->prob.min_phi) : -INFINITY;
-    void* args[] = {(void*)&a};
+    a.err = h->status;
+    a.tma_box = table ? 0 : h->tma_box;   // a batch's plans each have their own W: copies
+    void* args_pk[] = {(void*)&a, (void*)&h->tmap};
+    void* args1[] = {(void*)&a};
+    void** args = h->packed ? args_pk : args1;
     cudaError_t e = launch_step_kernel(h, h->fast_row_fn, dim3(h->fr_grid, count), dim3(h->fr_threads), args,
                                        h->fr_smem, s);
     ++h->launches;
@@ -1231,6 +1271,10 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   }
   int rc = h->fp32 ? set_smem_attrs<float>(h) : set_smem_attrs<double>(h);
   if (rc) return cleanup_fail(rc);
+  if (h->packed && (p->flags & PFC_FLAG_TMA)) {
+    rc = setup_tma(h);
+    if (rc) return cleanup_fail(rc);
+  }
   rc = setup_onecta(h);
   if (rc) return cleanup_fail(rc);
   *out = h;

@@ -364,10 +364,11 @@ def _kernel_flags(kernels, prob):
     the autotuner cached for this grid, else the defaults), "default", "generic" (the
     mixed-radix kernels everywhere), or a dict with any of "ee_row", "ee_col",
     "row_tile", "col_cta" (columns per CTA of the column kernel), "pdl" and "packed"
-    (the two-lane packed FP32 kernels; then ee_* count values per lane)."""
+    (the two-lane packed FP32 kernels; then ee_* count values per lane), "tma" (their row
+    tile staged by the tensor memory accelerator)."""
     if isinstance(kernels, dict):
         return _lib.flag_variant(**{k: kernels.get(k, 0) for k in ("ee_row", "ee_col", "row_tile", "col_cta",
-                                                                    "pdl", "packed")})
+                                                                    "pdl", "packed", "tma")})
     if kernels == "generic":
         return _lib.FLAG_GENERIC_ONLY
     if kernels == "default":
