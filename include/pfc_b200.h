@@ -166,6 +166,9 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
  * default 32; FP64: 8 or 16, default 16) and rows per CTA of the row kernel
  * (1, 2, 4, 8 or 16). Other values make pfc_plan_create return PFC_E_ARG. The
  * autotuner (pfc_models_b200/tune.py) measures these per grid and caches the best. */
+/* OR-ed into a PFC_FLAG_ROW_EE / PFC_FLAG_COL_EE value: that pass's two-lane packed FP32
+ * kernel (8 or 16 values per lane) */
+#define PFC_EE_PACKED 0x80
 #define PFC_FLAG_ROW_EE(e) ((int32_t)(e) << 8)
 #define PFC_FLAG_COL_EE(e) ((int32_t)(e) << 16)
 #define PFC_FLAG_ROW_TILE(r) ((int32_t)(r) << 24)

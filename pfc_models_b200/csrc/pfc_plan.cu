@@ -170,7 +170,8 @@ struct pfc_plan {
   void* fast_col_fn = nullptr;
   int fr_rows = 0, fr_threads = 0, fr_ld = 0, fr_grid = 0;
   int ee_row = 0, ee_col = 0;  // elements per thread of the fast kernels (per lane when packed)
-  bool packed = false;         // two-lane packed FP32 step kernels (pfc_pack_step.cuh)
+  bool packed = false;         // two-lane packed FP32 step kernels (pfc_pack_step.cuh) on either pass
+  bool packed_row = false, packed_col = false;
   // log PFC with an external potential (PFC_FLAG_EXTV, pfc_extv.cu)
   bool extv = false;
   pfc::ExtvState* extv_st = nullptr;   // device
@@ -344,23 +345,90 @@ bool fast_seq_tables(int lg, int ee, std::vector<long double>& tw, int& a, int& 
   return ee == 8 ? FastInst<double, 8>::tables(lg, tw, a, b) : FastInst<double, 16>::tables(lg, tw, a, b);
 }
 
-// The two-lane packed FP32 step kernels (PFC_FLAG_PACKED): row tiles of `rows` rows
-// (rows / 2 groups of one row pair), ngc column pairs per CTA; float4 pass tables.
-int setup_pack(pfc_plan* h, std::vector<long double>& tw) {
-  const int flags = h->prob.flags;
-  const int ee_r = PFC_FLAG_ROW_EE_OF(flags) ? PFC_FLAG_ROW_EE_OF(flags) : 16;
-  const int ee_c = PFC_FLAG_COL_EE_OF(flags) ? PFC_FLAG_COL_EE_OF(flags) : 16;
-  if ((ee_r != 8 && ee_r != 16) || (ee_c != 8 && ee_c != 16))
-    return fail(PFC_E_ARG, "pfc_plan_create: packed kernels take 8 or 16 values per lane (got %d, %d)", ee_r, ee_c);
-  const int tile = PFC_FLAG_ROW_TILE_OF(flags);
-  if (tile && (tile < 2 || tile > 16 || (tile & (tile - 1))))
-    return fail(PFC_E_ARG, "pfc_plan_create: packed row tile %d is not a power of two in [2, 16]", tile);
-  const int lm = ilog2_exact(h->m), ly = ilog2_exact(h->ny);
-  if ((flags & PFC_FLAG_GENERIC_ONLY) || lm < kPackMinLog || lm > kPackMaxLogRow || ly < kPackMinLog ||
-      ly > kPackMaxLogCol)
-    return PFC_OK;
-  FastKernel kr, kc;
-  if (!pack_row(lm, ee_r, h->prob.model, &kr) || !pack_col(ly, ee_c, &kc)) return PFC_OK;
+// Launch shape of the power-of-two row kernel (one side of the fast step).
+struct FastRowSide {
+  bool ok = false, packed = false;
+  void* fn = nullptr;
+  int ee = 0, rows = 0, threads = 0, ld = 0, grid = 0, tw_a = 0, tw_b = 0, rt4 = 0;
+  size_t smem = 0;
+};
+struct FastColSide {
+  bool ok = false, packed = false;
+  void* fn = nullptr;
+  int ee = 0, threads = 0, grid = 0, tw_a = 0, tw_b = 0;
+  size_t smem = 0;
+};
+
+// One-lane row kernel (pfc_fast.cuh): tile of rows (>= 64 B per kx run by default).
+template <class T>
+int fast_row_side(pfc_plan* h, int ee, int tile, std::vector<long double>& tw, FastRowSide& o) {
+  const int lm = ilog2_exact(h->m);
+  if (lm < kFastMinLog || lm > kFastMaxLogRow) return PFC_OK;
+  FastKernel kr;
+  if (!fast_lookup<T>(false, lm, ee, h->prob.model, &kr)) return PFC_OK;
+  // pad shift of the row tile as the kernel uses it (for length / threads per transform)
+  const int P = fast_pad_shift(sizeof(T) == 8, h->m / kr.tpf);
+  const int elt = (int)sizeof(cplx<T>);
+  const int tpr = kr.tpf;
+  int ngr = std::max(1, 256 / tpr);
+  int rows = tile ? tile : (sizeof(T) == 4 ? 8 : 4);
+  // smaller tiles for long rows so that the tile fits the shared-memory budget
+  while (rows > 1 && (size_t)rows * (h->m + (h->m >> P) + (1 << P)) * elt > 200 * 1024) rows /= 2;
+  ngr = std::min(ngr, rows);
+  rows = std::max(rows, ngr);
+  // row stride in shared memory: with S = 128 B / element slots per bank cycle,
+  // ld = S / rows (mod S) makes the transposing loads and stores of a warp hit
+  // distinct banks
+  const int slots = 128 / elt;
+  const int want = (slots / rows) % slots;
+  int ld = h->m + (h->m >> P);
+  while (ld % slots != want) ++ld;
+  const size_t smem = (size_t)rows * ld * elt;
+  if (ngr * tpr > 1024 || smem > 200 * 1024 || ilog2_exact(rows) < 0) return PFC_OK;
+  o.rows = rows;
+  o.threads = ngr * tpr;
+  o.ld = ld;
+  o.grid = (h->ny + rows - 1) / rows;
+  o.smem = smem;
+  o.fn = kr.fn;
+  o.ee = ee;
+  fast_seq_tables<T>(lm, ee, tw, o.tw_a, o.tw_b);
+  o.ok = true;
+  return PFC_OK;
+}
+
+// One-lane column kernel: one group of tpc threads per column.
+template <class T>
+int fast_col_side(pfc_plan* h, int ee, int col_cta, std::vector<long double>& tw, FastColSide& o) {
+  const int ly = ilog2_exact(h->ny);
+  if (ly < kFastMinLog || ly > kFastMaxLogCol) return PFC_OK;
+  FastKernel kc;
+  if (!fast_lookup<T>(true, ly, ee, h->prob.model, &kc)) return PFC_OK;
+  const int Pc = fast_pad_shift(sizeof(T) == 8, h->ny / kc.tpf);
+  const int elt = (int)sizeof(cplx<T>);
+  const int tpc = kc.tpf;
+  // (the kernels are built for at most 256 threads per CTA, or one group if larger)
+  const int ngc_max = std::max(1, 256 / tpc);
+  const int ngc = std::min(col_cta ? std::min(col_cta, ngc_max) : ngc_max, h->m);
+  const size_t smem = (size_t)ngc * (h->ny + (h->ny >> Pc) + 2) * elt;   // one exchange buffer per column
+  if (ngc * tpc > 1024 || smem > 200 * 1024) return PFC_OK;
+  o.threads = ngc * tpc;
+  o.grid = h->m / ngc;
+  o.smem = smem;
+  o.fn = kc.fn;
+  o.ee = ee;
+  fast_seq_tables<T>(ly, ee, tw, o.tw_a, o.tw_b);
+  o.ok = true;
+  return PFC_OK;
+}
+
+// Two-lane packed FP32 row kernel (pfc_pack_step.cuh): tiles of `rows` rows, rows / 2
+// groups of one row pair; float4 pass tables and the float4 real-packing table.
+int pack_row_side(pfc_plan* h, int ee, int tile, std::vector<long double>& tw, FastRowSide& o) {
+  const int lm = ilog2_exact(h->m);
+  if (lm < kPackMinLog || lm > kPackMaxLogRow) return PFC_OK;
+  FastKernel kr;
+  if (!pack_row(lm, ee, h->prob.model, &kr)) return PFC_OK;
   const size_t slot = 16;   // one pc (two complex floats)
   const size_t ld = (size_t)h->m + (h->m >> 4);
   int rows = tile ? tile : 8;
@@ -370,33 +438,42 @@ int setup_pack(pfc_plan* h, std::vector<long double>& tw) {
   while (rows > 2 && ((size_t)(rows / 2) * ld * slot > 110 * 1024 || (rows / 2) * kr.tpf > max_threads)) rows /= 2;
   if (h->ny % rows || (rows / 2) * kr.tpf > max_threads || (size_t)(rows / 2) * ld * slot > 200 * 1024)
     return PFC_OK;
-  const int col_cta = PFC_FLAG_COL_CTA_OF(flags), ngc_max = std::max(1, 256 / kc.tpf);
+  o.rows = rows;
+  o.threads = (rows / 2) * kr.tpf;
+  o.ld = (int)ld;
+  o.grid = h->ny / rows;
+  o.smem = (size_t)(rows / 2) * ld * slot;
+  o.fn = kr.fn;
+  o.ee = ee;
+  o.packed = true;
+  pack_tables(lm, ee, tw, o.tw_a, o.tw_b);
+  pack_real_table(h->nx, tw, o.rt4);
+  o.ok = true;
+  return PFC_OK;
+}
+
+// Two-lane packed FP32 column kernel: ngc column pairs per CTA.
+int pack_col_side(pfc_plan* h, int ee, int col_cta, std::vector<long double>& tw, FastColSide& o) {
+  const int ly = ilog2_exact(h->ny);
+  if (ly < kPackMinLog || ly > kPackMaxLogCol || h->m % 2) return PFC_OK;
+  FastKernel kc;
+  if (!pack_col(ly, ee, &kc)) return PFC_OK;
+  const size_t slot = 16;
+  const int ngc_max = std::max(1, 256 / kc.tpf);
   const int npairs = h->m / 2;
   int ngc = std::min(col_cta ? std::min(col_cta, ngc_max) : ngc_max, npairs);
   while (npairs % ngc) ngc /= 2;
   const size_t padn = (size_t)h->ny + (h->ny >> 4) + 2;
-  const size_t fc_smem = (size_t)ngc * padn * slot;
-  const size_t fr_smem = (size_t)(rows / 2) * ld * slot;
-  if (ngc * kc.tpf > std::max(256, kc.tpf) || fc_smem > 200 * 1024) return PFC_OK;
-  h->fr_rows = rows;
-  h->fr_threads = (rows / 2) * kr.tpf;
-  h->fr_ld = (int)ld;
-  h->fr_grid = h->ny / rows;
-  h->fr_smem = fr_smem;
-  h->fc_threads = ngc * kc.tpf;
-  h->fc_grid = npairs / ngc;
-  h->fc_smem = fc_smem;
-  h->fast_row_fn = kr.fn;
-  h->fast_col_fn = kc.fn;
-  h->ee_row = ee_r;
-  h->ee_col = ee_c;
-  pack_tables(lm, ee_r, tw, h->tw_ra, h->tw_rb);
-  pack_tables(ly, ee_c, tw, h->tw_ca, h->tw_cb);
-  pack_real_table(h->nx, tw, h->rt4_off);
-  if (int rc = raise_smem_limit(h->fast_row_fn, h->fr_smem)) return rc;
-  if (int rc = raise_smem_limit(h->fast_col_fn, h->fc_smem)) return rc;
-  h->fast = true;
-  h->packed = true;
+  const size_t smem = (size_t)ngc * padn * slot;
+  if (ngc * kc.tpf > std::max(256, kc.tpf) || smem > 200 * 1024) return PFC_OK;
+  o.threads = ngc * kc.tpf;
+  o.grid = npairs / ngc;
+  o.smem = smem;
+  o.fn = kc.fn;
+  o.ee = ee;
+  o.packed = true;
+  pack_tables(ly, ee, tw, o.tw_a, o.tw_b);
+  o.ok = true;
   return PFC_OK;
 }
 
@@ -433,72 +510,59 @@ int setup_tma(pfc_plan* h) {
 }
 
 // Chooses the fast kernels and their launch shapes; appends their twiddle tables to tw.
-// problem.flags may pick the elements per thread of each kernel and the row tile.
+// problem.flags may pick each kernel's values per thread (with PFC_EE_PACKED, or
+// PFC_FLAG_PACKED for both, the two-lane packed FP32 kernel of that pass), the row tile
+// and the columns per CTA. Both passes must have a fast kernel, else the plan uses the
+// mixed-radix kernels.
 template <class T>
 int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
   const int flags = h->prob.flags;
-  if (sizeof(T) == 4 && (flags & PFC_FLAG_PACKED)) return setup_pack(h, tw);
-  const int ee_r = PFC_FLAG_ROW_EE_OF(flags) ? PFC_FLAG_ROW_EE_OF(flags) : fast_ee_default<T>();
-  const int ee_c = PFC_FLAG_COL_EE_OF(flags) ? PFC_FLAG_COL_EE_OF(flags) : fast_ee_default<T>();
+  const int fr = PFC_FLAG_ROW_EE_OF(flags), fc = PFC_FLAG_COL_EE_OF(flags);
+  const bool all_packed = (flags & PFC_FLAG_PACKED) != 0;
+  const bool row_packed = all_packed || (fr & PFC_EE_PACKED), col_packed = all_packed || (fc & PFC_EE_PACKED);
+  if ((row_packed || col_packed) && sizeof(T) != 4)
+    return fail(PFC_E_ARG, "pfc_plan_create: the packed kernels are built for the FP32-mixed form only");
+  const int er = fr & ~PFC_EE_PACKED, ec = fc & ~PFC_EE_PACKED;
+  const int ee_r = er ? er : (row_packed ? 16 : fast_ee_default<T>());
+  const int ee_c = ec ? ec : (col_packed ? 16 : fast_ee_default<T>());
+  if (row_packed ? (ee_r != 8 && ee_r != 16) : !fast_ee_valid<T>(ee_r))
+    return fail(PFC_E_ARG, "pfc_plan_create: row kernel values per thread %d not built (FP32: 8, 16 or 32; "
+                "FP64: 8 or 16; packed: 8 or 16 per lane)", ee_r);
+  if (col_packed ? (ee_c != 8 && ee_c != 16) : !fast_ee_valid<T>(ee_c))
+    return fail(PFC_E_ARG, "pfc_plan_create: column kernel values per thread %d not built (FP32: 8, 16 or 32; "
+                "FP64: 8 or 16; packed: 8 or 16 per lane)", ee_c);
   const int tile = PFC_FLAG_ROW_TILE_OF(flags);
-  if (!fast_ee_valid<T>(ee_r) || !fast_ee_valid<T>(ee_c))
-    return fail(PFC_E_ARG, "pfc_plan_create: elements per thread (%d, %d) not built for this precision "
-                "(FP32: 8, 16 or 32; FP64: 8 or 16)", ee_r, ee_c);
-  if (tile && (tile > 16 || (tile & (tile - 1))))
-    return fail(PFC_E_ARG, "pfc_plan_create: row tile %d is not a power of two <= 16", tile);
-  const int lm = ilog2_exact(h->m), ly = ilog2_exact(h->ny);
-  if ((flags & PFC_FLAG_GENERIC_ONLY) || lm < kFastMinLog || lm > kFastMaxLogRow || ly < kFastMinLog ||
-      ly > kFastMaxLogCol)
-    return PFC_OK;
-  FastKernel kr, kc;
-  if (!fast_lookup<T>(false, lm, ee_r, h->prob.model, &kr) || !fast_lookup<T>(true, ly, ee_c, h->prob.model, &kc))
-    return PFC_OK;
-  // pad shifts of the row tile and the column exchange buffers, as the kernels use them
-  // (for the effective values per thread, length / threads per transform)
-  const int P = fast_pad_shift(sizeof(T) == 8, h->m / kr.tpf);
-  const int Pc = fast_pad_shift(sizeof(T) == 8, h->ny / kc.tpf);
-  const int elt = (int)sizeof(cplx<T>);
-  // row kernel: tile of fr_rows rows (>= 64 B per kx run by default), groups of tpf threads
-  const int tpr = kr.tpf;
-  int ngr = std::max(1, 256 / tpr);
-  int rows = tile ? tile : (sizeof(T) == 4 ? 8 : 4);
-  // smaller tiles for long rows so that the tile fits the shared-memory budget
-  while (rows > 1 && (size_t)rows * (h->m + (h->m >> P) + (1 << P)) * elt > 200 * 1024) rows /= 2;
-  ngr = std::min(ngr, rows);
-  rows = std::max(rows, ngr);
-  // row stride in shared memory: with S = 128 B / element slots per bank cycle,
-  // ld = S / rows (mod S) makes the transposing loads and stores of a warp hit
-  // distinct banks
-  const int slots = 128 / elt;
-  const int want = (slots / rows) % slots;
-  int ld = h->m + (h->m >> P);
-  while (ld % slots != want) ++ld;
-  // column kernel: one group of tpc threads per column
-  const int tpc = kc.tpf;
-  // (the kernels are built for at most 256 threads per CTA, or one group if larger)
-  const int col_cta = PFC_FLAG_COL_CTA_OF(flags), ngc_max = std::max(1, 256 / tpc);
-  const int ngc = std::min(col_cta ? std::min(col_cta, ngc_max) : ngc_max, h->m);
-  const size_t fr_smem = (size_t)rows * ld * elt;
-  const size_t fc_smem = (size_t)ngc * (h->ny + (h->ny >> Pc) + 2) * elt;   // one exchange buffer per column
-  if (ngr * tpr > 1024 || ngc * tpc > 1024 || fr_smem > 200 * 1024 || fc_smem > 200 * 1024 ||
-      ilog2_exact(rows) < 0)
-    return PFC_OK;  // generic path
-  h->fr_rows = rows;
-  h->fr_threads = ngr * tpr;
-  h->fr_ld = ld;
-  h->fr_grid = (h->ny + rows - 1) / rows;
-  h->fr_smem = fr_smem;
-  h->fc_threads = ngc * tpc;
-  h->fc_grid = h->m / ngc;
-  h->fc_smem = fc_smem;
-  h->fast_row_fn = kr.fn;
-  h->fast_col_fn = kc.fn;
-  h->ee_row = ee_r;
-  h->ee_col = ee_c;
-  fast_seq_tables<T>(lm, ee_r, tw, h->tw_ra, h->tw_rb);
-  fast_seq_tables<T>(ly, ee_c, tw, h->tw_ca, h->tw_cb);
-  if (int rc = raise_smem_limit(h->fast_row_fn, h->fr_smem)) return rc;
-  if (int rc = raise_smem_limit(h->fast_col_fn, h->fc_smem)) return rc;
+  if (tile && (tile > 16 || (tile & (tile - 1)) || (row_packed && tile < 2)))
+    return fail(PFC_E_ARG, "pfc_plan_create: row tile %d is not a power of two <= 16 (>= 2 packed)", tile);
+  if (flags & PFC_FLAG_GENERIC_ONLY) return PFC_OK;
+  const int col_cta = PFC_FLAG_COL_CTA_OF(flags);
+  FastRowSide r;
+  FastColSide c;
+  int rc = row_packed ? pack_row_side(h, ee_r, tile, tw, r) : fast_row_side<T>(h, ee_r, tile, tw, r);
+  if (rc) return rc;
+  rc = col_packed ? pack_col_side(h, ee_c, col_cta, tw, c) : fast_col_side<T>(h, ee_c, col_cta, tw, c);
+  if (rc) return rc;
+  if (!r.ok || !c.ok) return PFC_OK;   // generic path
+  h->fr_rows = r.rows;
+  h->fr_threads = r.threads;
+  h->fr_ld = r.ld;
+  h->fr_grid = r.grid;
+  h->fr_smem = r.smem;
+  h->fc_threads = c.threads;
+  h->fc_grid = c.grid;
+  h->fc_smem = c.smem;
+  h->fast_row_fn = r.fn;
+  h->fast_col_fn = c.fn;
+  h->ee_row = r.ee;
+  h->ee_col = c.ee;
+  h->tw_ra = r.tw_a; h->tw_rb = r.tw_b;
+  h->tw_ca = c.tw_a; h->tw_cb = c.tw_b;
+  h->rt4_off = r.rt4;
+  h->packed_row = r.packed;
+  h->packed_col = c.packed;
+  h->packed = r.packed || c.packed;
+  if (int e = raise_smem_limit(h->fast_row_fn, h->fr_smem)) return e;
+  if (int e = raise_smem_limit(h->fast_col_fn, h->fc_smem)) return e;
   h->fast = true;
   return PFC_OK;
 }
@@ -549,7 +613,7 @@ int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
     a.in = reinterpret_cast<const cplx<T>*>(h->W);
     a.out = reinterpret_cast<cplx<T>*>(h->V);
     const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(h->tw);
-    a.twA = tw + h->tw_ra; a.twB = tw + h->tw_rb; a.rtw = tw + (h->packed ? h->rt4_off : h->rt_off);
+    a.twA = tw + h->tw_ra; a.twB = tw + h->tw_rb; a.rtw = tw + (h->packed_row ? h->rt4_off : h->rt_off);
     a.scal = h->scal;
     a.clamp = h->prob.clamp_log;
     a.g = h->prob.g; a.min_phi = h->prob.min_phi;
@@ -558,7 +622,7 @@ int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
     a.tma_box = table ? 0 : h->tma_box;   // a batch's plans each have their own W: copies
     void* args_pk[] = {(void*)&a, (void*)&h->tmap};
     void* args1[] = {(void*)&a};
-    void** args = h->packed ? args_pk : args1;
+    void** args = h->packed_row ? args_pk : args1;
     cudaError_t e = launch_step_kernel(h, h->fast_row_fn, dim3(h->fr_grid, count), dim3(h->fr_threads), args,
                                        h->fr_smem, s);
     ++h->launches;
@@ -1271,7 +1335,7 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
   }
   int rc = h->fp32 ? set_smem_attrs<float>(h) : set_smem_attrs<double>(h);
   if (rc) return cleanup_fail(rc);
-  if (h->packed && (p->flags & PFC_FLAG_TMA)) {
+  if (h->packed_row && (p->flags & PFC_FLAG_TMA)) {
     rc = setup_tma(h);
     if (rc) return cleanup_fail(rc);
   }
@@ -1393,7 +1457,8 @@ int pfc_plan_variant(pfc_plan* h, int32_t* o) {
   o[0] = h->fast ? h->ee_row : 0;
   o[1] = h->fast ? h->ee_col : 0;
   o[2] = h->fast ? h->fr_rows : 0;
-  o[3] = h->packed ? 2 : h->fast ? 1 : 0;
+  // fast: 1 one-lane kernels, 2 packed row and column, 3 packed row only, 4 packed column only
+  o[3] = !h->fast ? 0 : h->packed_row && h->packed_col ? 2 : h->packed_row ? 3 : h->packed_col ? 4 : 1;
   return PFC_OK;
 }
 
@@ -1426,7 +1491,7 @@ int pfc_batch_create(pfc_plan* const* plans, int32_t count, pfc_batch** out) {
       // (mixed-radix plans of one size and precision share the FFT description, twiddle
       // tables and launch shape, all of which come from plans[0] of the class)
       if (r->fast == h->fast && r->onecta == h->onecta && r->fast_row_fn == h->fast_row_fn &&
-          r->fast_col_fn == h->fast_col_fn && r->packed == h->packed && r->fr_rows == h->fr_rows &&
+          r->fast_col_fn == h->fast_col_fn && r->packed_row == h->packed_row && r->fr_rows == h->fr_rows &&
           r->fc_threads == h->fc_threads &&
           r->row_rset == h->row_rset && r->col_rset == h->col_rset && r->prob.model == h->prob.model &&
           r->nx == h->nx && r->ny == h->ny && r->prob.g == h->prob.g && r->prob.clamp_log == h->prob.clamp_log &&

@@ -364,8 +364,9 @@ def _kernel_flags(kernels, prob):
     the autotuner cached for this grid, else the defaults), "default", "generic" (the
     mixed-radix kernels everywhere), or a dict with any of "ee_row", "ee_col",
     "row_tile", "col_cta" (columns per CTA of the column kernel), "pdl" and "packed"
-    (the two-lane packed FP32 kernels; then ee_* count values per lane), "tma" (their row
-    tile staged by the tensor memory accelerator)."""
+    (1: the two-lane packed FP32 kernels on both passes, 2: row pass only, 3: column pass
+    only; ee_* of a packed pass count values per lane), "tma" (the packed row kernel's tile
+    staged by the tensor memory accelerator)."""
     if isinstance(kernels, dict):
         return _lib.flag_variant(**{k: kernels.get(k, 0) for k in ("ee_row", "ee_col", "row_tile", "col_cta",
                                                                     "pdl", "packed", "tma")})

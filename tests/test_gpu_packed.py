@@ -40,6 +40,15 @@ def test_packed_variants_match_generic(nx, ny):
                 sim.TimeSteps(8)
                 assert rel_l2(sim.State.n.get() + 0.3, ref + 0.3) < 1e-5, v
                 sim.plan.close()
+    # one pass packed, the other one-lane (16 values per lane / 32 per thread)
+    for packed, code in ((2, 3), (3, 4)):
+        v = {"ee_row": 16 if packed == 2 else 32, "ee_col": 16 if packed == 3 else 32, "packed": packed}
+        sim = stdpfc.BuildB200_Simulation(prm, geom, precision="fp32", kernels=v)
+        assert sim.plan.variant()["fast"] == code, v
+        sim.State.n[...] = f0
+        sim.TimeSteps(8)
+        assert rel_l2(sim.State.n.get() + 0.3, ref + 0.3) < 1e-5, v
+        sim.plan.close()
 
 
 @pytest.mark.parametrize("model", ["std", "log"])
