@@ -68,11 +68,13 @@ def test_extv_smoke_behaviour(golden):
 
 def test_extv_refuses_other_forms():
     from pfc_models_b200 import logpfc
+    from pfc_models_b200.simulation import Simulation
     geom = logpfc.Build2DGeometry(64, 64, 50.0, 50.0)
     prm = logpfc.BuildLogPFCModelParameters(beta=0.5, epsilon=-0.9, g=-2.0, dt=0.1)
-    with pytest.raises(_lib.PfcError) as e:
-        logpfc.Simulation(prm, geom, precision="fp32", clamp_log=True, _flags=_lib.FLAG_EXTV)
-    assert e.value.code == _lib.PFC_E_ARG
+    for precision, clamp in (("fp32", True), ("fp64", False)):
+        with pytest.raises(_lib.PfcError) as e:
+            Simulation("log", prm, geom, precision=precision, clamp_log=clamp, _flags=_lib.FLAG_EXTV)
+        assert e.value.code == _lib.PFC_E_ARG
     sim = logpfc.Simulation(prm, geom, precision="fp64", clamp_log=True)
     v = np.zeros(64 * 64)
     import torch
