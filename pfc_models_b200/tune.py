@@ -4,8 +4,9 @@
 
 For one grid, precision and model it times every built variant of the two step
 kernels (complex values per thread of the row and the column kernel, rows per
-CTA of the row kernel) with CUDA events on a seeded noisy-liquid state, and keeps
-the fastest row and the fastest column variant. A second stage times that choice
+CTA of the row kernel; in FP32 also the two-lane packed kernels of either pass, and
+the packed row kernel's TMA-staged tile) with CUDA events on a seeded noisy-liquid
+state, and keeps the fastest row and the fastest column variant. A second stage times that choice
 with 1, 2 and 4 columns per CTA of the column kernel, with and without programmatic
 dependent launch, over whole steps replayed from CUDA graphs, and keeps a change only
 where it is at least 1 % faster (`--refine` runs this stage alone on the entries the
@@ -31,7 +32,9 @@ PACKAGED = os.path.join(HERE, "tuned_b200.json")
 EE_CHOICES = {_lib.FP32_MIXED: (8, 16, 32), _lib.FP64_PLAIN: (8, 16)}
 TILE_CHOICES = (1, 2, 4, 8, 16)
 COL_CTA_CHOICES = (1, 2, 4)
-VARIANT_KEYS = ("ee_row", "ee_col", "row_tile", "col_cta", "pdl")
+VARIANT_KEYS = ("ee_row", "ee_col", "row_tile", "col_cta", "pdl", "packed", "tma")
+PACKED_EE = (8, 16)                 # values per lane of the two-lane packed FP32 kernels
+PACKED_TILES = (2, 4, 8, 16)
 _lock = threading.Lock()
 _memo: dict = {}
 
@@ -119,11 +122,18 @@ def tune(nx, ny, precision="fp32", model="std", steps=20, warmup=3, save=True, p
         mean = -0.3
     f0 = fields.GenerateNoisyLiquid(geom, mean, 0.01, seed=0)
     ees = EE_CHOICES[prec]
+    # row candidates (packed?, values per thread or lane, tile, TMA) and column candidates
+    # (packed?, values); each row candidate is timed beside the column candidates in turn
+    row_c = [(False, e, t, 0) for e, t in itertools.product(ees, TILE_CHOICES)]
+    col_c = [(False, e) for e in ees]
+    if prec == _lib.FP32_MIXED:
+        row_c += [(True, e, t, m) for e, t, m in itertools.product(PACKED_EE, PACKED_TILES, (0, 1))]
+        col_c += [(True, e) for e in PACKED_EE]
     rows, cols = {}, {}
-    combos = list(itertools.product(ees, TILE_CHOICES))
-    for i, (ee_r, tile) in enumerate(combos):
-        ee_c = ees[i % len(ees)]
-        variant = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile}
+    for i, (rp, ee_r, tile, tma) in enumerate(row_c):
+        cp, ee_c = col_c[i % len(col_c)]
+        packed = {(False, False): 0, (True, True): 1, (True, False): 2, (False, True): 3}[(rp, cp)]
+        variant = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile, "packed": packed, "tma": tma}
         sim = mod.BuildB200_Simulation(prm, geom, precision=precision, kernels=variant)
         v = sim.plan.variant()
         if not v["fast"]:
@@ -138,17 +148,20 @@ def tune(nx, ny, precision="fp32", model="std", steps=20, warmup=3, save=True, p
         sim.plan.close()
         if not ok:
             continue
-        rk = (v["ee_row"], v["row_tile"])
+        rk = (rp, v["ee_row"], v["row_tile"], tma)
         rows[rk] = min(rows.get(rk, math.inf), 1e3 * ms_r / steps)
-        cols.setdefault(v["ee_col"], []).append(1e3 * ms_c / steps)
+        cols.setdefault((cp, v["ee_col"]), []).append(1e3 * ms_c / steps)
     if not rows or not cols:
         return None
-    (ee_r, tile), row_us = min(rows.items(), key=lambda kv: kv[1])
+    (rp, ee_r, tile, tma), row_us = min(rows.items(), key=lambda kv: kv[1])
     col_avg = {k: sum(v) / len(v) for k, v in cols.items()}
-    ee_c, col_us = min(col_avg.items(), key=lambda kv: kv[1])
-    entry = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile, "row_us": row_us, "col_us": col_us,
-             "rows_us": {f"{a}/{b}": u for (a, b), u in sorted(rows.items())},
-             "cols_us": {str(k): u for k, u in sorted(col_avg.items())}}
+    (cp, ee_c), col_us = min(col_avg.items(), key=lambda kv: kv[1])
+    packed = {(False, False): 0, (True, True): 1, (True, False): 2, (False, True): 3}[(rp, cp)]
+    tag = lambda pk: "p" if pk else "s"  # noqa: E731
+    entry = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile, "packed": packed, "tma": tma if rp else 0,
+             "row_us": row_us, "col_us": col_us,
+             "rows_us": {f"{tag(a)}{b}/{c}/{d}": u for (a, b, c, d), u in sorted(rows.items())},
+             "cols_us": {f"{tag(a)}{b}": u for (a, b), u in sorted(col_avg.items())}}
     entry.update(refine(nx, ny, precision, model, entry))
     if save:
         _store(path or cache_path(), _key(_device_name(), nx, ny, prec,
@@ -253,7 +266,7 @@ def refine(nx, ny, precision, model, base, batch=1, min_gain=0.01):
     launch for the row/column variant in `base`, timed over whole steps. Returns
     {"col_cta", "pdl", "refine_us"}; keeps the defaults (0, 0) unless a choice is at
     least `min_gain` faster than they are."""
-    v0 = {k: int(base.get(k) or 0) for k in ("ee_row", "ee_col", "row_tile")}
+    v0 = {k: int(base.get(k) or 0) for k in ("ee_row", "ee_col", "row_tile", "packed", "tma")}
     timed, seen = {}, set()
     for cc in (0,) + COL_CTA_CHOICES:
         for pdl in (0, 1):

@@ -34,12 +34,12 @@ def test_user_cache_overrides_and_round_trips(tmp_path, monkeypatch):
     tune._memo.clear()
     assert json.load(open(path))[key]["ee_col"] == 32
     assert tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200") == \
-        {"ee_row": 16, "ee_col": 32, "row_tile": 2, "col_cta": 0, "pdl": 0}
+        {"ee_row": 16, "ee_col": 32, "row_tile": 2, "col_cta": 0, "pdl": 0, "packed": 0, "tma": 0}
     # entries of the second stage carry the column CTA width and the launch mode
     tune._store(str(path), key, {"ee_row": 16, "ee_col": 16, "row_tile": 4, "col_cta": 1, "pdl": 1})
     tune._memo.clear()
     assert tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200") == \
-        {"ee_row": 16, "ee_col": 16, "row_tile": 4, "col_cta": 1, "pdl": 1}
+        {"ee_row": 16, "ee_col": 16, "row_tile": 4, "col_cta": 1, "pdl": 1, "packed": 0, "tma": 0}
     tune._memo.clear()
 
 
@@ -52,6 +52,13 @@ def test_flag_encoding_matches_header():
     assert shifts == {"ROW_EE": "8", "COL_EE": "16", "ROW_TILE": "24"}
     assert _lib.flag_variant(16, 32, 4) == (16 << 8) | (32 << 16) | (4 << 24)
     assert re.search(r"#define PFC_FLAG_PDL 4\b", src)
+    # packed kernels: both passes by flag, one pass by the EE bit; TMA staging by flag
+    assert re.search(r"#define PFC_FLAG_PACKED 16\b", src) and re.search(r"#define PFC_EE_PACKED 0x80\b", src)
+    assert re.search(r"#define PFC_FLAG_TMA 64\b", src) and re.search(r"#define PFC_FLAG_EXTV 32\b", src)
+    assert _lib.flag_variant(16, 32, 4, packed=1) & _lib.FLAG_PACKED
+    assert (_lib.flag_variant(16, 32, 4, packed=2) >> 8) & 0xff == 16 | _lib.EE_PACKED
+    assert (_lib.flag_variant(16, 16, 4, packed=3) >> 16) & 0xff == 16 | _lib.EE_PACKED
+    assert _lib.flag_variant(16, 32, 8, packed=2, tma=1) & _lib.FLAG_TMA
     assert re.search(r"#define PFC_FLAG_COL_CTA\(c\) .*<< 29\)", src)
     # columns per CTA 1, 2, 4 -> field values 1, 2, 3 in bits 29-30
     assert [_lib.flag_variant(col_cta=c) >> 29 for c in (0, 1, 2, 4)] == [0, 1, 2, 3]
