@@ -326,6 +326,15 @@ int pfc_extv_state(pfc_plan* plan, double* host_out6);
 /* Sets State.phi_floor_tol / State.phi_ceiling_tol (models/logpfc_extv/simulation.py:143-144). */
 int pfc_extv_set_tolerances(pfc_plan* plan, double floor_tol, double ceiling_tol);
 
+/* Testing the bounded device wait (no counterpart in the reference, whose CuPy path has
+ * no device waits): on a plan whose row pass stages its tile by TMA (PFC_FLAG_TMA), the
+ * following steps make that pass's mbarrier expect `extra_bytes` more than the tile
+ * (a multiple of 16, 0 restores the normal count), so its wait runs out after
+ * `wait_limit` polls (0: the default limit); the pass then leaves without computing and
+ * sets PFC_STATUS_TIMEOUT, which pfc_status reads, and the context stays usable. The
+ * plan's recorded graphs are dropped so the next steps use the new arguments. */
+int pfc_test_tma_wait(pfc_plan* plan, int32_t extra_bytes, int32_t wait_limit);
+
 #ifdef __cplusplus
 }
 #endif

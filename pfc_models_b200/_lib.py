@@ -79,6 +79,7 @@ SIGNATURES = {
     "pfc_set_potential": (ctypes.c_int, [_vp, _vp, _vp]),
     "pfc_extv_state": (ctypes.c_int, [_vp, ctypes.POINTER(_dbl)]),
     "pfc_extv_set_tolerances": (ctypes.c_int, [_vp, _dbl, _dbl]),
+    "pfc_test_tma_wait": (ctypes.c_int, [_vp, _i32, _i32]),
 }
 
 

@@ -185,6 +185,8 @@ struct FastRowArgs {
   double g, min_phi, min_log;
   int tma_box;               // packed row kernel: kx extent of a TMA box (0: asynchronous copies)
   int* err;                  // status word; a bounded wait that gave up ORs PFC_STATUS_TIMEOUT
+  unsigned tma_extra_tx;     // bytes the TMA barrier expects beyond the tile (0; a test sets more)
+  int tma_wait_limit;        // polls of that barrier before giving up (0: the default)
 };
 
 template <class T>

@@ -194,7 +194,7 @@ row_step_pk(FastRowArgs<float> a, const __grid_constant__ CUtensorMap tmap) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      const unsigned bytes = (unsigned)M * (unsigned)ib;
+      const unsigned bytes = (unsigned)M * (unsigned)ib + a.tma_extra_tx;
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
       const unsigned base = raw_s + pad_s;
       // x (the innermost coordinate, rows) = y0 is even: 16-byte aligned; kx is the outer one
@@ -207,7 +207,8 @@ row_step_pk(FastRowArgs<float> a, const __grid_constant__ CUtensorMap tmap) {
       }
     }
     unsigned done = 0;
-    for (long long it = 0; !done && it < kTmaWaitLimit; ++it) {
+    const long long limit = a.tma_wait_limit > 0 ? a.tma_wait_limit : kTmaWaitLimit;
+    for (long long it = 0; !done && it < limit; ++it) {
       asm volatile(
           "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
           "selp.u32 %0, 1, 0, p;\n\t}"
@@ -216,7 +217,8 @@ row_step_pk(FastRowArgs<float> a, const __grid_constant__ CUtensorMap tmap) {
           : "memory");
     }
     if (!done) {
-      // the boxes did not arrive within the limit: report and leave (nothing else reads them)
+      // the barrier did not complete within the limit: report and leave (nothing else reads
+      // the tile; the boxes themselves were issued before the wait)
       if (threadIdx.x == 0 && a.err) atomicOr(a.err, (int)kStatusTimeout);
       return;
     }

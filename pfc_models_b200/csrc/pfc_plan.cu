@@ -182,6 +182,8 @@ struct pfc_plan {
   int rt4_off = 0;             // packed kernels: offset of the float4 real-packing table in tw
   int tma_box = 0;             // packed row kernel staged by TMA: kx extent of a box (0: cp.async)
   CUtensorMap tmap{};          // its tensor map of W ([kx][y], 8-byte elements)
+  unsigned tma_extra_tx = 0;   // pfc_test_tma_wait: bytes its barrier waits for beyond the tile
+  int tma_wait_limit = 0;      //   and the polls before it gives up
   int fc_threads = 0, fc_grid = 0;
   size_t fr_smem = 0, fc_smem = 0;
   int tw_ra = 0, tw_rb = 0, tw_ca = 0, tw_cb = 0;  // table offsets (complex elements)
@@ -620,6 +622,8 @@ int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
     a.min_log = (h->prob.min_phi > 0) ? std::log(h->prob.min_phi) : -INFINITY;
     a.err = h->status;
     a.tma_box = table ? 0 : h->tma_box;   // a batch's plans each have their own W: copies
+    a.tma_extra_tx = h->tma_extra_tx;
+    a.tma_wait_limit = h->tma_wait_limit;
     void* args_pk[] = {(void*)&a, (void*)&h->tmap};
     void* args1[] = {(void*)&a};
     void** args = h->packed_row ? args_pk : args1;
@@ -1811,5 +1815,20 @@ extern "C" int pfc_extv_set_tolerances(pfc_plan* h, double floor_tol, double cei
   st.floor_tol = floor_tol;
   st.ceil_tol = ceiling_tol;
   PFC_CUDA(cudaMemcpy(h->extv_st, &st, sizeof(st), cudaMemcpyHostToDevice));
+  return PFC_OK;
+}
+
+extern "C" int pfc_test_tma_wait(pfc_plan* h, int32_t extra_bytes, int32_t wait_limit) {
+  if (!h) return fail(PFC_E_ARG, "pfc_test_tma_wait: null plan");
+  if (!h->tma_box) return fail(PFC_E_ARG, "pfc_test_tma_wait: the plan's row pass is not staged by TMA");
+  if (extra_bytes < 0 || extra_bytes % 16 || wait_limit < 0)
+    return fail(PFC_E_ARG, "pfc_test_tma_wait: extra bytes must be a non-negative multiple of 16, limit >= 0");
+  h->tma_extra_tx = (unsigned)extra_bytes;
+  h->tma_wait_limit = wait_limit;
+  // graphs recorded with the old arguments would replay them
+  for (auto& g : h->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto& g : h->graph1)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   return PFC_OK;
 }

@@ -121,3 +121,32 @@ def test_tma_staged_tile_matches_copies(nx, ny):
             assert sim.plan.status() == 0
             sim.plan.close()
         assert np.array_equal(out[0], out[1]), tile
+
+
+def test_tma_wait_runs_out_and_reports():
+    """The TMA-staged row pass waits on its mbarrier a bounded number of polls. With the
+    barrier made to expect 16 bytes more than the tile (pfc_test_tma_wait), the wait runs
+    out, the pass leaves without computing and sets PFC_STATUS_TIMEOUT; the context stays
+    usable and, with the normal count restored, a new plan steps exactly as before."""
+    from pfc_models_b200 import _lib
+    prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.3, g=0.0, dt=0.5)
+    geom = stdpfc.Build2DGeometry(512, 256, 128 * np.pi, 64 * np.pi)
+    f0 = -0.3 + 0.05 * np.random.default_rng(9).uniform(-1, 1, (256, 512))
+    v = {"packed": 2, "ee_row": 16, "ee_col": 16, "row_tile": 8, "tma": 1}
+    ref = stdpfc.BuildB200_Simulation(prm, geom, precision="fp32", kernels=v)
+    ref.State.n[...] = f0
+    ref.TimeSteps(3)
+    sim = stdpfc.BuildB200_Simulation(prm, geom, precision="fp32", kernels=v)
+    sim.State.n[...] = f0
+    lib, h = sim.plan.lib, sim.plan.handle
+    _lib.check(lib.pfc_test_tma_wait(h, 16, 1 << 12))
+    sim.TimeSteps(1)
+    assert sim.plan.status() & _lib.STATUS_TIMEOUT
+    _lib.check(lib.pfc_test_tma_wait(h, 0, 0))
+    again = stdpfc.BuildB200_Simulation(prm, geom, precision="fp32", kernels=v)
+    again.State.n[...] = f0
+    again.TimeSteps(3)
+    assert again.plan.status() == 0
+    assert np.array_equal(again.State.n.get(), ref.State.n.get())
+    with pytest.raises(_lib.PfcError):
+        _lib.check(lib.pfc_test_tma_wait(h, 8, 0))
