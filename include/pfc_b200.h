@@ -192,6 +192,9 @@ int pfc_plan_variant(pfc_plan* plan, int32_t* out4);
 #define PFC_PATH_MIXED_RADIX 0
 #define PFC_PATH_POW2 1
 #define PFC_PATH_ONE_CTA 2
+#define PFC_PATH_FAST_MIXED 3   /* the register-resident step kernels on a grid whose sides
+                                   are N = ODD * 2^k (ODD = 3, 5, 7; 2^k = 16 .. 512) or
+                                   powers of two, not both powers of two */
 int pfc_plan_path(pfc_plan* plan, int32_t* path);
 
 /* Kernel launches issued by this plan since creation (for accounting). */

@@ -25,7 +25,7 @@ FLAG_NO_ONE_CTA = 8
 FLAG_PACKED = 16
 FLAG_EXTV = 32
 FLAG_TMA = 64
-PATH_MIXED_RADIX, PATH_POW2, PATH_ONE_CTA = 0, 1, 2
+PATH_MIXED_RADIX, PATH_POW2, PATH_ONE_CTA, PATH_FAST_MIXED = 0, 1, 2, 3
 STATUS_NONFINITE = 1
 STATUS_TIMEOUT = 2
 

@@ -24,17 +24,31 @@
 
 namespace pfc {
 
+// Radix sequence of an N-point transform held EE values per thread. N = ODD * 2^K2 with
+// ODD = 1, 3, 5 or 7: EE_REQ is then the power-of-two part of the values per thread
+// (EE = ODD * E2), sequence A runs the radix-RC passes of the power-of-two part (the last
+// of them radix LAST2) and then one radix-ODD pass, sequence B the same in reverse, so
+// that every radix divides EE (each pass gives a thread EE / R whole butterflies) and the
+// last pass of A and the first of B still touch the same elements in the same thread.
 template <int N, int EE_REQ, int RMAX>
 struct FastSeq {
   __host__ __device__ static constexpr int lg(int x) { return x <= 1 ? 0 : 1 + lg(x >> 1); }
-  static constexpr int EE = EE_REQ < N ? EE_REQ : N;     // elements per thread
+  __host__ __device__ static constexpr int ctz(int x) { return (x & 1) ? 0 : 1 + ctz(x >> 1); }
+  static constexpr int K2 = ctz(N), ODD = N >> K2;        // N = ODD * 2^K2
+  static constexpr int P2 = 1 << K2;
+  static constexpr int E2 = EE_REQ < P2 ? EE_REQ : P2;    // power-of-two part of the values per thread
+  static constexpr int EE = ODD * E2;                     // elements per thread
   static constexpr int TPF = N / EE;                      // threads per transform
-  static constexpr int RC = RMAX < EE ? RMAX : EE;        // radix of the full passes
-  static constexpr int LN = lg(N), LE = lg(RC);
-  static constexpr int NPASS = (LN + LE - 1) / LE;
-  static constexpr int LAST = 1 << (LN - (NPASS - 1) * LE);
-  __host__ __device__ static constexpr int radA(int p) { return p == NPASS - 1 ? LAST : RC; }
-  __host__ __device__ static constexpr int radB(int p) { return p == 0 ? LAST : RC; }
+  static constexpr int RC = RMAX < E2 ? RMAX : E2;        // radix of the full power-of-two passes
+  static constexpr int LN = K2, LE = lg(RC);
+  static constexpr int NP2 = LE > 0 ? (LN + LE - 1) / LE : 0;
+  static constexpr int LAST2 = NP2 > 0 ? 1 << (LN - (NP2 - 1) * LE) : 1;
+  static constexpr int NPASS = NP2 + (ODD > 1 ? 1 : 0);
+  static constexpr int LAST = ODD > 1 ? ODD : LAST2;      // radix of A's last (B's first) pass
+  __host__ __device__ static constexpr int radA(int p) {
+    return p == NPASS - 1 ? LAST : (p == NP2 - 1 ? LAST2 : RC);
+  }
+  __host__ __device__ static constexpr int radB(int p) { return radA(NPASS - 1 - p); }
   __host__ __device__ static constexpr int nsA(int p) { return p == 0 ? 1 : nsA(p - 1) * radA(p - 1); }
   __host__ __device__ static constexpr int nsB(int p) { return p == 0 ? 1 : nsB(p - 1) * radB(p - 1); }
   // offset of pass p's twiddle table ([q-1][k], q < R, k < ns) within the sequence table
@@ -85,12 +99,13 @@ __device__ __forceinline__ void group_sync(int g) {
 // TPF threads holding EE = R * NB values each (v[b * R + q], butterfly j = t + b * TPF).
 template <class T, int N, int EE, int R, int NS, int P>
 struct FastPass {
-  static_assert(R <= (1 << P), "a butterfly's consecutive outputs must not straddle a pad");
+  static_assert(R <= (1 << P), "the padded exchange assumes radices up to 2^P");
   static constexpr int TPF = N / EE, NB = EE / R, NR = N / R;
   // padi(x + q * S) = padi(x) + q * (S + S / 2^P) whenever 2^P divides S
   static constexpr int NRP = NR + (NR >> P);
   static constexpr bool LIN_LOAD = (NR % (1 << P)) == 0;
-  static constexpr bool LIN_STORE = (NS % (1 << P)) == 0 || NS == 1;
+  // the R consecutive outputs of an NS = 1 pass stay inside one pad block when R divides 2^P
+  static constexpr bool LIN_STORE = (NS % (1 << P)) == 0 || (NS == 1 && ((1 << P) % R) == 0);
   static constexpr int NSP = NS == 1 ? 1 : NS + (NS >> P);
   static __device__ __forceinline__ void load(const cplx<T>* buf, cplx<T>* v, int t) {
 #pragma unroll
@@ -125,7 +140,7 @@ struct FastPass {
           v[b * R + q] = cmul(v[b * R + q], x);
         }
       }
-      dft<R, INV>(v + b * R, (const cplx<T>*)nullptr);
+      dft_c<R, INV>(v + b * R);
     }
   }
   // NS == 1: the R outputs of a butterfly are consecutive and R divides 2^P, so they
@@ -503,7 +518,8 @@ col_step_fast(FastColArgs<T> a) {
     // states of a whole chunk are loaded before any of its results is stored (the
     // compiler may not move a load above an earlier store to memory it cannot tell
     // apart), so the chunk's loads are in flight together.
-    constexpr int CH = (sizeof(T) == 4 && EE >= 16) ? 8 : 4;   // within the 64-register budget
+    // within the 64-register budget, and dividing EE (mixed-radix transforms hold 24 or 28)
+    constexpr int CH = (sizeof(T) == 4 && EE >= 16 && EE % 8 == 0) ? 8 : (EE % 4 == 0 ? 4 : 2);
     static_assert(EE % CH == 0, "chunks tile the modes of a thread");
 #pragma unroll 1
     for (int j0 = 0; j0 < EE; j0 += CH) {

@@ -184,6 +184,53 @@ template <int R, bool INV, class T> __device__ __forceinline__ void dft(cplx<T>*
   else dft_odd<R, INV>(v, roots);
 }
 
+// Odd-radix DFT with compile-time roots (R = 5 or 7): cos and sin of 2 pi m / R are
+// literal constants (to 20 digits) instead of a table in memory; the same
+// (s, d)-symmetric evaluation as dft_odd.
+template <int R> __device__ __forceinline__ double root_cos(int m) {
+  if (R == 5) return m == 1 ? 0.30901699437494742410 : -0.80901699437494742410;
+  // R == 7
+  return m == 1 ? 0.62348980185873353053 : m == 2 ? -0.22252093395631440429 : -0.90096886790241912624;
+}
+template <int R> __device__ __forceinline__ double root_sin(int m) {
+  if (R == 5) return m == 1 ? 0.95105651629515357212 : 0.58778525229247312917;
+  return m == 1 ? 0.78183148246802980871 : m == 2 ? 0.97492791218182360702 : 0.43388373911755812048;
+}
+template <int R, bool INV, class T> __device__ __forceinline__ void dft_odd_c(cplx<T>* v) {
+  constexpr int H = (R - 1) / 2;
+  cplx<T> s[H + 1], d[H + 1];
+#pragma unroll
+  for (int b = 1; b <= H; ++b) { s[b] = v[b] + v[R - b]; d[b] = v[b] - v[R - b]; }
+  const cplx<T> v0 = v[0];
+  cplx<T> tot = v0;
+#pragma unroll
+  for (int b = 1; b <= H; ++b) tot = tot + s[b];
+#pragma unroll
+  for (int a = 1; a <= H; ++a) {
+    cplx<T> A = v0, B = mk(T(0), T(0));
+#pragma unroll
+    for (int b = 1; b <= H; ++b) {
+      const int t = (a * b) % R;
+      const T c = (T)root_cos<R>(t <= H ? t : R - t);
+      const T sg = (T)(t <= H ? root_sin<R>(t) : -root_sin<R>(R - t));
+      A = A + c * s[b];
+      B = B + sg * d[b];
+    }
+    // forward: y_a = A - i B, y_{R-a} = A + i B; inverse swaps the signs
+    const cplx<T> iB = mul_i(B);
+    v[a] = INV ? A + iB : A - iB;
+    v[R - a] = INV ? A - iB : A + iB;
+  }
+  v[0] = tot;
+}
+
+// DFT of a compile-time radix without a root table (powers of two up to 32, 3, 5, 7).
+template <int R, bool INV, class T> __device__ __forceinline__ void dft_c(cplx<T>* v) {
+  if constexpr (R == 1) return;
+  else if constexpr (R == 5 || R == 7) dft_odd_c<R, INV>(v);
+  else dft<R, INV>(v, (const cplx<T>*)nullptr);
+}
+
 // Elements a thread may hold in registers during one pass.
 template <class T> struct MaxElems { static constexpr int value = PFC_MAXE_F; };
 template <> struct MaxElems<double> { static constexpr int value = PFC_MAXE_D; };

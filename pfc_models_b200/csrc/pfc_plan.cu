@@ -365,9 +365,14 @@ struct FastColSide {
 template <class T>
 int fast_row_side(pfc_plan* h, int ee, int tile, std::vector<long double>& tw, FastRowSide& o) {
   const int lm = ilog2_exact(h->m);
-  if (lm < kFastMinLog || lm > kFastMaxLogRow) return PFC_OK;
   FastKernel kr;
-  if (!fast_lookup<T>(false, lm, ee, h->prob.model, &kr)) return PFC_OK;
+  if (lm >= 0) {
+    if (lm < kFastMinLog || lm > kFastMaxLogRow || !fast_lookup<T>(false, lm, ee, h->prob.model, &kr)) return PFC_OK;
+  } else {
+    // one odd factor: the kernel's values per thread are fixed by the transform length
+    if (!MixInst<T>::row(h->m, h->prob.model, &kr)) return PFC_OK;
+    ee = h->m / kr.tpf;
+  }
   // pad shift of the row tile as the kernel uses it (for length / threads per transform)
   const int P = fast_pad_shift(sizeof(T) == 8, h->m / kr.tpf);
   const int elt = (int)sizeof(cplx<T>);
@@ -394,7 +399,8 @@ int fast_row_side(pfc_plan* h, int ee, int tile, std::vector<long double>& tw, F
   o.smem = smem;
   o.fn = kr.fn;
   o.ee = ee;
-  fast_seq_tables<T>(lm, ee, tw, o.tw_a, o.tw_b);
+  if (lm >= 0) fast_seq_tables<T>(lm, ee, tw, o.tw_a, o.tw_b);
+  else MixInst<T>::tables(h->m, tw, o.tw_a, o.tw_b);
   o.ok = true;
   return PFC_OK;
 }
@@ -403,15 +409,20 @@ int fast_row_side(pfc_plan* h, int ee, int tile, std::vector<long double>& tw, F
 template <class T>
 int fast_col_side(pfc_plan* h, int ee, int col_cta, std::vector<long double>& tw, FastColSide& o) {
   const int ly = ilog2_exact(h->ny);
-  if (ly < kFastMinLog || ly > kFastMaxLogCol) return PFC_OK;
   FastKernel kc;
-  if (!fast_lookup<T>(true, ly, ee, h->prob.model, &kc)) return PFC_OK;
+  if (ly >= 0) {
+    if (ly < kFastMinLog || ly > kFastMaxLogCol || !fast_lookup<T>(true, ly, ee, h->prob.model, &kc)) return PFC_OK;
+  } else {
+    if (!MixInst<T>::col(h->ny, &kc)) return PFC_OK;
+    ee = h->ny / kc.tpf;
+  }
   const int Pc = fast_pad_shift(sizeof(T) == 8, h->ny / kc.tpf);
   const int elt = (int)sizeof(cplx<T>);
   const int tpc = kc.tpf;
   // (the kernels are built for at most 256 threads per CTA, or one group if larger)
   const int ngc_max = std::max(1, 256 / tpc);
-  const int ngc = std::min(col_cta ? std::min(col_cta, ngc_max) : ngc_max, h->m);
+  int ngc = std::min(col_cta ? std::min(col_cta, ngc_max) : ngc_max, h->m);
+  while (h->m % ngc) ngc /= 2;
   const size_t smem = (size_t)ngc * (h->ny + (h->ny >> Pc) + 2) * elt;   // one exchange buffer per column
   if (ngc * tpc > 1024 || smem > 200 * 1024) return PFC_OK;
   o.threads = ngc * tpc;
@@ -419,7 +430,8 @@ int fast_col_side(pfc_plan* h, int ee, int col_cta, std::vector<long double>& tw
   o.smem = smem;
   o.fn = kc.fn;
   o.ee = ee;
-  fast_seq_tables<T>(ly, ee, tw, o.tw_a, o.tw_b);
+  if (ly >= 0) fast_seq_tables<T>(ly, ee, tw, o.tw_a, o.tw_b);
+  else MixInst<T>::tables(h->ny, tw, o.tw_a, o.tw_b);
   o.ok = true;
   return PFC_OK;
 }
@@ -1468,7 +1480,9 @@ int pfc_plan_variant(pfc_plan* h, int32_t* o) {
 
 int pfc_plan_path(pfc_plan* h, int32_t* path) {
   if (!h || !path) return fail(PFC_E_ARG, "pfc_plan_path: null argument");
-  *path = h->onecta ? PFC_PATH_ONE_CTA : h->fast ? PFC_PATH_POW2 : PFC_PATH_MIXED_RADIX;
+  *path = h->onecta ? PFC_PATH_ONE_CTA
+          : h->fast ? ((ilog2_exact(h->m) >= 0 && ilog2_exact(h->ny) >= 0) ? PFC_PATH_POW2 : PFC_PATH_FAST_MIXED)
+                    : PFC_PATH_MIXED_RADIX;
   return PFC_OK;
 }
 

@@ -40,6 +40,17 @@ struct FastInst {
   static bool tables(int lg, std::vector<long double>& tw, int& offA, int& offB);
 };
 
+// Register-resident step kernels for transforms of N = ODD * 2^k points, ODD = 3, 5, 7
+// and k = kMixMinLog2 .. kMixMaxLog2 (pfc_fastmix_inst.cuh), by transform length.
+constexpr int kMixMinLog2 = 4, kMixMaxLog2 = 9;
+template <class T>
+struct MixInst {
+  static bool row(int n, int model, FastKernel* out);
+  static bool col(int n, FastKernel* out);
+  static bool tables(int n, std::vector<long double>& tw, int& offA, int& offB);
+  static int values_per_thread(int n);
+};
+
 // Two-lane packed FP32 step kernels (pfc_pack_step.cuh), `ee` = 8 or 16 complex values
 // per lane and thread: row transforms of 2^lg points (M = nx/2), column transforms of
 // 2^lg points (ny). Their pass tables are float4 entries (c, c, s, s), appended to `tw`

@@ -143,10 +143,11 @@ class Plan:
         return int(self.lib.pfc_launch_count(self.handle))
 
     def path(self):
-        """'mixed_radix', 'pow2' or 'one_cta': the step kernels this plan uses."""
+        """'mixed_radix', 'pow2', 'fast_mixed' or 'one_cta': the step kernels this plan uses."""
         v = ctypes.c_int32(0)
         _lib.check(self.lib.pfc_plan_path(self.handle, ctypes.byref(v)))
-        return {_lib.PATH_MIXED_RADIX: "mixed_radix", _lib.PATH_POW2: "pow2", _lib.PATH_ONE_CTA: "one_cta"}[v.value]
+        return {_lib.PATH_MIXED_RADIX: "mixed_radix", _lib.PATH_POW2: "pow2", _lib.PATH_ONE_CTA: "one_cta",
+                _lib.PATH_FAST_MIXED: "fast_mixed"}[v.value]
 
     def variant(self):
         """{"ee_row", "ee_col", "row_tile", "fast"} of the step kernels this plan uses."""

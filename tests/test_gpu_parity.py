@@ -458,7 +458,8 @@ def test_mixed_radix_tiles_leave_no_sm_idle(nx, ny):
     n_sm = torch.cuda.get_device_properties(0).multi_processor_count
     prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.25, g=0.0, dt=0.5)
     for precision in ("fp32", "fp64"):
-        sim = stdpfc.BuildB200_Simulation(prm, stdpfc.Build2DGeometry(nx, ny, nx * 0.8, ny * 0.8), precision=precision)
+        sim = stdpfc.BuildB200_Simulation(prm, stdpfc.Build2DGeometry(nx, ny, nx * 0.8, ny * 0.8), precision=precision,
+                                          kernels="generic")
         info = sim.plan.info()
         assert info["fast"] == 0
         rows_min = max(1, 32 // info["row_threads_per_fft"])
@@ -466,3 +467,43 @@ def test_mixed_radix_tiles_leave_no_sm_idle(nx, ny):
         assert info["row_ctas"] >= 2 * n_sm or info["rows_per_cta"] == rows_min, info
         assert info["col_ctas"] >= 2 * n_sm or info["cols_per_cta"] == cols_min, info
         sim.plan.close()
+
+
+MIX_SIZES = [(96, 80), (160, 112), (448, 448), (256, 384), (1792, 1792), (3072, 48)]
+
+
+@pytest.mark.parametrize("nx,ny", MIX_SIZES)
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_register_resident_mixed_radix_against_oracle(nx, ny, precision):
+    """Grids whose sides have one odd factor (3, 5 or 7 times 16 .. 512, or powers of two)
+    step with the register-resident kernels (compile-time radix sequences ending in the
+    odd radix); 20 steps of both models within 1e-12 (FP64) / 2e-5 (FP32-mixed) relative
+    L2 of the oracle, as the other sizes."""
+    geom_o = orc.build_geometry(nx, ny, nx * 0.9, ny * 0.8)
+    for model in ("std", "log"):
+        if model == "std":
+            prm = dict(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.25, g=0.3, dt=0.2)
+            mean = -0.2
+        else:
+            prm = dict(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=0.05)
+            mean = 0.55
+        f0 = mean + 0.05 * np.random.default_rng(nx + ny).uniform(-1, 1, (ny, nx))
+        ref, _ = orc.run(model, orc.Params(**prm), geom_o, f0, 20)
+        mod = stdpfc if model == "std" else logpfc
+        builder = mod.BuildStdPFCModelParameters if model == "std" else mod.BuildLogPFCModelParameters
+        sim = mod.BuildB200_Simulation(builder(**prm), mod.Build2DGeometry(nx, ny, nx * 0.9, ny * 0.8),
+                                       precision=precision)
+        assert sim.plan.path() == "fast_mixed", (model, sim.plan.path())
+        field = sim.State.n if model == "std" else sim.State.phi
+        field[...] = f0
+        sim.TimeSteps(20)
+        tol = 1e-12 if precision == "fp64" else 2e-5
+        assert rel_l2(field.get() - mean, ref - mean) < tol, model
+        assert float(sim.CalculateFreeEnergy()) == pytest.approx(orc_F(model, prm, geom_o, ref), rel=1e-10 if
+                                                                  precision == "fp64" else 1e-6)
+
+
+def orc_F(model, prm, geom, field):
+    s = orc.OracleSim(model, orc.Params(**prm), geom)
+    s.set_field(field)
+    return s.free_energy()
