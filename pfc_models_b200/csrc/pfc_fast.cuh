@@ -127,7 +127,7 @@ struct FastPass {
     for (int b = 0; b < NB; ++b) {
       if constexpr (NS > 1) {
         const int j = t + b * TPF;
-        const int k = j & (NS - 1);
+        const int k = j % NS;   // NS need not be a power of two (mixed sequences)
         // table [q-1][k]: consecutive lanes read consecutive entries
         const cplx<T>* w = tw + k;
         cplx<T> wq[R];
@@ -149,7 +149,7 @@ struct FastPass {
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
       const int j = t + b * TPF;
-      const int k = j & (NS - 1);
+      const int k = j % NS;   // NS need not be a power of two (mixed sequences)
       const int base = (j - k) * R + k;
       if constexpr (LIN_STORE) {
         cplx<T>* p = buf + padi<P>(base);

@@ -68,7 +68,7 @@ struct PkPass {
     for (int b = 0; b < NB; ++b) {
       if constexpr (NS > 1) {
         const int j = t + b * TPF;
-        const int k = j & (NS - 1);
+        const int k = j % NS;   // NS need not be a power of two (mixed sequences)
         const float4* w = tw + k;
         float4 wq[R];
 #pragma unroll
@@ -84,7 +84,7 @@ struct PkPass {
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
       const int j = t + b * TPF;
-      const int k = j & (NS - 1);
+      const int k = j % NS;   // NS need not be a power of two (mixed sequences)
       const int base = (j - k) * R + k;
       if constexpr (LIN_STORE) {
         float4* p = buf + padi<P>(base);
