@@ -34,17 +34,18 @@ EE_PACKED = 0x80
 PACKED_NONE, PACKED_BOTH, PACKED_ROW, PACKED_COL = 0, 1, 2, 3
 
 
-def flag_variant(ee_row=0, ee_col=0, row_tile=0, col_cta=0, pdl=0, packed=0, tma=0):
+def flag_variant(ee_row=0, ee_col=0, row_tile=0, col_cta=0, pdl=0, packed=0, tma=0, generic=0):
     """problem.flags bits selecting a step-kernel variant (PFC_FLAG_ROW_EE & co.).
     `packed`: 0 one-lane kernels, 1 the two-lane packed FP32 kernels on both passes,
     2 on the row pass only, 3 on the column pass only (then ee_* of a packed pass count
-    values per lane)."""
+    values per lane). `generic`: the run-time mixed-radix kernels instead."""
     cc = {0: 0, 1: 1, 2: 2, 4: 3}[int(col_cta)]
     packed = int(packed)
     er = int(ee_row) | (EE_PACKED if packed == PACKED_ROW else 0)
     ec = int(ee_col) | (EE_PACKED if packed == PACKED_COL else 0)
     return (er << 8) | (ec << 16) | (int(row_tile) << 24) | (cc << 29) | \
-        (FLAG_PDL if pdl else 0) | (FLAG_PACKED if packed == PACKED_BOTH else 0) | (FLAG_TMA if tma else 0)
+        (FLAG_PDL if pdl else 0) | (FLAG_PACKED if packed == PACKED_BOTH else 0) | (FLAG_TMA if tma else 0) | \
+        (FLAG_GENERIC_ONLY if generic else 0)
 
 # every symbol include/pfc_b200.h declares, with (restype, argtypes)
 _vp, _i32, _i64, _dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double

@@ -370,7 +370,7 @@ def _kernel_flags(kernels, prob):
     staged by the tensor memory accelerator)."""
     if isinstance(kernels, dict):
         return _lib.flag_variant(**{k: kernels.get(k, 0) for k in ("ee_row", "ee_col", "row_tile", "col_cta",
-                                                                    "pdl", "packed", "tma")})
+                                                                    "pdl", "packed", "tma", "generic")})
     if kernels == "generic":
         return _lib.FLAG_GENERIC_ONLY
     if kernels == "default":

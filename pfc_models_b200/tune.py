@@ -32,7 +32,7 @@ PACKAGED = os.path.join(HERE, "tuned_b200.json")
 EE_CHOICES = {_lib.FP32_MIXED: (8, 16, 32), _lib.FP64_PLAIN: (8, 16)}
 TILE_CHOICES = (1, 2, 4, 8, 16)
 COL_CTA_CHOICES = (1, 2, 4)
-VARIANT_KEYS = ("ee_row", "ee_col", "row_tile", "col_cta", "pdl", "packed", "tma")
+VARIANT_KEYS = ("ee_row", "ee_col", "row_tile", "col_cta", "pdl", "packed", "tma", "generic")
 PACKED_EE = (8, 16)                 # values per lane of the two-lane packed FP32 kernels
 PACKED_TILES = (2, 4, 8, 16)
 _lock = threading.Lock()
@@ -268,6 +268,11 @@ def refine(nx, ny, precision, model, base, batch=1, min_gain=0.01):
     least `min_gain` faster than they are."""
     v0 = {k: int(base.get(k) or 0) for k in ("ee_row", "ee_col", "row_tile", "packed", "tma")}
     timed, seen = {}, set()
+    # sides with an odd factor: the register-resident kernels hold a fixed number of values
+    # per thread, and on small or skinny grids the run-time mixed-radix kernels can be faster
+    generic_us = None
+    if nx & (nx - 1) or ny & (ny - 1):
+        generic_us, _ = _time_blocks(nx, ny, precision, model, {"generic": 1}, batch)
     for cc in (0,) + COL_CTA_CHOICES:
         for pdl in (0, 1):
             us, threads = _time_blocks(nx, ny, precision, model, dict(v0, col_cta=cc, pdl=pdl), batch,
@@ -281,8 +286,12 @@ def refine(nx, ny, precision, model, base, batch=1, min_gain=0.01):
     best = min(timed.items(), key=lambda kv: kv[1])
     if best[1] > (1 - min_gain) * timed[(0, 0)]:
         best = ((0, 0), timed[(0, 0)])
-    (cc, pdl), _ = best
-    return {"col_cta": cc, "pdl": pdl, "refine_us": {f"{a}/{b}": u for (a, b), u in sorted(timed.items())}}
+    (cc, pdl), best_us = best
+    out = {"col_cta": cc, "pdl": pdl, "refine_us": {f"{a}/{b}": u for (a, b), u in sorted(timed.items())}}
+    if generic_us is not None:
+        out["generic_us"] = generic_us
+        out["generic"] = 1 if generic_us < (1 - min_gain) * best_us else 0
+    return out
 
 
 def refine_table(path_in, device_name, steps=320):

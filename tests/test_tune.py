@@ -34,12 +34,12 @@ def test_user_cache_overrides_and_round_trips(tmp_path, monkeypatch):
     tune._memo.clear()
     assert json.load(open(path))[key]["ee_col"] == 32
     assert tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200") == \
-        {"ee_row": 16, "ee_col": 32, "row_tile": 2, "col_cta": 0, "pdl": 0, "packed": 0, "tma": 0}
+        {"ee_row": 16, "ee_col": 32, "row_tile": 2, "col_cta": 0, "pdl": 0, "packed": 0, "tma": 0, "generic": 0}
     # entries of the second stage carry the column CTA width and the launch mode
     tune._store(str(path), key, {"ee_row": 16, "ee_col": 16, "row_tile": 4, "col_cta": 1, "pdl": 1})
     tune._memo.clear()
     assert tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200") == \
-        {"ee_row": 16, "ee_col": 16, "row_tile": 4, "col_cta": 1, "pdl": 1, "packed": 0, "tma": 0}
+        {"ee_row": 16, "ee_col": 16, "row_tile": 4, "col_cta": 1, "pdl": 1, "packed": 0, "tma": 0, "generic": 0}
     tune._memo.clear()
 
 
