@@ -264,6 +264,9 @@ def _count_steps(sim, n):
 # by one instead of as one batch launch (the schedulers group by parity, so this stays 0
 # unless a step path bypasses _count_steps; the GPU tests assert it).
 LOCKSTEP_FALLBACKS = {"parity": 0}
+# Lockstep groups (batches) the adaptive-dt scheduler built; a group of unchanged members
+# is reused from round to round.
+LOCKSTEP_BUILDS = {"groups": 0}
 
 
 class _PlanLockstep:
@@ -658,6 +661,11 @@ def _adaptive_batch(run, points, states, keep_state):
     gens = [_single_gen(run, p, s, keep_state) for p, s in zip(points, states)]
     results = [None] * len(gens)
     pending = {}
+    # lockstep groups by their member simulations (the key holds them, so identities are
+    # not reused while cached): a group of the same members, whatever its step count or
+    # parity, steps through the same batch in the next round; a group whose members
+    # changed is closed at the end of the round it was last used in
+    locks = {}
     try:
         for i, g in enumerate(gens):
             try:
@@ -669,12 +677,17 @@ def _adaptive_batch(run, points, states, keep_state):
             for i, (sim, n) in pending.items():
                 key = (n, ad.lockstep_key(sim) if hasattr(ad, 'lockstep_key') else None)
                 groups.setdefault(key, []).append(i)
+            used = set()
             for (n, _), idx in groups.items():
-                lock = _lockstep(ad, [pending[i][0] for i in idx])
-                try:
-                    lock.step(n)
-                finally:
-                    lock.close()
+                members = tuple(pending[i][0] for i in idx)
+                lock = locks.get(members)
+                if lock is None:
+                    lock = locks[members] = _lockstep(ad, list(members))
+                    LOCKSTEP_BUILDS["groups"] += 1
+                used.add(members)
+                lock.step(n)
+            for members in [m for m in locks if m not in used]:
+                locks.pop(members).close()
             for i in sorted(pending):
                 try:
                     pending[i] = gens[i].send(None)
@@ -683,6 +696,8 @@ def _adaptive_batch(run, points, states, keep_state):
                     del pending[i]
         return results
     finally:
+        for lock in locks.values():
+            lock.close()
         for g in gens:
             g.close()
 

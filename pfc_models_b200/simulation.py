@@ -494,7 +494,9 @@ class Batch:
     """Independent simulations stepped in lockstep through pfc_batch_* (one launch per
     class and pass). Accepts `Simulation` objects or `Plan`s of any supported grid (the
     power-of-two and the mixed-radix kernels both batch); they must use one precision and
-    one device. The batch borrows the plans: close it before them."""
+    one device. The batch borrows the plans: step it only while all of them are open.
+    Closing it frees only its own tables, graphs and streams, so it may come before or
+    after the plans are closed."""
 
     def __init__(self, items):
         self.items = list(items)

@@ -594,6 +594,58 @@ def test_adaptive_dt_batch_equals_one_point_runs():
     assert max(g.dt_max for g in got) > 0.1
 
 
+class _CountingLock(pd._LoopLockstep):
+    """A lockstep group that records its life: steps only while open, closed once."""
+
+    def __init__(self, ad, sims):
+        super().__init__(ad, sims)
+        self.closed = False
+        ad.locks.append(self)
+
+    def step(self, n):
+        assert not self.closed
+        assert all(not getattr(s, 'released', False) for s in self.sims)
+        self.ad.group_steps += 1
+        super().step(n)
+
+    def close(self):
+        assert not self.closed
+        self.closed = True
+
+
+class _LockingToy(ToyAdapter):
+    def __init__(self):
+        super().__init__()
+        self.locks = []
+        self.group_steps = 0
+
+    def lockstep(self, sims):
+        return _CountingLock(self, sims)
+
+    def release(self, sim):
+        sim.released = True
+
+
+def test_adaptive_dt_batch_reuses_unchanged_groups():
+    """The adaptive-dt scheduler keeps a lockstep group while its members are unchanged
+    (whatever their step count), builds a new one when a member leaves or is rebuilt, steps
+    no group holding a released plan and closes every group once."""
+    relax = pd.RelaxSettings(dt=0.1, totalT=1e4, stepT=10.0, divs=10, maxDepth=4, requiredFitness=0.99,
+                             minimumA=1e-6, dtMax=1.0)
+    points = [(0.1, 0.5, 1.0), (0.1, 0.75, 1.0), (0.1, 0.9, 1.0), (0.1, 0.6, 1.0), (0.1, 0.5, 1.3),
+              (0.2, 0.55, 0.98)]
+    ad = _LockingToy()
+    builds = pd.LOCKSTEP_BUILDS["groups"]
+    got = pd.get_f_abc_batch(ad, {}, 'blob', {}, {}, relax, points)
+    for g, p in zip(got, points):
+        w = pd.get_f_abc(ToyAdapter(), {}, 'blob', {}, {}, relax, *p)
+        assert (g.values(), g.stop, g.steps, g.dt_max) == (w.values(), w.stop, w.steps, w.dt_max), p
+    assert all(lock.closed for lock in ad.locks)
+    assert pd.LOCKSTEP_BUILDS["groups"] - builds == len(ad.locks)
+    # (1526 group steps through 306 groups when written)
+    assert len(ad.locks) * 3 < ad.group_steps
+
+
 @pytest.mark.gpu
 def test_log_adaptive_dt_batch_on_b200_plans():
     """Adaptive dt on B200 plans: the members ask for different step counts at different
