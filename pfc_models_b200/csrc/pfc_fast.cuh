@@ -81,6 +81,51 @@ template <class T> __device__ __forceinline__ cplx<T> ldgc(const cplx<T>* p) {
   return mk((T)v.x, (T)v.y);
 }
 
+// L1 eviction priorities. The step kernels stream every field element through the SM
+// once (the row tile's 8-byte asynchronous copies, the column loads), which would evict
+// the small twiddle tables that every transform re-reads: the tables are loaded
+// evict_last, streamed field data without allocating in L1.
+// Tables: written before the first launch and never again, so the load may be moved or
+// merged freely.
+__device__ __forceinline__ float2 ld_keep(const float2* p) {
+  float2 v;
+  asm("ld.global.nc.L1::evict_last.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double2 ld_keep(const double2* p) {
+  double2 v;
+  asm("ld.global.nc.L1::evict_last.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float4 ld_keep(const float4* p) {
+  float4 v;
+  asm("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
+}
+template <class T> __device__ __forceinline__ cplx<T> ldkc(const cplx<T>* p) {
+  using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+  const V v = ld_keep(reinterpret_cast<const V*>(p));
+  return mk((T)v.x, (T)v.y);
+}
+// Field data read once per launch and not written by it. Volatile: the loads keep their
+// place after griddepcontrol.wait (the data is the previous launch's output).
+__device__ __forceinline__ float2 ld_stream(const float2* p) {
+  float2 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double2 ld_stream(const double2* p) {
+  double2 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+template <class T> __device__ __forceinline__ cplx<T> ldsc(const cplx<T>* p) {
+  using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+  const V v = ld_stream(reinterpret_cast<const V*>(p));
+  return mk((T)v.x, (T)v.y);
+}
+
 // Synchronisation of one transform group (TPF threads, group index g within the CTA).
 template <int TPF>
 __device__ __forceinline__ void group_sync(int g) {
@@ -132,7 +177,7 @@ struct FastPass {
         const cplx<T>* w = tw + k;
         cplx<T> wq[R];
 #pragma unroll
-        for (int q = 1; q < R; ++q) wq[q] = ldgc(w + (q - 1) * NS);
+        for (int q = 1; q < R; ++q) wq[q] = ldkc(w + (q - 1) * NS);
 #pragma unroll
         for (int q = 1; q < R; ++q) {
           cplx<T> x = wq[q];
@@ -338,7 +383,7 @@ row_step_fast(FastRowArgs<T> a) {
       } else {
         const cplx<T> xk = row[padi<P>(k)], xm = row[padi<P>(M - k)];
         const cplx<T> s = xk + conj(xm), d = xk - conj(xm);
-        const cplx<T> u = mul_i(cmul(conj(ldgc(a.rtw + k)), d));
+        const cplx<T> u = mul_i(cmul(conj(ldkc(a.rtw + k)), d));
         row[padi<P>(k)] = s + u;
         if (k != M / 2) row[padi<P>(M - k)] = conj(s - u);
       }
@@ -410,7 +455,7 @@ row_step_fast(FastRowArgs<T> a) {
       } else {
         const cplx<T> zk = srow[padi<P>(k)], zm = srow[padi<P>(M - k)];
         const cplx<T> e = T(0.5) * (zk + conj(zm));
-        const cplx<T> o = cmul(ldgc(a.rtw + k), T(0.5) * rot4<false>(zk - conj(zm)));
+        const cplx<T> o = cmul(ldkc(a.rtw + k), T(0.5) * rot4<false>(zk - conj(zm)));
         col0[(size_t)k * ny] = e + o;
         if (k != M / 2) col0[(size_t)(M - k) * ny] = conj(e - o);
       }
@@ -484,7 +529,7 @@ col_step_fast(FastColArgs<T> a) {
 #pragma unroll
     for (int b = 0; b < NB; ++b)
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[b * R + q] = col[t + b * TPF + q * NR];
+      for (int q = 0; q < R; ++q) v[b * R + q] = ldsc(col + t + b * TPF + q * NR);
   }
   if constexpr (NP == 1) {
     FastPass<T, NY, EE, S::radA(0), 1, P>::template compute<false>(v, t, twA_s);
@@ -528,8 +573,8 @@ col_step_fast(FastColArgs<T> a) {
       for (int j = 0; j < CH; ++j) {
         const int ky = t + (j0 + j) * TPF;
         const int kh = ky <= NY / 2 ? ky : NY - ky;
-        cw[j] = gcoef[ccb + kh];
-        p[j] = static_cast<const cplx<T>*>(gnin)[cb + ky];
+        cw[j] = ldsc(gcoef + ccb + kh);
+        p[j] = ldsc(static_cast<const cplx<T>*>(gnin) + cb + ky);
       }
 #pragma unroll
       for (int j = 0; j < CH; ++j) {

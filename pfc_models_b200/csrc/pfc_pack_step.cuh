@@ -72,7 +72,7 @@ struct PkPass {
         const float4* w = tw + k;
         float4 wq[R];
 #pragma unroll
-        for (int q = 1; q < R; ++q) wq[q] = __ldg(w + (q - 1) * NS);
+        for (int q = 1; q < R; ++q) wq[q] = ld_keep(w + (q - 1) * NS);
 #pragma unroll
         for (int q = 1; q < R; ++q)
           v[b * R + q] = pk_tw<INV>(v[b * R + q], make_float2(wq[q].x, wq[q].y), make_float2(wq[q].z, wq[q].w));
@@ -265,7 +265,7 @@ row_step_pk(FastRowArgs<float> a, const __grid_constant__ CUtensorMap tmap) {
                                                                     tma_tile_off(M - k, g, ib, smask))
                                  : row + padi<P>(M - k);
           const pc y = raw2pc(*xm);
-          const float4 r = __ldg(rtw + k);
+          const float4 r = ld_keep(rtw + k);
           const float2 C = make_float2(r.x, r.y), Sn = make_float2(r.z, r.w);
           const pc s = mkpc(add2(x.r, y.r), sub2(x.i, y.i));
           const pc d = mkpc(sub2(x.r, y.r), add2(x.i, y.i));
@@ -347,7 +347,7 @@ row_step_pk(FastRowArgs<float> a, const __grid_constant__ CUtensorMap tmap) {
         col0[0] = pc2raw(mkpc(add2(zk.r, zk.i), sub2(zk.r, zk.i)));
       } else {
         const pc zm = pk_ld(srow + padi<P>(M - k));
-        const float4 r = __ldg(rtw + k);
+        const float4 r = ld_keep(rtw + k);
         const float2 C = make_float2(r.x, r.y), Sn = make_float2(r.z, r.w);
         const pc es = mkpc(add2(zk.r, zm.r), sub2(zk.i, zm.i));       // 2E
         const pc d = mkpc(sub2(zk.r, zm.r), add2(zk.i, zm.i));        // 2iO
@@ -425,7 +425,7 @@ col_step_pk(FastColArgs<float> a) {
 #pragma unroll
       for (int q = 0; q < R; ++q) {
         const int y = t + b * TPF + q * NR;
-        v[b * R + q] = mkpc2(col0[y], col1[y]);
+        v[b * R + q] = mkpc2(ld_stream(col0 + y), ld_stream(col1 + y));
       }
   }
   if constexpr (NP == 1) {
@@ -473,8 +473,8 @@ col_step_pk(FastColArgs<float> a) {
         for (int l = 0; l < 2; ++l) {
           const int kx = kx0 + l;
           if (l >= lfirst) {
-            cw[l][j] = reinterpret_cast<const float2*>(gcoef)[(size_t)kx * nyh + kh];
-            p[l][j] = nin[(size_t)kx * NY + ky];
+            cw[l][j] = ld_stream(reinterpret_cast<const float2*>(gcoef) + (size_t)kx * nyh + kh);
+            p[l][j] = ld_stream(nin + (size_t)kx * NY + ky);
           } else {
             cw[l][j] = make_float2(0.f, 0.f);
             p[l][j] = make_float2(0.f, 0.f);

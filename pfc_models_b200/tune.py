@@ -134,7 +134,10 @@ def tune(nx, ny, precision="fp32", model="std", steps=20, warmup=3, save=True, p
         cp, ee_c = col_c[i % len(col_c)]
         packed = {(False, False): 0, (True, True): 1, (True, False): 2, (False, True): 3}[(rp, cp)]
         variant = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile, "packed": packed, "tma": tma}
-        sim = mod.BuildB200_Simulation(prm, geom, precision=precision, kernels=variant)
+        try:
+            sim = mod.BuildB200_Simulation(prm, geom, precision=precision, kernels=variant)
+        except _lib.PfcError:
+            continue     # a candidate this grid cannot take
         v = sim.plan.variant()
         if not v["fast"]:
             sim.plan.close()
@@ -148,9 +151,13 @@ def tune(nx, ny, precision="fp32", model="std", steps=20, warmup=3, save=True, p
         sim.plan.close()
         if not ok:
             continue
-        rk = (rp, v["ee_row"], v["row_tile"], tma)
+        # a side with an odd factor holds a fixed number of values per thread (e.g. 28):
+        # recorded as 0, the plan's own choice, which is what a request gets there
+        er = v["ee_row"] if v["ee_row"] in (PACKED_EE if rp else ees) else 0
+        ec = v["ee_col"] if v["ee_col"] in (PACKED_EE if cp else ees) else 0
+        rk = (rp, er, v["row_tile"], tma)
         rows[rk] = min(rows.get(rk, math.inf), 1e3 * ms_r / steps)
-        cols.setdefault((cp, v["ee_col"]), []).append(1e3 * ms_c / steps)
+        cols.setdefault((cp, ec), []).append(1e3 * ms_c / steps)
     if not rows or not cols:
         return None
     (rp, ee_r, tile, tma), row_us = min(rows.items(), key=lambda kv: kv[1])
@@ -192,9 +199,16 @@ def _tune_batch(nx, ny, precision, model, steps, warmup, save, path, batch):
     timed = {}
     for ee_r, tile, ee_c in itertools.product(ees, TILE_CHOICES, ees):
         variant = {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile}
-        sims = [mod.BuildB200_Simulation(prm, geom, precision=precision, kernels=variant) for _ in range(batch)]
+        sims = []
+        try:
+            for _ in range(batch):
+                sims.append(mod.BuildB200_Simulation(prm, geom, precision=precision, kernels=variant))
+        except _lib.PfcError:
+            for s in sims:
+                s.plan.close()
+            continue
         v = sims[0].plan.variant()
-        key = (v["ee_row"], v["row_tile"], v["ee_col"])
+        key = (v["ee_row"] if v["ee_row"] in ees else 0, v["row_tile"], v["ee_col"] if v["ee_col"] in ees else 0)
         if not v["fast"] or key in timed:
             for s in sims:
                 s.plan.close()
@@ -225,19 +239,27 @@ def _tune_batch(nx, ny, precision, model, steps, warmup, save, path, batch):
     return entry
 
 
-def _time_blocks(nx, ny, precision, model, variant, batch, steps=320, skip=None):
+def _time_blocks(nx, ny, precision, model, variant, batch, steps=320, skip=None, fast=True):
     """(us per whole step, column-kernel threads per CTA) of `batch` plans (1: one plan)
     with this variant, replayed from 16-step graphs after a warm-up that records them.
-    (None, None) if the fast kernels do not apply; (None, threads) without timing when
-    skip(threads) is true (a launch equal to one timed already)."""
+    (None, None) if the variant cannot be built or (with `fast`) the fast kernels do not
+    apply; (None, threads) without timing when skip(threads) is true (a launch equal to one
+    timed already). `fast=False` times whatever kernels the variant selects."""
     import torch
 
     from .simulation import Batch
     mod, geom, prm, f0 = _setup(nx, ny, precision, model)
-    sims = [mod.BuildB200_Simulation(prm, geom, precision=precision, kernels=variant) for _ in range(batch)]
+    sims = []
+    try:
+        for _ in range(batch):
+            sims.append(mod.BuildB200_Simulation(prm, geom, precision=precision, kernels=variant))
+    except _lib.PfcError:
+        for s in sims:
+            s.plan.close()
+        return None, None
     b = None
     try:
-        if not sims[0].plan.variant()["fast"]:
+        if fast and not sims[0].plan.variant()["fast"]:
             return None, None
         threads = sims[0].plan.info()["fast_col_threads"]
         if skip is not None and skip(threads):
@@ -272,7 +294,7 @@ def refine(nx, ny, precision, model, base, batch=1, min_gain=0.01):
     # per thread, and on small or skinny grids the run-time mixed-radix kernels can be faster
     generic_us = None
     if nx & (nx - 1) or ny & (ny - 1):
-        generic_us, _ = _time_blocks(nx, ny, precision, model, {"generic": 1}, batch)
+        generic_us, _ = _time_blocks(nx, ny, precision, model, {"generic": 1}, batch, fast=False)
     for cc in (0,) + COL_CTA_CHOICES:
         for pdl in (0, 1):
             us, threads = _time_blocks(nx, ny, precision, model, dict(v0, col_cta=cc, pdl=pdl), batch,

@@ -14,7 +14,8 @@ def test_packaged_table_is_used_without_a_user_cache(tmp_path, monkeypatch):
     v = tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200")
     assert v == {k: int(table[key].get(k) or 0) for k in tune.VARIANT_KEYS}
     for e in table.values():
-        assert e["ee_row"] in (8, 16, 32) and e["ee_col"] in (8, 16, 32) and e["row_tile"] in (1, 2, 4, 8, 16)
+        # 0: the plan's own choice (a side with an odd factor holds a fixed number per thread)
+        assert e["ee_row"] in (0, 8, 16, 32) and e["ee_col"] in (0, 8, 16, 32) and e["row_tile"] in (1, 2, 4, 8, 16)
         assert e.get("col_cta", 0) in (0, 1, 2, 4) and e.get("pdl", 0) in (0, 1)
     # batch-measured entries are preferred for batches and fall back to the single-plan ones
     bkey = "NVIDIA B200|512x512|fp32|std|batch"
