@@ -65,6 +65,9 @@ PARAMS = dict(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.3, g=0.0, dt=0.5)
 BLOCK = 16                 # ETD1 time steps per bench step (one graph replay)
 E2E_BLOCKS = 8             # bench steps per e2e frame (one upload, one F read-back)
 ACCURACY_STEPS = 20000     # the workload's full length
+SWEEP_STEPS = 320          # timed sweep steps (20 graph blocks of 16)
+SWEEP_BLOCK = 160          # steps per event pair in the sweep leg
+SWEEP_WARMUP = 32
 FLUSH_BYTES = 256 << 20
 
 
@@ -337,6 +340,13 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    def sum_over_ranks(x):
+        if not distributed:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
     from pfc_models_b200 import stdpfc, workloads
 
     geom, f0 = initial_field()
@@ -449,6 +459,26 @@ def run_ours(args):
             del bsim
         del bic
         torch.cuda.empty_cache()
+
+    # ---- the 512-point phase-diagram sweep (128^2 / 256^2 / 512^2 boxes), one batch;
+    # each rank steps its shard of the points, the slowest rank's time counts
+    swp = None
+    if not args.no_sweep:
+        from pfc_models_b200 import sweep
+        pts = sweep.shard(sweep.sweep_points(), rank, world)
+        _, tm = sweep.run_points(pts, SWEEP_STEPS, "fp32", block=SWEEP_BLOCK, settle=0, warmup=SWEEP_WARMUP,
+                                 mark=clocks.mark)
+        sw_ms = max_over_ranks(tm["ms"])
+        sw_sites = int(sum_over_ranks(float(tm["sites"])))
+        swp = {"workload": "512 stdPFC points, r in [-0.6, -0.05] x mean psi in [-0.6, 0], boxes 128^2 / 256^2 / "
+                           "512^2 (seeded choice), half crystal / half liquid starts, FP32-mixed, one batch "
+                           "(a launch per size class and pass, classes on concurrent streams, 16-step graphs)",
+               "steps": SWEEP_STEPS, "warmup": SWEEP_WARMUP, "points": 512, "sites": sw_sites,
+               "value": sw_sites * SWEEP_STEPS / (sw_ms / 1e3), "unit": UNIT, "ms": sw_ms,
+               "gpu_launches": tm["launches"],
+               "l2": "not flushed: the 1.4 GB working set exceeds L2"}
+        swp["step_achieved_gbs"] = 24 * swp["value"] / 1e9
+        torch.cuda.empty_cache()
     clk = clocks.stop()
 
     # ---- accuracy over the workload's full length (outside every timed region)
@@ -521,6 +551,9 @@ def run_ours(args):
                 "fp32": b32, "fp64": big["fp64"], "fp32_over_fp64": b32["value"] / big["fp64"]["value"],
                 "step_achieved_gbs": 24 * 8192 * 8192 / (b32["us_per_step"] * 1e-6) / 1e9,
                 "step_frac": 24 * 8192 * 8192 / (b32["us_per_step"] * 1e-6) / 1e9 / hbm}
+        if swp:
+            swp["step_frac"] = swp["step_achieved_gbs"] / hbm
+            line["sweep512"] = swp
         if acc:
             line["accuracy"] = acc
         if world == 1 and not args.no_cpu_baseline:
@@ -548,6 +581,7 @@ def main():
     ap.add_argument("--no-cupy-baseline", action="store_true", help="skip the reference GPU path leg")
     ap.add_argument("--no-8192", action="store_true", help="skip the 8192^2 HBM-bound key")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the 20000-step FP32 vs FP64 record")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the 512-point sweep key")
     kc = ap.add_argument_group("kernel case (short fixed workload for profiling)")
     kc.add_argument("--kernel-case", action="store_true")
     kc.add_argument("--nx", type=int, default=2048)

@@ -88,10 +88,12 @@ def shard(points, rank, world):
     return points[rank::world]
 
 
-def run_points(points, steps, precision="fp32", block=1000, device=None, settle=500):
+def run_points(points, steps, precision="fp32", block=1000, device=None, settle=500, warmup=0, mark=None):
     """Steps the points together on one GPU; returns (per-point results, timing).
     F is also reduced `settle` steps before the end (F_prev), so that states still
-    evolving can be told from settled ones."""
+    evolving can be told from settled ones. `warmup` untimed steps come first (the
+    batch's graphs are recorded there); the results then belong to warmup + steps.
+    `mark(True)` / `mark(False)` are called around each timed block (a clock sampler)."""
     import torch
 
     from . import stdpfc
@@ -110,6 +112,9 @@ def run_points(points, steps, precision="fp32", block=1000, device=None, settle=
     batch = Batch(sims)
     dev = sims[0].plan.device
     s = torch.cuda.current_stream(dev)
+    if warmup:
+        batch.step(warmup)
+        torch.cuda.synchronize(dev)
     done, ms = 0, 0.0
     settle = min(settle, steps)
     red_prev = None
@@ -120,10 +125,14 @@ def run_points(points, steps, precision="fp32", block=1000, device=None, settle=
         if done < steps - settle:
             k = min(k, steps - settle - done)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if mark:
+            mark(True)
         e0.record(s)
         batch.step(k)
         e1.record(s)
         e1.synchronize()
+        if mark:
+            mark(False)
         ms += e0.elapsed_time(e1)
         done += k
     red = batch.reduce()
