@@ -276,14 +276,15 @@ def run_kernel_case(a):
         prm = logpfc.BuildLogPFCModelParameters(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=0.1)
         mean = 0.55
     if a.batch > 0:
-        from pfc_models_b200.simulation import Batch
+        from pfc_models_b200.simulation import Batch, QueueBatch, queue_kernels
         sims = []
         for k in range(a.batch):
-            s = mod.BuildB200_Simulation(prm, geom, precision=a.precision)
+            s = mod.BuildB200_Simulation(prm, geom, precision=a.precision,
+                                         kernels=queue_kernels(a.nx, a.ny, a.precision) if a.queue else "auto")
             (s.State.n if a.model == "std" else s.State.phi)[...] = fields.GenerateNoisyLiquid(geom, mean, 0.01,
                                                                                                  seed=k)
             sims.append(s)
-        b = Batch(sims)
+        b = QueueBatch(sims) if a.queue else Batch(sims)
         b.step(1)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -294,7 +295,7 @@ def run_kernel_case(a):
         F = b.reduce()[:, 0]
         us = 1e3 * e0.elapsed_time(e1) / a.steps
         print(json.dumps({"nx": a.nx, "ny": a.ny, "precision": a.precision, "model": a.model, "steps": a.steps,
-                          "batch": a.batch, "path": sims[0].plan.path(), "classes": b.classes,
+                          "batch": a.batch, "queue": a.queue, "path": sims[0].plan.path(), "classes": b.classes,
                           "us_per_step": us, "site_steps_per_s": a.batch * a.nx * a.ny / (us * 1e-6),
                           "finite": bool(np.isfinite(F).all())}))
         b.close()
@@ -589,6 +590,7 @@ def main():
     kc.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     kc.add_argument("--model", default="std", choices=["std", "log"])
     kc.add_argument("--batch", type=int, default=0)
+    kc.add_argument("--queue", action="store_true", help="step the batch through the work-queue kernel")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

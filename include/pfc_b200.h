@@ -229,6 +229,44 @@ int pfc_batch_destroy(pfc_batch* batch);
 int64_t pfc_batch_launch_count(pfc_batch* batch);
 int pfc_batch_classes(pfc_batch* batch);
 
+/*
+ * Work-queue batches: the same lockstep stepping of many plans (the ad.step loop of
+ * phase_diagram/q0star.py:271-272, as for pfc_batch) in ONE persistent launch per block
+ * of steps. The launch is cooperative (every CTA resident) and walks a device list of
+ * work items, one row or column tile of one plan at one step, each waiting only for the
+ * tiles of its own plan that it depends on (per-plan completion counters, bounded waits).
+ * No counterpart in the reference. Plans must be FP32-mixed or FP64 stdPFC on the
+ * one-lane power-of-two kernels, nx in 64 .. 1024 and ny in 64 .. 1024, holding the
+ * values per thread the queue kernel is built with (FP32: 8 for row transforms of up
+ * to 128 points and columns of up to 512, else 16; FP64: 8), with CTAs of whole warps
+ * and at most 48 KiB of shared memory per pass; else PFC_E_ARG says which. Results are
+ * bit-identical to pfc_step of each plan. Blocks of 16 steps replay a recorded graph.
+ */
+typedef struct pfc_queue pfc_queue;
+
+int pfc_queue_create(pfc_plan* const* plans, int32_t count, pfc_queue** out);
+
+/* As pfc_batch_step. A wait that runs out sets PFC_STATUS_TIMEOUT (pfc_queue_status)
+ * and ends the launch early, leaving the plans' states undefined. */
+int pfc_queue_step(pfc_queue* queue, int64_t nsteps, void* stream);
+
+/* Synchronises the device and writes the status bits of the queue's launches so far
+ * (0, or PFC_STATUS_TIMEOUT). */
+int pfc_queue_status(pfc_queue* queue, int32_t* status);
+
+/* out4: CTAs of the launch, CTAs per SM, work items per step, classes. */
+int pfc_queue_info(pfc_queue* queue, int32_t* out4);
+
+int64_t pfc_queue_launch_count(pfc_queue* queue);
+
+int pfc_queue_destroy(pfc_queue* queue);
+
+/* Test hook, no counterpart in the reference: makes the first column item of the next
+ * launches wait for `extra` more completions than exist (0 restores the normal waits)
+ * and sets the poll limit of every wait (0: the default, about a second), so that a test
+ * can run a wait out and read PFC_STATUS_TIMEOUT. */
+int pfc_test_queue_wait(pfc_queue* queue, int32_t extra, int64_t wait_limit);
+
 /* The mean of `count` FP64 values at dev_field, summed with compensation
  * (Neumaier) on the device, written as one double to dev_mean. This entry point
  * has no counterpart in the reference. It exists for callers that must not

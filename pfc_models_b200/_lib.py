@@ -73,6 +73,13 @@ SIGNATURES = {
     "pfc_batch_destroy": (ctypes.c_int, [_vp]),
     "pfc_batch_launch_count": (_i64, [_vp]),
     "pfc_batch_classes": (ctypes.c_int, [_vp]),
+    "pfc_queue_create": (ctypes.c_int, [ctypes.POINTER(_vp), _i32, ctypes.POINTER(_vp)]),
+    "pfc_queue_step": (ctypes.c_int, [_vp, _i64, _vp]),
+    "pfc_queue_status": (ctypes.c_int, [_vp, ctypes.POINTER(_i32)]),
+    "pfc_queue_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i32)]),
+    "pfc_queue_launch_count": (_i64, [_vp]),
+    "pfc_queue_destroy": (ctypes.c_int, [_vp]),
+    "pfc_test_queue_wait": (ctypes.c_int, [_vp, _i32, _i64]),
     "pfc_locate_vacancies": (ctypes.c_int, [_vp, _i32, _i32, _dbl, _dbl, _vp, _i32, _vp, _vp]),
     "pfc_diagnose_modes": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _dbl, _vp, _vp]),
     "pfc_frozen_moments": (ctypes.c_int, [_vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _dbl, _vp, _vp]),

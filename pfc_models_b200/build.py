@@ -25,9 +25,10 @@ OUT = os.path.join(HERE, "libpfc_b200.so")
 SOURCES = ["pfc_plan.cu", "pfc_generic_f32.cu", "pfc_generic_f64.cu",
            "pfc_fast_f32_e8.cu", "pfc_fast_f32_e16.cu", "pfc_fast_f32_e32.cu", "pfc_fast_f64_e8.cu",
            "pfc_fast_f64_e16.cu", "pfc_track.cu", "pfc_diag.cu", "pfc_onecta.cu", "pfc_pack_inst.cu", "pfc_extv.cu",
-           "pfc_fastmix_f32.cu", "pfc_fastmix_f64.cu"]
+           "pfc_fastmix_f32.cu", "pfc_fastmix_f64.cu", "pfc_queue_f32.cu", "pfc_queue_f64.cu"]
 HEADERS = ["pfc_fft.cuh", "pfc_kernels.cuh", "pfc_fast.cuh", "pfc_small.cuh", "pfc_registry.h",
-           "pfc_fast_inst.cuh", "pfc_generic_inst.cuh", "pfc_pack.cuh", "pfc_pack_step.cuh", "pfc_fastmix_inst.cuh"]
+           "pfc_fast_inst.cuh", "pfc_generic_inst.cuh", "pfc_pack.cuh", "pfc_pack_step.cuh", "pfc_fastmix_inst.cuh",
+           "pfc_queue.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC"]

@@ -230,6 +230,8 @@ __device__ __forceinline__ void fast_mid(cplx<T>* buf, cplx<T>* v, int t, int g,
 }
 
 
+constexpr unsigned kStatusTimeout = 2;   // PFC_STATUS_TIMEOUT: a bounded wait gave up
+
 template <class T>
 struct FastRowArgs {
   int ny, rows, ld;
@@ -288,6 +290,24 @@ __device__ __forceinline__ void l2_prefetch_range(const void* p, unsigned bytes,
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Synchronisation hook of the step bodies: in the step kernels, the point where a kernel
+// launched with programmatic dependent launch waits for its predecessor; in the work-queue
+// kernel, whose items wait for their dependencies before the body starts, nothing.
+struct PdlSync {
+  __device__ __forceinline__ void operator()() const { pdl_wait(); pdl_trigger(); }
+};
+struct NoSync {
+  __device__ __forceinline__ void operator()() const {}
+};
+
+// CTA-wide barrier of the threads that run a step body: the whole CTA in the step kernels,
+// the first `nthreads` threads (whole warps) in the work-queue kernel, on named barrier 15,
+// which no transform group uses (group barriers are 1 + group index, at most 4 groups).
+__device__ __forceinline__ void body_sync(int nthreads) {
+  if (nthreads == (int)blockDim.x) __syncthreads();
+  else asm volatile("bar.sync 15, %0;" ::"r"(nthreads) : "memory");
+}
+
 template <int TPF> struct FastBound { static constexpr int value = TPF > 256 ? TPF : 256; };
 // minimum resident CTAs per SM requested from the register allocator (256-thread CTAs)
 // from the registers the values held take (2 per real): with up to 32 of them the
@@ -300,41 +320,39 @@ template <class T, int EE, int TPF> struct FastMinBlocks {
 // ------------------------------------------------------------------ row kernel
 // CTA: `rows` consecutive rows (tile), groups of TPF threads each process rows
 // g, g + ngroups, ... The tile is staged through shared memory with a transposing
-// load/store (global layout is column-major).
-template <class T, int M, int EE_REQ, int MODEL>
-__global__ void __launch_bounds__(FastBound<FastSeq<M, EE_REQ, RadixCap<T>::value>::TPF>::value,
-                  FastMinBlocks<T, FastSeq<M, EE_REQ, RadixCap<T>::value>::EE,
-                                FastSeq<M, EE_REQ, RadixCap<T>::value>::TPF>::value)
-row_step_fast(FastRowArgs<T> a) {
+// load/store (global layout is column-major). The body runs row tile `tile` of batch member
+// `member` (of `batch`, or the plan in `a` when null) on the CTA's first `nthreads` threads.
+template <class T, int M, int EE_REQ, int MODEL, class Sync>
+__device__ __forceinline__ void row_step_body(const FastRowArgs<T>& a, const BatchBufs* batch, int tile, int member,
+                                              int nthreads, Sync sync) {
   using S = FastSeq<M, EE_REQ, RadixCap<T>::value>;
   constexpr int P = FastPad<T, S::EE>::value;
   constexpr int EE = S::EE, TPF = S::TPF, NP = S::NPASS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
   const int ny = a.ny, rows = a.rows, ld = a.ld, rl2 = a.rows_log2;
-  const int y0 = blockIdx.x * rows;
-  const int ngroups = blockDim.x / TPF;
+  const int y0 = tile * rows;
+  const int ngroups = nthreads / TPF;
   const int g = threadIdx.x / TPF, t = threadIdx.x - g * TPF;
   const bool dev = (sizeof(T) == 4);
   const cplx<T>* gin = a.in;
   cplx<T>* gout = a.out;
   const double* scal = a.scal;
-  if (a.batch) {
-    const BatchBufs& b = a.batch[blockIdx.y];
+  if (batch) {
+    const BatchBufs& b = batch[member];
     gin = static_cast<const cplx<T>*>(b.w);
     gout = static_cast<cplx<T>*>(b.v);
     scal = b.scal;
   }
 
   // W is the previous column pass's output
-  pdl_wait();
-  pdl_trigger();
+  sync();
 
   // ---- transposing tile load: element (kx, y0 + r) -> sm[r * ld + pad(kx)], issued as
   // asynchronous global->shared copies so that every load of the tile is in flight at once.
-  // blockDim is a multiple of rows: each thread keeps one row and walks kx with a fixed
+  // nthreads is a multiple of rows: each thread keeps one row and walks kx with a fixed
   // stride, so the addresses advance by constants.
-  const int tr = threadIdx.x & (rows - 1), kx0 = threadIdx.x >> rl2, kstep = blockDim.x >> rl2;
+  const int tr = threadIdx.x & (rows - 1), kx0 = threadIdx.x >> rl2, kstep = nthreads >> rl2;
   const bool rvalid = y0 + tr < ny;
   const size_t gstep = (size_t)kstep * ny;
   {
@@ -356,7 +374,7 @@ row_step_fast(FastRowArgs<T> a) {
   const cplx<T>* twB_s = a.twB;
   asm volatile("cp.async.commit_group;" ::: "memory");
   asm volatile("cp.async.wait_group 0;" ::: "memory");
-  __syncthreads();
+  body_sync(nthreads);
 
   // nonlinearity parameters
   float c1 = 0.f, c2 = 0.f, inv = 0.f, lmin = 0.f;
@@ -439,7 +457,7 @@ row_step_fast(FastRowArgs<T> a) {
 #pragma unroll
       for (int q = 0; q < RL; ++q) row[padi<P>(QO::out_index(t, b, q))] = v[b * RL + q];
   }
-  __syncthreads();
+  body_sync(nthreads);
   // ---- forward-real post-twiddle fused with the transposing tile store: one (k, M - k)
   // pair per step, Y[k] = E + r_k O, Y[M - k] = conj(E - r_k O), with
   // E = (Z[k] + conj Z[M-k]) / 2, O = -i (Z[k] - conj Z[M-k]) / 2, written to V[k][y]
@@ -463,24 +481,49 @@ row_step_fast(FastRowArgs<T> a) {
   }
 }
 
+template <class T, int M, int EE_REQ, int MODEL>
+__global__ void __launch_bounds__(FastBound<FastSeq<M, EE_REQ, RadixCap<T>::value>::TPF>::value,
+                  FastMinBlocks<T, FastSeq<M, EE_REQ, RadixCap<T>::value>::EE,
+                                FastSeq<M, EE_REQ, RadixCap<T>::value>::TPF>::value)
+row_step_fast(FastRowArgs<T> a) {
+  row_step_body<T, M, EE_REQ, MODEL>(a, a.batch, blockIdx.x, blockIdx.y, blockDim.x, PdlSync{});
+}
+
+// Loads of field data in the column body. The step kernels read V and n_hat, outputs of
+// earlier launches, without allocating in L1 through the non-coherent path; the work-queue
+// kernel reads them while other CTAs of the same launch write them, so through L2 only.
+template <bool COHERENT, class T>
+__device__ __forceinline__ cplx<T> ld_field(const cplx<T>* p) {
+  if constexpr (!COHERENT) {
+    return ldsc(p);
+  } else {
+    using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+    V v;
+    if constexpr (sizeof(T) == 4)
+      asm volatile("ld.global.cg.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    else
+      asm volatile("ld.global.cg.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return mk((T)v.x, (T)v.y);
+  }
+}
+
 // ------------------------------------------------------------------ column kernel
 // CTA: ngroups consecutive columns, one group of TPF threads per column. Global
 // reads and writes go straight between registers and HBM (the first pass of each
-// sequence reads, and the last pass writes, consecutive elements per lane).
-template <class T, int NY, int EE_REQ>
-__global__ void __launch_bounds__(FastBound<FastSeq<NY, EE_REQ, RadixCap<T>::value>::TPF>::value,
-                                  FastMinBlocks<T, FastSeq<NY, EE_REQ, RadixCap<T>::value>::EE,
-                                                FastSeq<NY, EE_REQ, RadixCap<T>::value>::TPF>::value)
-col_step_fast(FastColArgs<T> a) {
+// sequence reads, and the last pass writes, consecutive elements per lane). The body runs
+// column tile `tile` of member `member` on the CTA's first `nthreads` threads.
+template <class T, int NY, int EE_REQ, bool COHERENT, class Sync>
+__device__ __forceinline__ void col_step_body(const FastColArgs<T>& a, const BatchBufs* batch, int tile, int member,
+                                              int nthreads, Sync sync) {
   using S = FastSeq<NY, EE_REQ, RadixCap<T>::value>;
   constexpr int P = FastPad<T, S::EE>::value;
   constexpr int EE = S::EE, TPF = S::TPF, NP = S::NPASS;
   constexpr int PADN = NY + (NY >> P) + 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
-  const int ngroups = blockDim.x / TPF;
+  const int ngroups = nthreads / TPF;
   const int g = threadIdx.x / TPF, t = threadIdx.x - g * TPF;
-  const int kx = blockIdx.x * ngroups + g;      // m is a multiple of ngroups
+  const int kx = tile * ngroups + g;      // m is a multiple of ngroups
   const cplx<T>* twA_s = a.twA;                   // twiddle tables, read through L1
   const cplx<T>* twB_s = a.twB;
   cplx<T>* buf = sm + g * PADN;                   // exchange buffer of this column
@@ -493,8 +536,8 @@ col_step_fast(FastColArgs<T> a) {
   cplx<T>* gwout = a.wout;
   const cplx<T>* gcoef = a.coef;
   const cplx<double>* gcoef64 = a.coef64;
-  if (a.batch) {
-    const BatchBufs& b = a.batch[blockIdx.y];
+  if (batch) {
+    const BatchBufs& b = batch[member];
     gin = static_cast<const cplx<T>*>(b.v);
     gnin = b.nin;
     gnout = b.nout;
@@ -519,8 +562,7 @@ col_step_fast(FastColArgs<T> a) {
 
   // V is the row pass's output (n_hat and the coefficients above were written two or
   // more launches back)
-  pdl_wait();
-  pdl_trigger();
+  sync();
 
   // ---- forward sequence A; pass 0 reads the column of V from HBM
   {
@@ -529,7 +571,7 @@ col_step_fast(FastColArgs<T> a) {
 #pragma unroll
     for (int b = 0; b < NB; ++b)
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[b * R + q] = ldsc(col + t + b * TPF + q * NR);
+      for (int q = 0; q < R; ++q) v[b * R + q] = ld_field<COHERENT>(col + t + b * TPF + q * NR);
   }
   if constexpr (NP == 1) {
     FastPass<T, NY, EE, S::radA(0), 1, P>::template compute<false>(v, t, twA_s);
@@ -574,7 +616,7 @@ col_step_fast(FastColArgs<T> a) {
         const int ky = t + (j0 + j) * TPF;
         const int kh = ky <= NY / 2 ? ky : NY - ky;
         cw[j] = ldsc(gcoef + ccb + kh);
-        p[j] = ldsc(static_cast<const cplx<T>*>(gnin) + cb + ky);
+        p[j] = ld_field<COHERENT>(static_cast<const cplx<T>*>(gnin) + cb + ky);
       }
 #pragma unroll
       for (int j = 0; j < CH; ++j) {
@@ -681,6 +723,14 @@ col_step_fast(FastColArgs<T> a) {
         col[QO::out_index(t, b, q)] = mk(s * x.x, s * x.y);
       }
   }
+}
+
+template <class T, int NY, int EE_REQ>
+__global__ void __launch_bounds__(FastBound<FastSeq<NY, EE_REQ, RadixCap<T>::value>::TPF>::value,
+                                  FastMinBlocks<T, FastSeq<NY, EE_REQ, RadixCap<T>::value>::EE,
+                                                FastSeq<NY, EE_REQ, RadixCap<T>::value>::TPF>::value)
+col_step_fast(FastColArgs<T> a) {
+  col_step_body<T, NY, EE_REQ, false>(a, a.batch, blockIdx.x, blockIdx.y, blockDim.x, PdlSync{});
 }
 
 }  // namespace pfc

@@ -136,7 +136,6 @@ __device__ __forceinline__ unsigned tma_tile_off(int kx, int p, int ib, unsigned
   return o ^ (((o >> 7) & smask) << 4);
 }
 
-constexpr unsigned kStatusTimeout = 2;   // PFC_STATUS_TIMEOUT
 constexpr long long kTmaWaitLimit = 1LL << 22;
 
 // ------------------------------------------------------------------ row kernel

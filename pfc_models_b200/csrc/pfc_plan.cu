@@ -16,6 +16,7 @@
 #include "pfc_b200.h"
 #include "pfc_fast.cuh"
 #include "pfc_kernels.cuh"
+#include "pfc_queue.cuh"
 #include "pfc_registry.h"
 #include "pfc_small.cuh"
 
@@ -215,6 +216,28 @@ struct pfc_batch {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   cudaEvent_t fork = nullptr;
   long long launches = 0;
+};
+
+// Work-queue batch (pfc_queue.cuh): members in the caller's order, their classes, the
+// device copies of the class descriptions, one step's item list and the counters.
+struct pfc_queue {
+  bool fp32 = false;
+  std::vector<pfc_plan*> plans;
+  std::vector<std::vector<int>> classes;   // member indices of each class
+  void* cls_dev = nullptr;                 // QueueClass<T>[classes]
+  std::vector<void*> tables;               // BatchBufs arrays, two per class
+  int4* items = nullptr;
+  int nitems = 0;
+  int first_col_item = 0;
+  unsigned* counters = nullptr;            // rows done [n], columns done [n], ticket
+  int* flags = nullptr;                    // status word, abort flag
+  void* fn = nullptr;
+  int grid = 0, per_sm = 0;
+  size_t smem = 0;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long long launches = 0;
+  long long wait_limit = kQueueWaitLimit;
+  int extra = 0;
 };
 
 // FP32 form: modes with |A - 1| below this are "slow" and keep an FP64-accurate state
@@ -618,24 +641,52 @@ ExtvCoefArgs extv_coef_args(const pfc_plan* h) {
 // decision and coefficient kernels)
 int launches_per_step(const pfc_plan* h) { return h->extv ? 4 : 2; }
 
+// Arguments of the fast row kernel for plan h (a batch's members from `table`).
+template <class T>
+FastRowArgs<T> fast_row_args(const pfc_plan* h, const BatchBufs* table) {
+  FastRowArgs<T> a{};
+  a.batch = table;
+  a.ny = h->ny; a.rows = h->fr_rows; a.ld = h->fr_ld; a.rows_log2 = ilog2_exact(h->fr_rows);
+  a.in = reinterpret_cast<const cplx<T>*>(h->W);
+  a.out = reinterpret_cast<cplx<T>*>(h->V);
+  const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(h->tw);
+  a.twA = tw + h->tw_ra; a.twB = tw + h->tw_rb; a.rtw = tw + (h->packed_row ? h->rt4_off : h->rt_off);
+  a.scal = h->scal;
+  a.clamp = h->prob.clamp_log;
+  a.g = h->prob.g; a.min_phi = h->prob.min_phi;
+  a.min_log = (h->prob.min_phi > 0) ? std::log(h->prob.min_phi) : -INFINITY;
+  a.err = h->status;
+  a.tma_box = table ? 0 : h->tma_box;   // a batch's plans each have their own W: copies
+  a.tma_extra_tx = h->tma_extra_tx;
+  a.tma_wait_limit = h->tma_wait_limit;
+  return a;
+}
+
+// Arguments of the fast column kernel for plan h (a batch's members from `table`).
+template <class T>
+FastColArgs<T> fast_col_args(const pfc_plan* h, const BatchBufs* table) {
+  FastColArgs<T> a{};
+  a.batch = table;
+  a.m = h->m; a.ny = h->ny; a.nyh = h->nyh;
+  a.in = reinterpret_cast<const cplx<T>*>(h->V);
+  a.nin = h->nhat[h->cur];
+  a.nout = h->nhat[h->cur ^ 1];
+  a.nin_lo = static_cast<const cplx<float>*>(h->nhat_lo[h->cur]);
+  a.nout_lo = static_cast<cplx<float>*>(h->nhat_lo[h->cur ^ 1]);
+  a.coef64 = static_cast<const cplx<double>*>(h->coef64);
+  a.slow_tau = kSlowTau;
+  a.wout = reinterpret_cast<cplx<T>*>(h->W);
+  a.coef = static_cast<const cplx<T>*>(h->coef);
+  const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(h->tw);
+  a.twA = tw + h->tw_ca; a.twB = tw + h->tw_cb;
+  a.scale = (T)(1.0 / ((double)h->nx * (double)h->ny));
+  return a;
+}
+
 template <class T>
 int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullptr, int count = 1) {
   if (h->fast) {
-    FastRowArgs<T> a{};
-    a.batch = table;
-    a.ny = h->ny; a.rows = h->fr_rows; a.ld = h->fr_ld; a.rows_log2 = ilog2_exact(h->fr_rows);
-    a.in = reinterpret_cast<const cplx<T>*>(h->W);
-    a.out = reinterpret_cast<cplx<T>*>(h->V);
-    const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(h->tw);
-    a.twA = tw + h->tw_ra; a.twB = tw + h->tw_rb; a.rtw = tw + (h->packed_row ? h->rt4_off : h->rt_off);
-    a.scal = h->scal;
-    a.clamp = h->prob.clamp_log;
-    a.g = h->prob.g; a.min_phi = h->prob.min_phi;
-    a.min_log = (h->prob.min_phi > 0) ? std::log(h->prob.min_phi) : -INFINITY;
-    a.err = h->status;
-    a.tma_box = table ? 0 : h->tma_box;   // a batch's plans each have their own W: copies
-    a.tma_extra_tx = h->tma_extra_tx;
-    a.tma_wait_limit = h->tma_wait_limit;
+    FastRowArgs<T> a = fast_row_args<T>(h, table);
     void* args_pk[] = {(void*)&a, (void*)&h->tmap};
     void* args1[] = {(void*)&a};
     void** args = h->packed_row ? args_pk : args1;
@@ -666,21 +717,7 @@ int launch_step_row(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
 template <class T>
 int launch_step_col(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullptr, int count = 1) {
   if (h->fast) {
-    FastColArgs<T> a{};
-    a.batch = table;
-    a.m = h->m; a.ny = h->ny; a.nyh = h->nyh;
-    a.in = reinterpret_cast<const cplx<T>*>(h->V);
-    a.nin = h->nhat[h->cur];
-    a.nout = h->nhat[h->cur ^ 1];
-    a.nin_lo = static_cast<const cplx<float>*>(h->nhat_lo[h->cur]);
-    a.nout_lo = static_cast<cplx<float>*>(h->nhat_lo[h->cur ^ 1]);
-    a.coef64 = static_cast<const cplx<double>*>(h->coef64);
-    a.slow_tau = kSlowTau;
-    a.wout = reinterpret_cast<cplx<T>*>(h->W);
-    a.coef = static_cast<const cplx<T>*>(h->coef);
-    const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(h->tw);
-    a.twA = tw + h->tw_ca; a.twB = tw + h->tw_cb;
-    a.scale = (T)(1.0 / ((double)h->nx * (double)h->ny));
+    FastColArgs<T> a = fast_col_args<T>(h, table);
     void* args[] = {(void*)&a};
     cudaError_t e = launch_step_kernel(h, h->fast_col_fn, dim3(h->fc_grid, count), dim3(h->fc_threads), args,
                                        h->fc_smem, s);
@@ -1844,5 +1881,267 @@ extern "C" int pfc_test_tma_wait(pfc_plan* h, int32_t extra_bytes, int32_t wait_
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   for (auto& g : h->graph1)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return PFC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Work-queue batches: the members' row and column tiles of a block of steps as the items
+// of one cooperative launch (pfc_queue.cuh).
+namespace {
+
+constexpr size_t kQueueSmemMax = 48 * 1024;
+constexpr int kQueueItemsPerPass = 8;
+
+// Why plan h cannot join a work-queue batch, or nullptr.
+const char* queue_refusal(const pfc_plan* h) {
+  const int lr = ilog2_exact(h->m), lc = ilog2_exact(h->ny);
+  if (lr < 0 || lc < 0) return "the work-queue kernel steps power-of-two grids";
+  if (!h->fast || h->packed || h->onecta || h->extv) return "plans must use the one-lane power-of-two step kernels";
+  if (h->prob.model != PFC_MODEL_STD) return "the work-queue kernel steps stdPFC plans";
+  if (lr < kQueueMinLogRow || lr > kQueueMaxLogRow || lc < kQueueMinLogCol || lc > kQueueMaxLogCol)
+    return "grid sides must be 64 .. 1024";
+  if (h->ee_row != queue_row_ee(!h->fp32, h->m) || h->ee_col != queue_col_ee(!h->fp32, h->ny))
+    return "the plan's values per thread differ from the work-queue kernel's";
+  if (h->fr_threads > kQueueThreads || h->fc_threads > kQueueThreads || h->fr_threads % 32 || h->fc_threads % 32)
+    return "a pass's CTA is not whole warps of at most 256 threads";
+  if (h->fr_smem > kQueueSmemMax || h->fc_smem > kQueueSmemMax) return "a pass needs more than 48 KiB of shared memory";
+  return nullptr;
+}
+
+template <class T>
+int queue_build(pfc_queue* q) {
+  const int n = (int)q->plans.size();
+  // classes: the batch's (everything the kernels take from the plan besides the table)
+  for (int i = 0; i < n; ++i) {
+    const pfc_plan* h = q->plans[i];
+    int c = 0;
+    for (; c < (int)q->classes.size(); ++c) {
+      const pfc_plan* r = q->plans[q->classes[c][0]];
+      if (r->fast_row_fn == h->fast_row_fn && r->fast_col_fn == h->fast_col_fn && r->fr_rows == h->fr_rows &&
+          r->fc_threads == h->fc_threads && r->nx == h->nx && r->ny == h->ny && r->prob.g == h->prob.g &&
+          r->prob.clamp_log == h->prob.clamp_log && r->prob.min_phi == h->prob.min_phi)
+        break;
+    }
+    if (c == (int)q->classes.size()) q->classes.emplace_back();
+    q->classes[c].push_back(i);
+  }
+  const int ncls = (int)q->classes.size();
+  std::vector<QueueClass<T>> host(ncls);
+  std::vector<int4> items;
+  for (int c = 0; c < ncls; ++c) {
+    const std::vector<int>& mem = q->classes[c];
+    const pfc_plan* r = q->plans[mem[0]];
+    QueueClass<T>& k = host[c];
+    k.row = fast_row_args<T>(r, nullptr);
+    k.col = fast_col_args<T>(r, nullptr);
+    k.row_log = ilog2_exact(r->m);
+    k.col_log = ilog2_exact(r->ny);
+    k.row_threads = r->fr_threads;
+    k.col_threads = r->fc_threads;
+    // a few items per member and pass: each item pays one dependency check and one
+    // completion, and a pass of more, smaller items gains little from the finer grain
+    k.row_group = std::max(1, r->fr_grid / kQueueItemsPerPass);
+    k.col_group = std::max(1, r->fc_grid / kQueueItemsPerPass);
+    k.row_items = r->fr_grid / k.row_group;
+    k.col_items = r->fc_grid / k.col_group;
+    q->smem = std::max(q->smem, std::max(r->fr_smem, r->fc_smem));
+    for (int p = 0; p < 2; ++p) {
+      std::vector<BatchBufs> tb(mem.size());
+      for (size_t j = 0; j < mem.size(); ++j) {
+        const pfc_plan* h = q->plans[mem[j]];
+        tb[j].w = h->W;
+        tb[j].v = h->V;
+        tb[j].nin = h->nhat[p];
+        tb[j].nout = h->nhat[p ^ 1];
+        tb[j].nin_lo = h->nhat_lo[p];
+        tb[j].nout_lo = h->nhat_lo[p ^ 1];
+        tb[j].coef = h->coef;
+        tb[j].coef64 = h->coef64;
+        tb[j].scal = h->scal;
+      }
+      void* d = nullptr;
+      PFC_CUDA(cudaMalloc(&d, tb.size() * sizeof(BatchBufs)));
+      q->tables.push_back(d);
+      PFC_CUDA(cudaMemcpy(d, tb.data(), tb.size() * sizeof(BatchBufs), cudaMemcpyHostToDevice));
+      k.table[p] = static_cast<const BatchBufs*>(d);
+    }
+  }
+  // one step: every row tile (class by class), then every column tile
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) q->first_col_item = (int)items.size();
+    for (int c = 0; c < ncls; ++c)
+      for (size_t j = 0; j < q->classes[c].size(); ++j) {
+        const int nit = pass ? host[c].col_items : host[c].row_items;
+        for (int t = 0; t < nit; ++t)
+          items.push_back(make_int4(q->classes[c][j], c, (int)j, t | (pass ? kQueueColBit : 0)));
+      }
+  }
+  q->nitems = (int)items.size();
+  PFC_CUDA(cudaMalloc(&q->cls_dev, ncls * sizeof(QueueClass<T>)));
+  PFC_CUDA(cudaMemcpy(q->cls_dev, host.data(), ncls * sizeof(QueueClass<T>), cudaMemcpyHostToDevice));
+  PFC_CUDA(cudaMalloc(&q->items, items.size() * sizeof(int4)));
+  PFC_CUDA(cudaMemcpy(q->items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  PFC_CUDA(cudaMalloc(&q->counters, (2 * (size_t)n + 1) * sizeof(unsigned)));
+  PFC_CUDA(cudaMalloc(&q->flags, 2 * sizeof(int)));
+  PFC_CUDA(cudaMemset(q->flags, 0, 2 * sizeof(int)));
+  q->fn = QueueInst<T>::kernel();
+  PFC_CUDA(cudaFuncSetAttribute(q->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q->smem));
+  int dev = 0, n_sm = 0;
+  PFC_CUDA(cudaGetDevice(&dev));
+  PFC_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  PFC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&q->per_sm, q->fn, kQueueThreads, q->smem));
+  if (q->per_sm < 1) return fail(PFC_E_ARG, "pfc_queue_create: the work-queue kernel does not fit an SM");
+  q->grid = q->per_sm * n_sm;
+  return PFC_OK;
+}
+
+template <class T>
+int queue_launch(pfc_queue* q, int parity, int nsteps, cudaStream_t s) {
+  const size_t n = q->plans.size();
+  PFC_CUDA(cudaMemsetAsync(q->counters, 0, (2 * n + 1) * sizeof(unsigned), s));
+  PFC_CUDA(cudaMemsetAsync(q->flags + 1, 0, sizeof(int), s));
+  QueueArgs<T> a{};
+  a.classes = static_cast<const QueueClass<T>*>(q->cls_dev);
+  a.items = q->items;
+  a.nitems = q->nitems;
+  a.nsteps = nsteps;
+  a.parity0 = parity;
+  a.rows_done = q->counters;
+  a.cols_done = q->counters + n;
+  a.ticket = q->counters + 2 * n;
+  a.status = q->flags;
+  a.abort = q->flags + 1;
+  a.wait_limit = q->wait_limit;
+  a.extra_item = q->extra ? q->first_col_item : -1;
+  a.extra = q->extra;
+  void* args[] = {(void*)&a};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(q->grid);
+  cfg.blockDim = dim3(kQueueThreads);
+  cfg.dynamicSmemBytes = q->smem;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelExC(&cfg, q->fn, args);
+  ++q->launches;
+  if (e != cudaSuccess) return fail(PFC_E_CUDA, "work-queue launch failed: %s", cudaGetErrorString(e));
+  return PFC_OK;
+}
+
+template <class T>
+int do_queue_step(pfc_queue* q, long long nsteps, cudaStream_t s) {
+  const int parity = q->plans[0]->cur;
+  for (pfc_plan* h : q->plans) {
+    if (!h->state_set) return fail(PFC_E_STATE, "pfc_queue_step: a plan has no state");
+    if (h->cur != parity)
+      return fail(PFC_E_STATE, "pfc_queue_step: plans must have taken the same number of steps mod 2");
+  }
+  const long long blocks = nsteps / kGraphBlock;
+  if (blocks > 0) {
+    if (!q->graph[parity]) {
+      const long long launches = q->launches;
+      int rc = capture_graph([&](cudaStream_t cs) { return queue_launch<T>(q, parity, kGraphBlock, cs); },
+                             &q->graph[parity]);
+      q->launches = launches;
+      if (rc) return rc;
+    }
+    for (long long k = 0; k < blocks; ++k) {
+      cudaError_t e = cudaGraphLaunch(q->graph[parity], s);
+      if (e != cudaSuccess) return fail(PFC_E_CUDA, "cudaGraphLaunch failed: %s", cudaGetErrorString(e));
+    }
+    q->launches += blocks;
+  }
+  const long long rest = nsteps - blocks * kGraphBlock;   // kGraphBlock is even: parity unchanged
+  if (rest > 0) {
+    int rc = queue_launch<T>(q, parity, (int)rest, s);
+    if (rc) return rc;
+  }
+  for (pfc_plan* h : q->plans) {
+    h->cur ^= (int)(nsteps & 1);
+    h->steps_since_set += nsteps;
+  }
+  return PFC_OK;
+}
+
+void queue_drop_graphs(pfc_queue* q) {
+  for (auto& g : q->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+}  // namespace
+
+extern "C" int pfc_queue_destroy(pfc_queue* q) {
+  if (!q) return PFC_OK;
+  queue_drop_graphs(q);
+  for (void* t : q->tables)
+    if (t) cudaFree(t);
+  if (q->cls_dev) cudaFree(q->cls_dev);
+  if (q->items) cudaFree(q->items);
+  if (q->counters) cudaFree(q->counters);
+  if (q->flags) cudaFree(q->flags);
+  delete q;
+  return PFC_OK;
+}
+
+extern "C" int pfc_queue_create(pfc_plan* const* plans, int32_t count, pfc_queue** out) {
+  if (!plans || count <= 0 || !out) return fail(PFC_E_ARG, "pfc_queue_create: need plans and an output");
+  *out = nullptr;
+  for (int i = 0; i < count; ++i) {
+    if (!plans[i]) return fail(PFC_E_ARG, "pfc_queue_create: null plan %d", i);
+    if (plans[i]->fp32 != plans[0]->fp32) return fail(PFC_E_ARG, "pfc_queue_create: plans mix precisions");
+    if (plans[i]->device != plans[0]->device) return fail(PFC_E_ARG, "pfc_queue_create: plans on different devices");
+    if (const char* why = queue_refusal(plans[i])) return fail(PFC_E_ARG, "pfc_queue_create: plan %d: %s", i, why);
+    for (int j = 0; j < i; ++j)
+      if (plans[j] == plans[i]) return fail(PFC_E_ARG, "pfc_queue_create: plan %d appears twice", i);
+  }
+  pfc_queue* q = new pfc_queue();
+  q->fp32 = plans[0]->fp32;
+  q->plans.assign(plans, plans + count);
+  const int rc = q->fp32 ? queue_build<float>(q) : queue_build<double>(q);
+  if (rc) {
+    pfc_queue_destroy(q);
+    return rc;
+  }
+  *out = q;
+  return PFC_OK;
+}
+
+extern "C" int pfc_queue_step(pfc_queue* q, int64_t nsteps, void* stream) {
+  if (!q) return fail(PFC_E_ARG, "pfc_queue_step: null queue");
+  if (nsteps < 0) return fail(PFC_E_ARG, "pfc_queue_step: negative step count");
+  if (nsteps == 0) return PFC_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  return q->fp32 ? do_queue_step<float>(q, nsteps, s) : do_queue_step<double>(q, nsteps, s);
+}
+
+extern "C" int pfc_queue_status(pfc_queue* q, int32_t* status) {
+  if (!q || !status) return fail(PFC_E_ARG, "pfc_queue_status: null argument");
+  PFC_CUDA(cudaDeviceSynchronize());
+  int v = 0;
+  PFC_CUDA(cudaMemcpy(&v, q->flags, sizeof(int), cudaMemcpyDeviceToHost));
+  *status = v;
+  return PFC_OK;
+}
+
+extern "C" int pfc_queue_info(pfc_queue* q, int32_t* out4) {
+  if (!q || !out4) return fail(PFC_E_ARG, "pfc_queue_info: null argument");
+  out4[0] = q->grid;
+  out4[1] = q->per_sm;
+  out4[2] = q->nitems;
+  out4[3] = (int32_t)q->classes.size();
+  return PFC_OK;
+}
+
+extern "C" int64_t pfc_queue_launch_count(pfc_queue* q) { return q ? q->launches : 0; }
+
+extern "C" int pfc_test_queue_wait(pfc_queue* q, int32_t extra, int64_t wait_limit) {
+  if (!q) return fail(PFC_E_ARG, "pfc_test_queue_wait: null queue");
+  if (extra < 0 || wait_limit < 0) return fail(PFC_E_ARG, "pfc_test_queue_wait: negative argument");
+  q->extra = extra;
+  q->wait_limit = wait_limit ? wait_limit : kQueueWaitLimit;
+  queue_drop_graphs(q);   // graphs recorded with the old arguments would replay them
   return PFC_OK;
 }

@@ -26,6 +26,12 @@ constexpr long long kDenseMinSites = 1LL << 20;
 // column transforms of ny points
 constexpr int kFastMinLog = 5, kFastMaxLogRow = 12, kFastMaxLogCol = 13;
 
+// Work-queue step kernel of one precision (pfc_queue.cuh; pfc_queue_f32.cu, pfc_queue_f64.cu).
+template <class T>
+struct QueueInst {
+  static void* kernel();
+};
+
 struct FastKernel {
   void* fn = nullptr;  // kernel entry, for cudaLaunchKernel
   int tpf = 0;         // threads per transform

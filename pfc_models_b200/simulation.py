@@ -516,13 +516,16 @@ class Batch:
         nsteps = int(nsteps)
         if nsteps <= 0:
             return
-        _lib.check(self.lib.pfc_batch_step(self.handle, nsteps, _stream_ptr(self.torch, self.device)))
+        self._step_call(nsteps)
         for s in self.items:
             if isinstance(s, Simulation):
                 s._version += 1
                 s._mu_current = False
                 for _ in range(nsteps):
                     s.State.t += s.Model.dt
+
+    def _step_call(self, nsteps):
+        _lib.check(self.lib.pfc_batch_step(self.handle, nsteps, _stream_ptr(self.torch, self.device)))
 
     def reduce(self):
         """(F per site, mu per site, mean density) of every simulation as an (n, 3) FP64
@@ -550,6 +553,77 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class QueueBatch(Batch):
+    """The same lockstep stepping as `Batch` in one persistent, cooperative launch per
+    block of steps over a device list of work items (a row or column tile of one member at
+    one step; pfc_queue_*), each item waiting only for the tiles of its own member that it
+    needs. Members must be stdPFC plans on the one-lane power-of-two kernels with the
+    values per thread the work-queue kernel is built with (`queue_kernels(nx, ny,
+    precision)` gives a kernel choice that has them), sides 64 .. 1024. Results are bit
+    for bit those of stepping each plan alone."""
+
+    def __init__(self, items):
+        self.items = list(items)
+        if not self.items:
+            raise ValueError("QueueBatch needs at least one simulation")
+        self.plans = [s.plan if isinstance(s, Simulation) else s for s in self.items]
+        self.lib = self.plans[0].lib
+        self.torch = self.plans[0].torch
+        self.device = self.plans[0].device
+        arr = (ctypes.c_void_p * len(self.plans))(*[p.handle.value for p in self.plans])
+        self.handle = ctypes.c_void_p()
+        with self.torch.cuda.device(self.device):
+            _lib.check(self.lib.pfc_queue_create(arr, len(self.plans), ctypes.byref(self.handle)))
+
+    def _step_call(self, nsteps):
+        _lib.check(self.lib.pfc_queue_step(self.handle, nsteps, _stream_ptr(self.torch, self.device)))
+
+    def status(self):
+        """Status bits of the launches so far (synchronises): 0, or STATUS_TIMEOUT when a
+        bounded wait gave up (the members' states are then undefined)."""
+        v = ctypes.c_int32()
+        _lib.check(self.lib.pfc_queue_status(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def info(self):
+        """{"ctas", "ctas_per_sm", "items_per_step", "classes"} of the launch."""
+        o = (ctypes.c_int32 * 4)()
+        _lib.check(self.lib.pfc_queue_info(self.handle, o))
+        return {"ctas": o[0], "ctas_per_sm": o[1], "items_per_step": o[2], "classes": o[3]}
+
+    @property
+    def classes(self):
+        return self.info()["classes"]
+
+    def launches(self):
+        return int(self.lib.pfc_queue_launch_count(self.handle))
+
+    def _test_wait(self, extra, wait_limit):
+        _lib.check(self.lib.pfc_test_queue_wait(self.handle, int(extra), int(wait_limit)))
+
+    def close(self):
+        if self.handle and self.handle.value:
+            self.lib.pfc_queue_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
+def queue_kernels(nx, ny, precision="fp32"):
+    """A `kernels` choice for plans that join a `QueueBatch`: the values per thread the
+    work-queue kernel holds (FP32: 8 for rows of up to 256 sites and columns of up to 512,
+    else 16; FP64: 8), row tiles of up to 256 threads within 48 KiB of shared memory and
+    the widest column CTA."""
+    fp64 = precision == "fp64"
+    m = nx // 2
+    ee_r = 8 if fp64 or m <= 128 else 16
+    ee_c = 8 if fp64 or ny <= 512 else 16
+    elt = 16 if fp64 else 8
+    tpr = max(1, m // ee_r)
+    tile = 16
+    while tile > 1 and (tile * tpr > 256 or tile * (m + m // 16 + 16) * elt > 48 * 1024):
+        tile //= 2
+    return {"ee_row": ee_r, "ee_col": ee_c, "row_tile": tile, "col_cta": 0}
 
 
 def make_parameters(**kw):

@@ -88,28 +88,36 @@ def shard(points, rank, world):
     return points[rank::world]
 
 
-def run_points(points, steps, precision="fp32", block=1000, device=None, settle=500, warmup=0, mark=None):
+def run_points(points, steps, precision="fp32", block=1000, device=None, settle=500, warmup=0, mark=None,
+               engine="batch"):
     """Steps the points together on one GPU; returns (per-point results, timing).
     F is also reduced `settle` steps before the end (F_prev), so that states still
     evolving can be told from settled ones. `warmup` untimed steps come first (the
     batch's graphs are recorded there); the results then belong to warmup + steps.
-    `mark(True)` / `mark(False)` are called around each timed block (a clock sampler)."""
+    `mark(True)` / `mark(False)` are called around each timed block (a clock sampler).
+    `engine`: "batch" (a `Batch`: one launch per size class and pass, classes on concurrent
+    streams, plans with the batch-tuned kernel variants) or "queue" (a `QueueBatch`: one
+    persistent launch per block of steps over a device work list, plans with the variants
+    of `queue_kernels`)."""
     import torch
 
     from . import stdpfc
-    from .simulation import Batch
+    from .simulation import Batch, QueueBatch, queue_kernels
     from . import _lib, tune
     from .simulation import _PRECISIONS
     sims = []
     for p in points:
         prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=p.r, g=0.0, dt=DT)
-        # the kernel variant measured for batches of this box size, if there is one
-        variant = tune.lookup(p.n, p.n, _PRECISIONS[precision], _lib.MODEL_STD, batched=True) or "auto"
+        if engine == "queue":
+            variant = queue_kernels(p.n, p.n, precision)
+        else:
+            # the kernel variant measured for batches of this box size, if there is one
+            variant = tune.lookup(p.n, p.n, _PRECISIONS[precision], _lib.MODEL_STD, batched=True) or "auto"
         sim = stdpfc.BuildB200_Simulation(prm, stdpfc.Build2DGeometry(p.n, p.n, p.lx, p.ly), precision=precision,
                                           device=device, kernels=variant)
         sim.State.n[...] = initial_field(p)
         sims.append(sim)
-    batch = Batch(sims)
+    batch = QueueBatch(sims) if engine == "queue" else Batch(sims)
     dev = sims[0].plan.device
     s = torch.cuda.current_stream(dev)
     if warmup:
@@ -138,6 +146,7 @@ def run_points(points, steps, precision="fp32", block=1000, device=None, settle=
     red = batch.reduce()
     launches = batch.launches()
     classes = batch.classes
+    status = batch.status() if engine == "queue" else 0
     batch.close()
     for sim in sims:
         sim.plan.close()
@@ -148,18 +157,20 @@ def run_points(points, steps, precision="fp32", block=1000, device=None, settle=
                 F_prev=float(red_prev[i, 0]), settle=settle)
            for i, p in enumerate(points)]
     timing = {"steps": steps, "ms": ms, "sites": sites, "site_steps_per_s": sites * steps / (ms / 1e3),
-              "launches": launches, "classes": classes, "points": len(points)}
+              "launches": launches, "classes": classes, "points": len(points), "engine": engine}
+    if status:
+        raise RuntimeError(f"work-queue batch status {status}: a bounded wait gave up")
     return res, timing
 
 
-def run_sweep(steps=5000, precision="fp32", points=None, block=1000):
+def run_sweep(steps=5000, precision="fp32", points=None, block=1000, engine="batch"):
     """The sweep on every rank of the process group (or alone); results gathered on
     every rank, sorted by point index; timing is the max over ranks."""
     import torch.distributed as dist
     points = sweep_points() if points is None else points
     world = dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
     rank = dist.get_rank() if world > 1 else 0
-    res, timing = run_points(shard(points, rank, world), steps, precision, block)
+    res, timing = run_points(shard(points, rank, world), steps, precision, block, engine=engine)
     if world > 1:
         res, timing = gather_results(res, timing, world)
     return sorted(res, key=lambda d: d["index"]), timing
@@ -260,6 +271,7 @@ def main():
     ap.add_argument("--precision", default="fp32")
     ap.add_argument("--block", type=int, default=1000)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--engine", default="batch", choices=["batch", "queue"])
     a = ap.parse_args()
     import os
 
@@ -272,7 +284,7 @@ def main():
     report = {}
     for precision in a.precision.split(","):
         t0 = time.time()
-        res, timing = run_sweep(a.steps, precision, block=a.block)
+        res, timing = run_sweep(a.steps, precision, block=a.block, engine=a.engine)
         timing["wall_s"] = time.time() - t0
         coex = coexistence(res)
         report[precision] = {"timing": timing, "coexistence": coex, "points": res}
