@@ -467,19 +467,28 @@ def run_ours(args):
     if not args.no_sweep:
         from pfc_models_b200 import sweep
         pts = sweep.shard(sweep.sweep_points(), rank, world)
-        _, tm = sweep.run_points(pts, SWEEP_STEPS, "fp32", block=SWEEP_BLOCK, settle=0, warmup=SWEEP_WARMUP,
-                                 mark=clocks.mark)
-        sw_ms = max_over_ranks(tm["ms"])
-        sw_sites = int(sum_over_ranks(float(tm["sites"])))
+        legs = {}
+        for engine in ("batch", "queue"):
+            _, tm = sweep.run_points(pts, SWEEP_STEPS, "fp32", block=SWEEP_BLOCK, settle=0, warmup=SWEEP_WARMUP,
+                                     mark=clocks.mark, engine=engine)
+            sw_ms = max_over_ranks(tm["ms"])
+            sw_sites = int(sum_over_ranks(float(tm["sites"])))
+            legs[engine] = {"value": sw_sites * SWEEP_STEPS / (sw_ms / 1e3), "ms": sw_ms, "sites": sw_sites,
+                            "gpu_launches": tm["launches"]}
+            torch.cuda.empty_cache()
         swp = {"workload": "512 stdPFC points, r in [-0.6, -0.05] x mean psi in [-0.6, 0], boxes 128^2 / 256^2 / "
-                           "512^2 (seeded choice), half crystal / half liquid starts, FP32-mixed, one batch "
-                           "(a launch per size class and pass, classes on concurrent streams, 16-step graphs)",
-               "steps": SWEEP_STEPS, "warmup": SWEEP_WARMUP, "points": 512, "sites": sw_sites,
-               "value": sw_sites * SWEEP_STEPS / (sw_ms / 1e3), "unit": UNIT, "ms": sw_ms,
-               "gpu_launches": tm["launches"],
+                           "512^2 (seeded choice), half crystal / half liquid starts, FP32-mixed",
+               "steps": SWEEP_STEPS, "warmup": SWEEP_WARMUP, "points": 512, "unit": UNIT,
+               "batch": dict(legs["batch"], engine="a launch per size class and pass, classes on concurrent "
+                                                    "streams, 16-step graphs, batch-tuned variants"),
+               "queue": dict(legs["queue"], engine="one persistent cooperative launch per 16 steps over a device "
+                                                    "work list of row and column tiles, per-plan dependency "
+                                                    "counters"),
                "l2": "not flushed: the 1.4 GB working set exceeds L2"}
+        best = max(legs, key=lambda k: legs[k]["value"])
+        swp["value"] = legs[best]["value"]
+        swp["faster_engine"] = best
         swp["step_achieved_gbs"] = 24 * swp["value"] / 1e9
-        torch.cuda.empty_cache()
     clk = clocks.stop()
 
     # ---- accuracy over the workload's full length (outside every timed region)
