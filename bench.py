@@ -286,6 +286,7 @@ def run_kernel_case(a):
             sims.append(s)
         b = QueueBatch(sims) if a.queue else Batch(sims)
         b.step(1)
+        b.step(16)   # records the 16-step graphs outside the timed region
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record()
