@@ -164,7 +164,10 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
 /* Variant of the power-of-two step kernels (0 in a field = the precision's default):
  * complex values per thread of the row and of the column kernel (FP32: 8, 16 or 32,
  * default 32; FP64: 8 or 16, default 16) and rows per CTA of the row kernel
- * (1, 2, 4, 8 or 16). Other values make pfc_plan_create return PFC_E_ARG. The
+ * (1 .. 16; a height other than a power of two, which spreads the rows evenly over the
+ * SMs, is taken where the CTA is whole multiples of it, else the plan uses the run-time
+ * kernels; packed: a power of two >= 2). Other values make pfc_plan_create return
+ * PFC_E_ARG. The
  * autotuner (pfc_models_b200/tune.py) measures these per grid and caches the best. */
 /* OR-ed into a PFC_FLAG_ROW_EE / PFC_FLAG_COL_EE value: that pass's two-lane packed FP32
  * kernel (8 or 16 values per lane) */

@@ -235,7 +235,7 @@ constexpr unsigned kStatusTimeout = 2;   // PFC_STATUS_TIMEOUT: a bounded wait g
 template <class T>
 struct FastRowArgs {
   int ny, rows, ld;
-  int rows_log2;             // rows = 1 << rows_log2
+  int rows_log2;             // rows = 1 << rows_log2, or -1 when rows is not a power of two
   const BatchBufs* batch;    // null: one plan, the pointers below
   const cplx<T>* in;         // W, column-major [kx][y]
   cplx<T>* out;              // V, column-major
@@ -351,8 +351,12 @@ __device__ __forceinline__ void row_step_body(const FastRowArgs<T>& a, const Bat
   // ---- transposing tile load: element (kx, y0 + r) -> sm[r * ld + pad(kx)], issued as
   // asynchronous global->shared copies so that every load of the tile is in flight at once.
   // nthreads is a multiple of rows: each thread keeps one row and walks kx with a fixed
-  // stride, so the addresses advance by constants.
-  const int tr = threadIdx.x & (rows - 1), kx0 = threadIdx.x >> rl2, kstep = nthreads >> rl2;
+  // stride, so the addresses advance by constants. (A tile of a row count other than a
+  // power of two spreads a grid's rows evenly over the SMs: 2048 rows in 293 tiles of 7,
+  // two per SM, where 256 tiles of 8 leave 40 SMs with one.)
+  const int tr = rl2 >= 0 ? (int)(threadIdx.x & (rows - 1)) : (int)threadIdx.x % rows;
+  const int kx0 = rl2 >= 0 ? (int)(threadIdx.x >> rl2) : (int)threadIdx.x / rows;
+  const int kstep = rl2 >= 0 ? nthreads >> rl2 : nthreads / rows;
   const bool rvalid = y0 + tr < ny;
   const size_t gstep = (size_t)kstep * ny;
   {

@@ -414,7 +414,9 @@ int fast_row_side(pfc_plan* h, int ee, int tile, std::vector<long double>& tw, F
   int ld = h->m + (h->m >> P);
   while (ld % slots != want) ++ld;
   const size_t smem = (size_t)rows * ld * elt;
-  if (ngr * tpr > 1024 || smem > 200 * 1024 || ilog2_exact(rows) < 0) return PFC_OK;
+  // a row count other than a power of two needs the CTA to be whole multiples of it (the
+  // transposing tile copies give each thread one row)
+  if (ngr * tpr > 1024 || smem > 200 * 1024 || (ilog2_exact(rows) < 0 && (ngr * tpr) % rows)) return PFC_OK;
   o.rows = rows;
   o.threads = ngr * tpr;
   o.ld = ld;
@@ -569,8 +571,8 @@ int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
     return fail(PFC_E_ARG, "pfc_plan_create: column kernel values per thread %d not built (FP32: 8, 16 or 32; "
                 "FP64: 8 or 16; packed: 8 or 16 per lane)", ee_c);
   const int tile = PFC_FLAG_ROW_TILE_OF(flags);
-  if (tile && (tile > 16 || (tile & (tile - 1)) || (row_packed && tile < 2)))
-    return fail(PFC_E_ARG, "pfc_plan_create: row tile %d is not a power of two <= 16 (>= 2 packed)", tile);
+  if (tile && (tile > 16 || (row_packed && ((tile & (tile - 1)) || tile < 2))))
+    return fail(PFC_E_ARG, "pfc_plan_create: row tile %d: at most 16 rows (packed: a power of two >= 2)", tile);
   if (flags & PFC_FLAG_GENERIC_ONLY) return PFC_OK;
   const int col_cta = PFC_FLAG_COL_CTA_OF(flags);
   FastRowSide r;

@@ -100,6 +100,22 @@ def _store(path, key, entry):
         _memo[path] = d
 
 
+def balanced_tiles(ny, sms=None):
+    """Row-tile heights other than powers of two that spread ny rows evenly over the SMs at
+    two and four CTAs per SM (2048 rows: 7, 293 tiles, two per SM, where 8-row tiles leave 40
+    of 148 SMs with one). The plan takes a height only where its CTA is whole multiples of
+    it."""
+    if sms is None:
+        import torch
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    out = []
+    for per_sm in (2, 4):
+        t = -(-ny // (per_sm * sms))
+        if 2 < t < 16 and t & (t - 1) and t not in out:
+            out.append(t)
+    return tuple(out)
+
+
 def tune(nx, ny, precision="fp32", model="std", steps=20, warmup=3, save=True, path=None, batch=1):
     """Times the variants for one grid; returns the chosen entry (and caches it).
     With batch > 1 every variant steps `batch` plans together through a `Batch` and the
@@ -124,7 +140,7 @@ def tune(nx, ny, precision="fp32", model="std", steps=20, warmup=3, save=True, p
     ees = EE_CHOICES[prec]
     # row candidates (packed?, values per thread or lane, tile, TMA) and column candidates
     # (packed?, values); each row candidate is timed beside the column candidates in turn
-    row_c = [(False, e, t, 0) for e, t in itertools.product(ees, TILE_CHOICES)]
+    row_c = [(False, e, t, 0) for e, t in itertools.product(ees, TILE_CHOICES + balanced_tiles(ny))]
     col_c = [(False, e) for e in ees]
     if prec == _lib.FP32_MIXED:
         row_c += [(True, e, t, m) for e, t, m in itertools.product(PACKED_EE, PACKED_TILES, (0, 1))]

@@ -508,3 +508,34 @@ def orc_F(model, prm, geom, field):
     s = orc.OracleSim(model, orc.Params(**prm), geom)
     s.set_field(field)
     return s.free_energy()
+
+
+@pytest.mark.parametrize("precision,ee", [("fp32", 32), ("fp32", 16), ("fp64", 16), ("fp64", 8)])
+@pytest.mark.parametrize("model", ["std", "log"])
+def test_row_tile_heights_other_than_powers_of_two(precision, ee, model):
+    """Row tiles of 3, 5, 6 and 7 rows (the heights that spread a grid's rows evenly over the
+    SMs; the last tile of 2048 rows in 7s holds 4) partition the same row transforms as
+    8-row tiles: the states are bit-identical after 12 steps, on the power-of-two and the
+    odd-factor register-resident kernels."""
+    for nx, ny in ((128, 2048), (96, 2048)):
+        mod = stdpfc if model == "std" else logpfc
+        if model == "std":
+            prm = stdpfc.BuildStdPFCModelParameters(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.3, g=0.2, dt=0.3)
+            mean = -0.3
+        else:
+            prm = logpfc.BuildLogPFCModelParameters(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=0.05)
+            mean = 0.55
+        geom = mod.Build2DGeometry(nx, ny, nx * np.pi / 4, ny * np.pi / 4)
+        f0 = mean + 0.05 * np.random.default_rng(nx + ny).uniform(-1, 1, (ny, nx))
+        out = {}
+        for tile in (8, 7, 6, 5, 3):
+            sim = mod.BuildB200_Simulation(prm, geom, precision=precision,
+                                           kernels={"ee_row": ee, "ee_col": 8, "row_tile": tile})
+            v = sim.plan.variant()
+            assert v["fast"] and v["row_tile"] == tile, (nx, tile, v)
+            (sim.State.n if model == "std" else sim.State.phi)[...] = f0
+            sim.TimeSteps(12)
+            out[tile] = sim.plan.get_state().cpu().numpy()
+            sim.plan.close()
+        for tile in (7, 6, 5, 3):
+            assert np.array_equal(out[tile], out[8]), (nx, tile)
