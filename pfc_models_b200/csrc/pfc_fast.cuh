@@ -359,10 +359,13 @@ __device__ __forceinline__ void row_step_body(const FastRowArgs<T>& a, const Bat
   const int kstep = rl2 >= 0 ? nthreads >> rl2 : nthreads / rows;
   const bool rvalid = y0 + tr < ny;
   const size_t gstep = (size_t)kstep * ny;
+  // With one row per transform group (rows == groups, the usual tile) the stride is TPF:
+  // the loops over a thread's elements then have compile-time trip counts and unroll.
+  const bool unit = kstep == TPF;
   {
     cplx<T>* drow = sm + tr * ld;
-    const cplx<T>* src = gin + (size_t)kx0 * ny + (y0 + tr);
-    for (int kx = kx0; kx < M; kx += kstep, src += gstep) {
+    const cplx<T>* src0 = gin + (size_t)kx0 * ny + (y0 + tr);
+    auto copy = [&](int kx, const cplx<T>* src) {
       cplx<T>* dst = drow + padi<P>(kx);
       if (rvalid) {
         const unsigned sdst = (unsigned)__cvta_generic_to_shared(dst);
@@ -371,6 +374,13 @@ __device__ __forceinline__ void row_step_body(const FastRowArgs<T>& a, const Bat
       } else {
         *dst = mk(T(0), T(0));
       }
+    };
+    if (unit) {
+#pragma unroll
+      for (int j = 0; j < M / TPF; ++j) copy(kx0 + j * TPF, src0 + (size_t)j * gstep);
+    } else {
+      const cplx<T>* src = src0;
+      for (int kx = kx0; kx < M; kx += kstep, src += gstep) copy(kx, src);
     }
   }
   // twiddle tables are read through the L1 cache
@@ -397,8 +407,11 @@ __device__ __forceinline__ void row_step_body(const FastRowArgs<T>& a, const Bat
     cplx<T> v[EE];
     // ---- inverse-real pre-twiddle, in place, one (k, M - k) pair per step:
     // Z[k] = S + U, Z[M - k] = conj(S - U), S = X[k] + conj X[M-k], U = i conj(r_k) (X[k] - conj X[M-k])
-#pragma unroll 2
-    for (int k = t; k <= M / 2; k += TPF) {
+    // (k = t + j TPF, j < M / (2 TPF) + 1, the last only while k <= M / 2)
+#pragma unroll
+    for (int j = 0; j <= M / (2 * TPF); ++j) {
+      const int k = t + j * TPF;
+      if (k > M / 2) break;
       if (k == 0) {
         const cplx<T> x0 = row[0];
         row[0] = mk(x0.x + x0.y, x0.x - x0.y);
@@ -469,8 +482,7 @@ __device__ __forceinline__ void row_step_body(const FastRowArgs<T>& a, const Bat
   if (rvalid) {
     const cplx<T>* srow = sm + tr * ld;
     cplx<T>* col0 = gout + (y0 + tr);
-#pragma unroll 2
-    for (int k = kx0; k <= M / 2; k += kstep) {
+    auto post = [&](int k) {
       if (k == 0) {
         const cplx<T> z0 = srow[0];
         col0[0] = mk(z0.x + z0.y, z0.x - z0.y);
@@ -481,6 +493,17 @@ __device__ __forceinline__ void row_step_body(const FastRowArgs<T>& a, const Bat
         col0[(size_t)k * ny] = e + o;
         if (k != M / 2) col0[(size_t)(M - k) * ny] = conj(e - o);
       }
+    };
+    if (unit) {
+#pragma unroll
+      for (int j = 0; j <= M / (2 * TPF); ++j) {
+        const int k = kx0 + j * TPF;
+        if (k > M / 2) break;
+        post(k);
+      }
+    } else {
+#pragma unroll 2
+      for (int k = kx0; k <= M / 2; k += kstep) post(k);
     }
   }
 }

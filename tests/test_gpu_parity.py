@@ -444,7 +444,7 @@ def test_kernel_variant_errors():
     from pfc_models_b200 import _lib
     prm = stdpfc.BuildStdPFCModelParameters(epsilon=-0.3, g=0.0, dt=0.5)
     geom = stdpfc.Build2DGeometry(128, 128, 32 * np.pi, 32 * np.pi)
-    for bad in ({"ee_row": 4}, {"ee_col": 64}, {"row_tile": 3}):
+    for bad in ({"ee_row": 4}, {"ee_col": 64}, {"row_tile": 17}, {"row_tile": 3, "packed": 1}):
         with pytest.raises(_lib.PfcError) as e:
             stdpfc.BuildB200_Simulation(prm, geom, precision="fp32", kernels=bad)
         assert e.value.code == _lib.PFC_E_ARG
