@@ -642,7 +642,7 @@ __device__ __forceinline__ void col_step_body(const FastColArgs<T>& a, const Bat
       for (int j = 0; j < CH; ++j) {
         const int ky = t + (j0 + j) * TPF;
         const int kh = ky <= NY / 2 ? ky : NY - ky;
-        cw[j] = ldsc(gcoef + ccb + kh);
+        cw[j] = ldgc(gcoef + ccb + kh);   // cached: modes ky and NY - ky share an entry
         p[j] = ld_field<COHERENT>(static_cast<const cplx<T>*>(gnin) + cb + ky);
       }
 #pragma unroll
