@@ -145,6 +145,8 @@ int pfc_plan_info(pfc_plan* plan, int64_t* out16);
 #define PFC_FLAG_PDL 4            /* launch the power-of-two step kernels with programmatic
                                      dependent launch: each may start (and send its column's
                                      state towards L2) while the kernel before it drains */
+#define PFC_FLAG_PDL_COL 128      /* as PFC_FLAG_PDL for the column step kernel only (the row
+                                     kernel waits for the column kernel before it launches) */
 #define PFC_FLAG_NO_ONE_CTA 8     /* step small FP64 mixed-radix grids with the two-kernel
                                      step instead of the one-CTA whole-grid kernel */
 #define PFC_FLAG_EXTV 32          /* log PFC with an external potential and the re-optimised

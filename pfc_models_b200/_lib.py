@@ -21,6 +21,7 @@ FIELD_N, FIELD_MU, FIELD_LOCAL_MU, FIELD_LOCAL_N, FIELD_NONLIN_MU = range(5)
 FIELD_OF_CURRENT = 0x100
 SPEC_N_HAT, SPEC_N_HAT_NOW = 0, 1
 FLAG_GENERIC_ONLY, FLAG_NO_GRAPHS, FLAG_PDL = 1, 2, 4
+FLAG_PDL_COL = 128
 FLAG_NO_ONE_CTA = 8
 FLAG_PACKED = 16
 FLAG_EXTV = 32
@@ -38,13 +39,15 @@ def flag_variant(ee_row=0, ee_col=0, row_tile=0, col_cta=0, pdl=0, packed=0, tma
     """problem.flags bits selecting a step-kernel variant (PFC_FLAG_ROW_EE & co.).
     `packed`: 0 one-lane kernels, 1 the two-lane packed FP32 kernels on both passes,
     2 on the row pass only, 3 on the column pass only (then ee_* of a packed pass count
-    values per lane). `generic`: the run-time mixed-radix kernels instead."""
+    values per lane). `pdl`: 1 both step kernels as programmatic dependent launches, 2 the
+    column kernel only. `generic`: the run-time mixed-radix kernels instead."""
     cc = {0: 0, 1: 1, 2: 2, 4: 3}[int(col_cta)]
     packed = int(packed)
     er = int(ee_row) | (EE_PACKED if packed == PACKED_ROW else 0)
     ec = int(ee_col) | (EE_PACKED if packed == PACKED_COL else 0)
     return (er << 8) | (ec << 16) | (int(row_tile) << 24) | (cc << 29) | \
-        (FLAG_PDL if pdl else 0) | (FLAG_PACKED if packed == PACKED_BOTH else 0) | (FLAG_TMA if tma else 0) | \
+        (FLAG_PDL if pdl == 1 else FLAG_PDL_COL if pdl == 2 else 0) | \
+        (FLAG_PACKED if packed == PACKED_BOTH else 0) | (FLAG_TMA if tma else 0) | \
         (FLAG_GENERIC_ONLY if generic else 0)
 
 # every symbol include/pfc_b200.h declares, with (restype, argtypes)

@@ -607,11 +607,12 @@ int setup_fast(pfc_plan* h, std::vector<long double>& tw) {
 }
 
 // One row pass of a step: W -> V (of every plan in `table` when batched).
-// Launches a power-of-two step kernel, with PFC_FLAG_PDL as a programmatic dependent
-// launch (the kernel may start while the previous kernel of the stream drains; it waits
-// for it with griddepcontrol.wait before reading its outputs).
+// Launches a power-of-two step kernel, with PFC_FLAG_PDL (or, for the column kernel,
+// PFC_FLAG_PDL_COL) as a programmatic dependent launch (the kernel may start while the
+// previous kernel of the stream drains; it waits for it with griddepcontrol.wait before
+// reading its outputs).
 inline cudaError_t launch_step_kernel(const pfc_plan* h, const void* fn, dim3 grid, dim3 block, void** args,
-                                      size_t smem, cudaStream_t s) {
+                                      size_t smem, cudaStream_t s, bool col = false) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = grid;
   cfg.blockDim = block;
@@ -621,7 +622,7 @@ inline cudaError_t launch_step_kernel(const pfc_plan* h, const void* fn, dim3 gr
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = (h->prob.flags & PFC_FLAG_PDL) ? 1 : 0;
+  cfg.numAttrs = ((h->prob.flags & PFC_FLAG_PDL) || (col && (h->prob.flags & PFC_FLAG_PDL_COL))) ? 1 : 0;
   return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
@@ -722,7 +723,7 @@ int launch_step_col(pfc_plan* h, cudaStream_t s, const BatchBufs* table = nullpt
     FastColArgs<T> a = fast_col_args<T>(h, table);
     void* args[] = {(void*)&a};
     cudaError_t e = launch_step_kernel(h, h->fast_col_fn, dim3(h->fc_grid, count), dim3(h->fc_threads), args,
-                                       h->fc_smem, s);
+                                       h->fc_smem, s, true);
     ++h->launches;
     if (e != cudaSuccess) return fail(PFC_E_CUDA, "column step launch failed: %s", cudaGetErrorString(e));
     return PFC_OK;

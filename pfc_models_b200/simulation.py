@@ -364,7 +364,8 @@ def _kernel_flags(kernels, prob):
     """problem.flags bits for the `kernels` choice of a Simulation: "auto" (the variant
     the autotuner cached for this grid, else the defaults), "default", "generic" (the
     mixed-radix kernels everywhere), or a dict with any of "ee_row", "ee_col",
-    "row_tile", "col_cta" (columns per CTA of the column kernel), "pdl" and "packed"
+    "row_tile", "col_cta" (columns per CTA of the column kernel), "pdl" (1: both step kernels
+    as programmatic dependent launches, 2: the column kernel only) and "packed"
     (1: the two-lane packed FP32 kernels on both passes, 2: row pass only, 3: column pass
     only; ee_* of a packed pass count values per lane), "tma" (the packed row kernel's tile
     staged by the tensor memory accelerator)."""
@@ -408,7 +409,7 @@ class Simulation:
         prob.clamp_log = 1 if clamp_log else 0
         prob.flags = _kernel_flags(kernels, prob) | (0 if graphs else _lib.FLAG_NO_GRAPHS)
         if pdl is not None:   # None: as the variant says
-            prob.flags = (prob.flags & ~_lib.FLAG_PDL) | (_lib.FLAG_PDL if pdl else 0)
+            prob.flags = (prob.flags & ~(_lib.FLAG_PDL | _lib.FLAG_PDL_COL)) | (_lib.FLAG_PDL if pdl else 0)
         if not one_cta:       # small FP64 mixed-radix grids: keep the two-kernel step
             prob.flags |= _lib.FLAG_NO_ONE_CTA
         prob.flags |= int(_flags)

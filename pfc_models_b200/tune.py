@@ -312,7 +312,7 @@ def refine(nx, ny, precision, model, base, batch=1, min_gain=0.01):
     if nx & (nx - 1) or ny & (ny - 1):
         generic_us, _ = _time_blocks(nx, ny, precision, model, {"generic": 1}, batch, fast=False)
     for cc in (0,) + COL_CTA_CHOICES:
-        for pdl in (0, 1):
+        for pdl in (0, 1, 2):   # 2: the column kernel only
             us, threads = _time_blocks(nx, ny, precision, model, dict(v0, col_cta=cc, pdl=pdl), batch,
                                        skip=lambda th: (th, pdl) in seen)
             if threads is None:

@@ -88,19 +88,22 @@ def test_graph_replay_matches_direct_launches(precision):
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("model", ["std", "log"])
 def test_launch_modes_match_serialised_launches(precision, model):
-    """A step kernel that starts while the previous one drains (griddepcontrol), and
-    column kernels of 1, 2 or 4 columns per CTA, give the same bits as serialised
-    launches of the default shape, replayed from graphs or launched directly."""
-    def make(graphs, pdl, col_cta=0):
+    """A step kernel that starts while the previous one drains (griddepcontrol; both
+    kernels, or the column kernel only), and column kernels of 1, 2 or 4 columns per CTA,
+    give the same bits as serialised launches of the default shape, replayed from graphs or
+    launched directly."""
+    def make(graphs, pdl, col_cta=0, pdl_col=False):
         kernels = "auto"
-        if col_cta:
+        if col_cta or pdl_col:
             v = make(False, False).plan.variant()
-            kernels = {"ee_row": v["ee_row"], "ee_col": v["ee_col"], "row_tile": v["row_tile"], "col_cta": col_cta}
+            kernels = {"ee_row": v["ee_row"], "ee_col": v["ee_col"], "row_tile": v["row_tile"], "col_cta": col_cta,
+                       "pdl": 2 if pdl_col else 0}
         if model == "std":
             return _std_sim(512, 256, -0.25, -0.25, precision, seed=5, graphs=graphs, pdl=pdl, kernels=kernels)
         return _log_sim(256, 256, precision, seed=5, graphs=graphs, pdl=pdl, kernels=kernels)
     ref = make(False, False)
-    sims = [make(True, True), make(False, True), make(True, False, 1), make(True, True, 4)]
+    sims = [make(True, True), make(False, True), make(True, False, 1), make(True, True, 4),
+            make(True, None, pdl_col=True), make(False, None, pdl_col=True)]
     assert sims[2].plan.info()["fast_col_ctas"] == sims[2].Geometry.Nx // 2    # one column per CTA
     for n in (17, 1, 32, 3):
         ref.TimeSteps(n)

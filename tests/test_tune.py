@@ -16,7 +16,7 @@ def test_packaged_table_is_used_without_a_user_cache(tmp_path, monkeypatch):
     for e in table.values():
         # 0: the plan's own choice (a side with an odd factor holds a fixed number per thread)
         assert e["ee_row"] in (0, 8, 16, 32) and e["ee_col"] in (0, 8, 16, 32) and e["row_tile"] in (1, 2, 4, 8, 16)
-        assert e.get("col_cta", 0) in (0, 1, 2, 4) and e.get("pdl", 0) in (0, 1)
+        assert e.get("col_cta", 0) in (0, 1, 2, 4) and e.get("pdl", 0) in (0, 1, 2)
     # batch-measured entries are preferred for batches and fall back to the single-plan ones
     bkey = "NVIDIA B200|512x512|fp32|std|batch"
     assert bkey in table
@@ -64,10 +64,13 @@ def test_flag_encoding_matches_header():
     # columns per CTA 1, 2, 4 -> field values 1, 2, 3 in bits 29-30
     assert [_lib.flag_variant(col_cta=c) >> 29 for c in (0, 1, 2, 4)] == [0, 1, 2, 3]
     assert _lib.flag_variant(pdl=1) == _lib.FLAG_PDL
+    assert _lib.flag_variant(pdl=2) == _lib.FLAG_PDL_COL
+    assert re.search(r"#define PFC_FLAG_PDL_COL 128", src)
 
 
 def test_refine_keeps_defaults_unless_clearly_faster(monkeypatch):
-    """Second stage: (columns per CTA, programmatic launch) is taken from whole-step
+    """Second stage: (columns per CTA, programmatic launch of both kernels or the column
+    kernel only) is taken from whole-step
     timings only when at least 1 % faster than the defaults; choices whose launch equals
     one timed already (same column-kernel threads) are not timed again. The timings are
     faked, so this runs without a GPU."""
@@ -86,15 +89,15 @@ def test_refine_keeps_defaults_unless_clearly_faster(monkeypatch):
     base = {"ee_row": 32, "ee_col": 16, "row_tile": 8}
     # 256 threads by default (2 columns of 128); 4 columns clamp to the same launch
     threads = {0: 256, 1: 128, 2: 256, 4: 256}
-    times = {(0, 0): 40.0, (0, 1): 39.8, (1, 0): 45.0, (1, 1): 47.0}
+    times = {(0, 0): 40.0, (0, 1): 39.8, (0, 2): 39.9, (1, 0): 45.0, (1, 1): 47.0, (1, 2): 46.0}
     monkeypatch.setattr(tune, "_time_blocks", fake(times, threads))
     r = tune.refine(2048, 2048, "fp32", "std", base)
     assert (r["col_cta"], r["pdl"]) == (0, 0)            # 0.5 % faster is not enough
     # 2 and 4 columns per CTA launch like the default here: skipped, not timed
-    assert calls == [(0, 0), (0, 1), (1, 0), (1, 1)]
-    assert set(r["refine_us"]) == {"0/0", "0/1", "1/0", "1/1"}
+    assert calls == [(0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2)]
+    assert set(r["refine_us"]) == {"0/0", "0/1", "0/2", "1/0", "1/1", "1/2"}
     calls.clear()
-    times = {(0, 0): 12.0, (0, 1): 11.5, (1, 0): 9.4, (1, 1): 8.6}
+    times = {(0, 0): 12.0, (0, 1): 11.5, (0, 2): 11.6, (1, 0): 9.4, (1, 1): 8.6, (1, 2): 8.9}
     monkeypatch.setattr(tune, "_time_blocks", fake(times, {0: 256, 1: 128, 2: 256, 4: 256}))
     r = tune.refine(128, 128, "fp32", "std", base)
     assert (r["col_cta"], r["pdl"]) == (1, 1)
