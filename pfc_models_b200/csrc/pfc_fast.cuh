@@ -56,6 +56,11 @@ struct FastSeq {
   __host__ __device__ static constexpr int twB(int p) { return p <= 1 ? 0 : twB(p - 1) + nsB(p - 1) * (radB(p - 1) - 1); }
   __host__ __device__ static constexpr int sizeA() { return twA(NPASS); }
   __host__ __device__ static constexpr int sizeB() { return twB(NPASS); }
+  // A and B run the same radices in the same order (all passes of one radix): their pass
+  // tables are equal, and the plans keep one copy for both
+  __host__ __device__ static constexpr bool symmetric(int p = 0) {
+    return p >= NPASS ? true : (radA(p) == radB(p) && symmetric(p + 1));
+  }
 };
 
 // Pad shift of the exchange buffers for EE values per thread (the effective EE of the

@@ -18,6 +18,10 @@ void seq_tables(std::vector<long double>& tw, int& offA, int& offB) {
   using S = FastSeq<N, EE, RadixCap<T>::value>;
   const long double twopi = 6.283185307179586476925286766559L;
   for (int seq = 0; seq < 2; ++seq) {
+    if (seq == 1 && S::symmetric()) {   // B's table is A's: one copy (half the L1 footprint)
+      offB = offA;
+      break;
+    }
     (seq == 0 ? offA : offB) = (int)(tw.size() / 2);
     for (int p = 1; p < S::NPASS; ++p) {
       const int R = seq == 0 ? S::radA(p) : S::radB(p);

@@ -26,6 +26,10 @@ template <int N, int EE>
 void seq_tables(std::vector<long double>& tw, int& offA, int& offB) {
   using S = PkSeq<N, EE>;
   for (int seq = 0; seq < 2; ++seq) {
+    if (seq == 1 && S::symmetric()) {   // B's table is A's: one copy (half the L1 footprint)
+      offB = offA;
+      break;
+    }
     align4(tw);
     (seq == 0 ? offA : offB) = (int)(tw.size() / 2);
     for (int p = 1; p < S::NPASS; ++p) {
