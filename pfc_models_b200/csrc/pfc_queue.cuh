@@ -103,8 +103,8 @@ __device__ __forceinline__ bool queue_wait(const unsigned* cnt, unsigned target,
 // registers and unrolling of its step kernel (plus the saved registers of the call).
 template <class T, int M>
 __device__ __noinline__ void queue_row_body(const QueueClass<T>* C, const BatchBufs* table, int tile, int local) {
-  row_step_body<T, M, queue_row_ee(sizeof(T) == 8, M), kModelStd>(C->row, table, tile, local, C->row_threads,
-                                                                  NoSync{});
+  row_step_body<T, M, queue_row_ee(sizeof(T) == 8, M), kModelStd, true>(C->row, table, tile, local,
+                                                                        C->row_threads, NoSync{});
 }
 template <class T, int NY>
 __device__ __noinline__ void queue_col_body(const QueueClass<T>* C, const BatchBufs* table, int tile, int local) {
