@@ -140,9 +140,14 @@ template <class T>
 __global__ void __launch_bounds__(kQueueThreads, 4) queue_step_kernel(QueueArgs<T> q) {
   __shared__ int go, item;
   const unsigned total = (unsigned)q.nitems * (unsigned)q.nsteps;
+  // the first thread takes the next ticket while the current item runs (its round trip to
+  // L2 then overlaps the body); items are still claimed in order, and a claimed item waits
+  // only for earlier ones, so the walk stays free of deadlock
+  unsigned next = 0;
+  if (threadIdx.x == 0) next = atomicAdd(q.ticket, 1u);
   for (;;) {
     if (threadIdx.x == 0) {
-      const unsigned gi = atomicAdd(q.ticket, 1u);
+      const unsigned gi = next;
       bool ok = gi < total && !*reinterpret_cast<volatile int*>(q.abort);
       if (ok) {
         const int s = (int)(gi / (unsigned)q.nitems), i = (int)(gi - (unsigned)s * (unsigned)q.nitems);
@@ -157,6 +162,7 @@ __global__ void __launch_bounds__(kQueueThreads, 4) queue_step_kernel(QueueArgs<
       }
       go = ok;
       item = (int)gi;
+      if (ok) next = atomicAdd(q.ticket, 1u);
     }
     __syncthreads();
     if (!go) return;
