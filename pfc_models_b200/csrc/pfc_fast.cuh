@@ -394,6 +394,19 @@ __device__ __forceinline__ void row_step_body(const FastRowArgs<T>& a, const Bat
     } else if (unit) {
 #pragma unroll
       for (int j = 0; j < M / TPF; ++j) copy(kx0 + j * TPF, src0 + (size_t)j * gstep);
+    } else if (!COHERENT && rvalid) {
+      // several rows per transform group: the same loads, eight in flight at a time
+      constexpr int B = 8;
+      const cplx<T>* src = src0;
+      int kx = kx0;
+      for (; kx + (B - 1) * kstep < M; kx += B * kstep, src += (size_t)B * gstep) {
+        cplx<T> tmp[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) tmp[b] = ldsc(src + (size_t)b * gstep);
+#pragma unroll
+        for (int b = 0; b < B; ++b) drow[padi<P>(kx + b * kstep)] = tmp[b];
+      }
+      for (; kx < M; kx += kstep, src += gstep) drow[padi<P>(kx)] = ldsc(src);
     } else {
       const cplx<T>* src = src0;
       for (int kx = kx0; kx < M; kx += kstep, src += gstep) copy(kx, src);
