@@ -28,6 +28,9 @@ void* pick_row(int model, int rset) {
   if (rset == kRadixSmall)
     return log ? (void*)row_kernel<T, MODE, kModelLog, kRadixSmall, 256>
                : (void*)row_kernel<T, MODE, kModelStd, kRadixSmall, 256>;
+  if (rset == kRadixSmallBig)
+    return log ? (void*)row_kernel<T, MODE, kModelLog, kRadixSmall, 1024>
+               : (void*)row_kernel<T, MODE, kModelStd, kRadixSmall, 1024>;
   if (rset == kRadixPow2Big)
     return log ? (void*)row_kernel<T, MODE, kModelLog, kRadixPow2, 1024>
                : (void*)row_kernel<T, MODE, kModelStd, kRadixPow2, 1024>;
@@ -50,6 +53,9 @@ void* pick_col(int rset) {
   }
   if (rset == kRadixSmall && MODE != kColParseval && MODE != kColExport) return (void*)col_kernel<T, MODE, kRadixSmall, 256>;
   if (rset == kRadixPow2Big) return (void*)col_kernel<T, MODE, kRadixPow2, 1024>;
+  if (rset == kRadixSmallBig)   // (the Parseval and export modes transform nothing)
+    return (MODE == kColParseval || MODE == kColExport) ? (void*)col_kernel<T, MODE, kRadixPow2, 1024>
+                                                        : (void*)col_kernel<T, MODE, kRadixSmall, 1024>;
   if (MODE == kColParseval || MODE == kColExport || rset == kRadixPow2) return (void*)col_kernel<T, MODE, kRadixPow2, 256>;
   return (void*)col_kernel<T, MODE, kRadixAll, 256>;
 }

@@ -1253,7 +1253,10 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
     h->row_ld = generic_pad(m - 1) + 2;
     if (h->row_ld % 2 == 0) ++h->row_ld;
     if (h->row_tpf > kBlockMax && h->row_rset == kRadixPow2 && h->row_tpf <= 1024) h->row_rset = kRadixPow2Big;
-    const int kBlockMax = h->row_rset == kRadixPow2Big ? 1024 : pfc_block_max;
+    if (h->row_tpf > kBlockMax && (h->row_rset == kRadixSmall || h->row_rset == kRadixSmallDense) &&
+        h->row_tpf <= 1024)
+      h->row_rset = kRadixSmallBig;
+    const int kBlockMax = (h->row_rset == kRadixPow2Big || h->row_rset == kRadixSmallBig) ? 1024 : pfc_block_max;
     if (h->row_tpf > kBlockMax)
       return cleanup_fail(fail(PFC_E_ARG, "pfc_plan_create: row transform of %d points needs %d threads", m, h->row_tpf));
     const int rows_min = std::max(1, 32 / h->row_tpf);       // whole warps
@@ -1275,7 +1278,10 @@ int pfc_plan_create(const pfc_problem* p, pfc_plan** out) {
     h->col_ld = generic_pad(p->ny - 1) + 2;   // padded column plus one
     if (h->col_ld % 2 == 0) ++h->col_ld;
     if (h->col_tpf > kBlockMax && h->col_rset == kRadixPow2 && h->col_tpf <= 1024) h->col_rset = kRadixPow2Big;
-    const int kBlockMax = h->col_rset == kRadixPow2Big ? 1024 : pfc_block_max;
+    if (h->col_tpf > kBlockMax && (h->col_rset == kRadixSmall || h->col_rset == kRadixSmallDense) &&
+        h->col_tpf <= 1024)
+      h->col_rset = kRadixSmallBig;
+    const int kBlockMax = (h->col_rset == kRadixPow2Big || h->col_rset == kRadixSmallBig) ? 1024 : pfc_block_max;
     if (h->col_tpf > kBlockMax)
       return cleanup_fail(fail(PFC_E_ARG, "pfc_plan_create: column transform of %d points needs %d threads", p->ny, h->col_tpf));
     int cols = std::max(1, 32 / h->col_tpf);

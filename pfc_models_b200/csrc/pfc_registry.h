@@ -20,6 +20,10 @@ constexpr int kRadixAllDense = 3;
 // Grids with prime factors 2, 3, 5, 7 only: the smaller radix set (kRadixSmall), and its
 // two-CTA step build as above.
 constexpr int kRadixSmallDense = 5;
+// The small-radix generic kernels built for 1024-thread blocks: transforms whose radix-5 or
+// radix-7 pass has more than 256 butterflies (2560 = 5 x 512, 3584 = 7 x 512, 5120 points);
+// they hold one butterfly of such a pass per thread, so the block grows with the length.
+constexpr int kRadixSmallBig = 6;
 constexpr long long kDenseMinSites = 1LL << 20;
 
 // log2 sizes of the power-of-two step kernels: row transforms of M = nx/2 points,
