@@ -543,29 +543,38 @@ def test_row_tile_heights_other_than_powers_of_two(precision, ee, model):
 
 @pytest.mark.parametrize("nx,ny", [(2560, 2560), (1792, 3584), (640, 5120)])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_long_odd_factor_sides_against_oracle(nx, ny, precision):
+@pytest.mark.parametrize("model", ["std", "log"])
+def test_long_odd_factor_sides_against_oracle(nx, ny, precision, model):
     """Sides whose radix-5 or radix-7 pass has more than 256 butterflies (2560 = 5 x 512,
     3584 = 7 x 512, 5120 = 5 x 1024): the state upload and the fields run the run-time
     kernels built for 1024-thread blocks, the steps the register-resident kernels where the
     length allows (else the run-time ones); 12 steps within 1e-12 (FP64) / 2e-5 (FP32-mixed)
     relative L2 of the oracle."""
     geom_o = orc.build_geometry(nx, ny, nx * 0.9, ny * 0.8)
-    prm = dict(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.25, g=0.3, dt=0.2)
-    f0 = -0.2 + 0.05 * np.random.default_rng(nx + ny).uniform(-1, 1, (ny, nx))
-    ref, rec = orc.run("std", orc.Params(**prm), geom_o, f0, 12, record_every=12)
-    sim = stdpfc.BuildB200_Simulation(stdpfc.BuildStdPFCModelParameters(**prm),
-                                      stdpfc.Build2DGeometry(nx, ny, nx * 0.9, ny * 0.8), precision=precision)
+    if model == "std":
+        prm = dict(Gamma=1.0, beta=1.0, q0=1.0, epsilon=-0.25, g=0.3, dt=0.2)
+        mean = -0.2
+    else:
+        prm = dict(Gamma=1.0, beta=0.5, q0=1.0, epsilon=-0.9, g=-2.0, dt=0.05)
+        mean = 0.55
+    f0 = mean + 0.05 * np.random.default_rng(nx + ny).uniform(-1, 1, (ny, nx))
+    ref, rec = orc.run(model, orc.Params(**prm), geom_o, f0, 12, record_every=12)
+    mod = stdpfc if model == "std" else logpfc
+    builder = mod.BuildStdPFCModelParameters if model == "std" else mod.BuildLogPFCModelParameters
+    sim = mod.BuildB200_Simulation(builder(**prm), mod.Build2DGeometry(nx, ny, nx * 0.9, ny * 0.8),
+                                   precision=precision)
     info = sim.plan.info()
     assert info["row_threads_per_fft"] > 256 or info["col_threads_per_fft"] > 256, info
-    sim.State.n[...] = f0
+    field = sim.State.n if model == "std" else sim.State.phi
+    field[...] = f0
     sim.TimeSteps(12)
     tol = 1e-12 if precision == "fp64" else 2e-5
-    got = sim.State.n.get()
+    got = field.get()
     assert rel_l2(got - f0.mean(), ref - f0.mean()) < tol, sim.plan.path()
     # the reductions and the fields of these plans (Parseval and the materialising passes)
     assert float(sim.CalculateFreeEnergy()) == pytest.approx(rec[-1][1], rel=1e-10 if precision == "fp64" else 1e-6)
     from pfc_models_b200 import _lib
-    o = orc.OracleSim("std", orc.Params(**prm), geom_o)
+    o = orc.OracleSim(model, orc.Params(**prm), geom_o)
     o.set_field(ref)
     local = sim.plan.get_field(_lib.FIELD_LOCAL_N | _lib.FIELD_OF_CURRENT).cpu().numpy()
     assert rel_l2(local - f0.mean(), o.local_field() - f0.mean()) < tol
