@@ -322,6 +322,22 @@ template <class T, int EE, int TPF> struct FastMinBlocks {
   static constexpr int value = TPF > 256 ? 1 : (data_regs <= 32 ? 4 : 2);
 };
 
+// Chunk of the column kernel's ETD1 update: the modes whose coefficients and states are
+// loaded together (4 registers per mode in FP32, 8 in FP64), a power of two dividing EE,
+// at most 8 for FP32 transforms of 16 or more values per thread, else 4 or 2. The update
+// runs in registers (REG) where the launch bounds leave room for the chunk on top of the
+// EE values held and about 28 registers of addresses and indices (the 128-register
+// kernels); in the 64-register kernels the values wait in the exchange buffer instead.
+template <class T, int EE, int TPF>
+struct ColChunk {
+  using MB = FastMinBlocks<T, EE, TPF>;
+  static constexpr int value = (sizeof(T) == 4 && EE >= 16 && EE % 8 == 0) ? 8 : (EE % 4 == 0 ? 4 : 2);
+  static constexpr int limit0 = 65536 / (MB::value * FastBound<TPF>::value);
+  static constexpr int limit = limit0 > 255 ? 255 : limit0;
+  static constexpr int per_mode = 4 * (int)(sizeof(T) / 4);
+  static constexpr bool REG = (EE & (EE - 1)) == 0 && limit >= 128 && value * per_mode <= limit - MB::data_regs - 28;
+};
+
 // ------------------------------------------------------------------ row kernel
 // CTA: `rows` consecutive rows (tile), groups of TPF threads each process rows
 // g, g + ngroups, ... The tile is staged through shared memory with a transposing
@@ -643,30 +659,62 @@ __device__ __forceinline__ void col_step_body(const FastColArgs<T>& a, const Bat
     PL::template compute<false>(v, t, twA_s + S::twA(NP - 1));
   }
 
-  // ---- ETD1 update in FP64 through the exchange buffer: publish the natural-order
-  // spectrum, update it in a loop of bounded register use with coalesced n_hat and
-  // coefficient accesses, then reload it for sequence B
+  // ---- ETD1 update. After A's last pass register v[b * RL + q] holds mode
+  // ky = t + (b + q NBL) TPF (its natural-order index), the element B's first pass loads
+  // into the same register. Where the registers allow (ColChunk::REG) the columns other
+  // than the packed one update in registers; otherwise, and for the packed column, which
+  // pairs ky with NY - ky held by another thread, the spectrum goes through the exchange
+  // buffer in natural order and is reloaded for sequence B.
   constexpr int RL = S::radA(NP - 1), NBL = EE / RL;
   using PO = FastPass<T, NY, EE, RL, NY / RL, P>;
-#pragma unroll
-  for (int b = 0; b < NBL; ++b)
-#pragma unroll
-    for (int q = 0; q < RL; ++q) buf[padi<P>(PO::out_index(t, b, q))] = v[b * RL + q];
-  group_sync<TPF>(g);
+  using CC = ColChunk<T, EE, TPF>;
   const size_t cb = (size_t)kx * NY;
   const float tau = a.slow_tau;
-  if (kx != 0) {
+  const bool packed = kx == 0;
+  if (!CC::REG || packed) {
+#pragma unroll
+    for (int b = 0; b < NBL; ++b)
+#pragma unroll
+      for (int q = 0; q < RL; ++q) buf[padi<P>(PO::out_index(t, b, q))] = v[b * RL + q];
+    group_sync<TPF>(g);
+  }
+  if (!packed) {
     const size_t ccb = (size_t)kx * nyh;
-    // Each thread updates modes ky = t + j TPF, j < EE, in chunks: the coefficients and
-    // states of a whole chunk are loaded before any of its results is stored (the
+    // mode ky of coefficient cw, state p, transformed nonlinearity gv (updated in place)
+    auto update = [&](int ky, const cplx<T>& cw, const cplx<T>& p, cplx<T>& gv) {
+      const int kh = ky <= NY / 2 ? ky : NY - ky;
+      if constexpr (sizeof(T) == 4) {
+        if (fabsf(cw.x) >= tau) {
+          // fast modes (|A - 1| >= tau): the update in FP32 on hi alone; their rounding
+          // errors are damped by at least tau every step
+          const cplx<float> o = mk(fmaf(cw.x, p.x, p.x) + cw.y * gv.x, fmaf(cw.x, p.y, p.y) + cw.y * gv.y);
+          static_cast<cplx<float>*>(gnout)[cb + ky] = o;
+          gv = o;
+        } else {
+          // slow modes: FP64 coefficients and the state with its residual
+          const cplx<double> c = gcoef64[ccb + kh];
+          const cplx<float> l = gnin_lo[cb + ky];
+          cplx<double> pd = mk((double)p.x, (double)p.y);
+          pd.x += (double)l.x;
+          pd.y += (double)l.y;
+          const cplx<double> o = pd + c.x * pd + c.y * mk((double)gv.x, (double)gv.y);
+          state_st<T>(gnout, gnout_lo, cb + ky, o, true);
+          gv = mk((T)o.x, (T)o.y);
+        }
+      } else {
+        const cplx<double> c = cw, pd = p;
+        const cplx<double> o = pd + c.x * pd + c.y * mk((double)gv.x, (double)gv.y);
+        state_st<T>(gnout, gnout_lo, cb + ky, o, true);
+        gv = mk((T)o.x, (T)o.y);
+      }
+    };
+    // Each thread updates its modes ky = t + j TPF, j < EE, in chunks: the coefficients
+    // and states of a whole chunk are loaded before any of its results is stored (the
     // compiler may not move a load above an earlier store to memory it cannot tell
     // apart), so the chunk's loads are in flight together.
-    // within the 64-register budget, and dividing EE (mixed-radix transforms hold 24 or 28)
-    constexpr int CH = (sizeof(T) == 4 && EE >= 16 && EE % 8 == 0) ? 8 : (EE % 4 == 0 ? 4 : 2);
+    constexpr int CH = CC::value;
     static_assert(EE % CH == 0, "chunks tile the modes of a thread");
-#pragma unroll 1
-    for (int j0 = 0; j0 < EE; j0 += CH) {
-      cplx<T> cw[CH], p[CH];
+    auto chunk_loads = [&](int j0, cplx<T>* cw, cplx<T>* p) {
 #pragma unroll
       for (int j = 0; j < CH; ++j) {
         const int ky = t + (j0 + j) * TPF;
@@ -674,35 +722,29 @@ __device__ __forceinline__ void col_step_body(const FastColArgs<T>& a, const Bat
         cw[j] = ldgc(gcoef + ccb + kh);   // cached: modes ky and NY - ky share an entry
         p[j] = ld_field<COHERENT>(static_cast<const cplx<T>*>(gnin) + cb + ky);
       }
+    };
+    if constexpr (CC::REG) {
 #pragma unroll
-      for (int j = 0; j < CH; ++j) {
-        const int ky = t + (j0 + j) * TPF;
-        const int kh = ky <= NY / 2 ? ky : NY - ky;
-        const cplx<T> gv = buf[padi<P>(ky)];
-        if constexpr (sizeof(T) == 4) {
-          if (fabsf(cw[j].x) >= tau) {
-            // fast modes (|A - 1| >= tau): the update in FP32 on hi alone; their
-            // rounding errors are damped by at least tau every step
-            const cplx<float> o = mk(fmaf(cw[j].x, p[j].x, p[j].x) + cw[j].y * gv.x,
-                                     fmaf(cw[j].x, p[j].y, p[j].y) + cw[j].y * gv.y);
-            static_cast<cplx<float>*>(gnout)[cb + ky] = o;
-            buf[padi<P>(ky)] = o;
-          } else {
-            // slow modes: FP64 coefficients and the state with its residual
-            const cplx<double> c = gcoef64[ccb + kh];
-            const cplx<float> l = gnin_lo[cb + ky];
-            cplx<double> pd = mk((double)p[j].x, (double)p[j].y);
-            pd.x += (double)l.x;
-            pd.y += (double)l.y;
-            const cplx<double> o = pd + c.x * pd + c.y * mk((double)gv.x, (double)gv.y);
-            state_st<T>(gnout, gnout_lo, cb + ky, o, true);
-            buf[padi<P>(ky)] = mk((T)o.x, (T)o.y);
-          }
-        } else {
-          const cplx<double> c = cw[j], pd = p[j];
-          const cplx<double> o = pd + c.x * pd + c.y * mk((double)gv.x, (double)gv.y);
-          state_st<T>(gnout, gnout_lo, cb + ky, o, true);
-          buf[padi<P>(ky)] = mk((T)o.x, (T)o.y);
+      for (int j0 = 0; j0 < EE; j0 += CH) {
+        cplx<T> cw[CH], p[CH];
+        chunk_loads(j0, cw, p);
+#pragma unroll
+        for (int j = 0; j < CH; ++j) {
+          const int jj = j0 + j;
+          update(t + jj * TPF, cw[j], p[j], v[(jj % NBL) * RL + jj / NBL]);
+        }
+      }
+    } else {
+#pragma unroll 1
+      for (int j0 = 0; j0 < EE; j0 += CH) {
+        cplx<T> cw[CH], p[CH];
+        chunk_loads(j0, cw, p);
+#pragma unroll
+        for (int j = 0; j < CH; ++j) {
+          const int ky = t + (j0 + j) * TPF;
+          cplx<T> gv = buf[padi<P>(ky)];
+          update(ky, cw[j], p[j], gv);
+          buf[padi<P>(ky)] = gv;
         }
       }
     }
@@ -749,9 +791,11 @@ __device__ __forceinline__ void col_step_body(const FastColArgs<T>& a, const Bat
       }
     }
   }
-  group_sync<TPF>(g);
-  FastPass<T, NY, EE, S::radB(0), 1, P>::load(buf, v, t);
-  group_sync<TPF>(g);
+  if (!CC::REG || packed) {
+    group_sync<TPF>(g);
+    FastPass<T, NY, EE, S::radB(0), 1, P>::load(buf, v, t);
+    group_sync<TPF>(g);
+  }
 
   // ---- inverse sequence B; the last pass writes W to HBM
   if constexpr (NP == 1) {
