@@ -108,8 +108,12 @@ __device__ __noinline__ void queue_row_body(const QueueClass<T>* C, const BatchB
 }
 template <class T, int NY>
 __device__ __noinline__ void queue_col_body(const QueueClass<T>* C, const BatchBufs* table, int tile, int local) {
-  col_step_body<T, NY, queue_col_ee(sizeof(T) == 8, NY), true>(C->col, table, tile, local, C->col_threads,
-                                                               NoSync{});
+  constexpr int EE = queue_col_ee(sizeof(T) == 8, NY);
+  // the queue kernel runs in 64 registers: its column bodies keep the buffered ETD1 update
+  static_assert(!ColChunk<T, FastSeq<NY, EE, RadixCap<T>::value>::EE,
+                          FastSeq<NY, EE, RadixCap<T>::value>::TPF>::REG,
+                "queue column bodies update through the exchange buffer");
+  col_step_body<T, NY, EE, true>(C->col, table, tile, local, C->col_threads, NoSync{});
 }
 
 template <class T, int L>
