@@ -323,15 +323,17 @@ template <class T, int EE, int TPF> struct FastMinBlocks {
 };
 
 // Chunk of the column kernel's ETD1 update: the modes whose coefficients and states are
-// loaded together (4 registers per mode in FP32, 8 in FP64), a power of two dividing EE,
-// at most 8 for FP32 transforms of 16 or more values per thread, else 4 or 2. The update
+// loaded together (4 registers per mode in FP32, 8 in FP64), a power of two dividing EE:
+// 8 for FP32 transforms of 16 or 24 values per thread, 4 for 32 (with 8 the in-register
+// update spilled 16 bytes per thread and ran 0.5-1 % slower), else 4 or 2. The update
 // runs in registers (REG) where the launch bounds leave room for the chunk on top of the
 // EE values held and about 28 registers of addresses and indices (the 128-register
 // kernels); in the 64-register kernels the values wait in the exchange buffer instead.
 template <class T, int EE, int TPF>
 struct ColChunk {
   using MB = FastMinBlocks<T, EE, TPF>;
-  static constexpr int value = (sizeof(T) == 4 && EE >= 16 && EE % 8 == 0) ? 8 : (EE % 4 == 0 ? 4 : 2);
+  static constexpr int value =
+      (sizeof(T) == 4 && EE == 32) ? 4 : ((sizeof(T) == 4 && EE >= 16 && EE % 8 == 0) ? 8 : (EE % 4 == 0 ? 4 : 2));
   static constexpr int limit0 = 65536 / (MB::value * FastBound<TPF>::value);
   static constexpr int limit = limit0 > 255 ? 255 : limit0;
   static constexpr int per_mode = 4 * (int)(sizeof(T) / 4);
