@@ -13,10 +13,20 @@ def test_packaged_table_is_used_without_a_user_cache(tmp_path, monkeypatch):
     assert key in table
     v = tune.lookup(2048, 2048, _lib.FP32_MIXED, _lib.MODEL_STD, device_name="NVIDIA B200")
     assert v == {k: int(table[key].get(k) or 0) for k in tune.VARIANT_KEYS}
-    for e in table.values():
+    for k, e in table.items():
         # 0: the plan's own choice (a side with an odd factor holds a fixed number per thread)
         assert e["ee_row"] in (0, 8, 16, 32) and e["ee_col"] in (0, 8, 16, 32) and 1 <= e["row_tile"] <= 16
         assert e.get("col_cta", 0) in (0, 1, 2, 4) and e.get("pdl", 0) in (0, 1, 2)
+        assert e.get("packed") in (None, 0, 1, 2, 3) and e.get("tma") in (None, 0, 1)
+        _, grid, prec, model = k.split("|")[:4]
+        nx, ny = (int(x) for x in grid.split("x"))
+        assert prec in ("fp32", "fp64") and model in ("std", "log"), k
+        if prec == "fp64":
+            # 16 complex doubles per thread at most; the two-lane kernels are FP32 only
+            assert e["ee_row"] <= 16 and e["ee_col"] <= 16 and not e.get("packed") and not e.get("tma"), k
+        assert e["ee_row"] <= nx // 2 and e["ee_col"] <= ny, k
+        # every entry encodes into the plan's flag bits
+        _lib.flag_variant(**{v: int(e.get(v) or 0) for v in tune.VARIANT_KEYS})
     # batch-measured entries are preferred for batches and fall back to the single-plan ones
     bkey = "NVIDIA B200|512x512|fp32|std|batch"
     assert bkey in table
