@@ -339,6 +339,10 @@ struct ColChunk {
   static constexpr int per_mode = 4 * (int)(sizeof(T) / 4);
   static constexpr bool REG = (EE & (EE - 1)) == 0 && limit >= 128 && value * per_mode <= limit - MB::data_regs - 28;
 };
+// the 2048-point columns: FP32 with 16 values per thread (64 registers) buffered, with 32 in
+// registers; FP64 with 8 buffered, with 16 in registers
+static_assert(!ColChunk<float, 16, 128>::REG && ColChunk<float, 32, 64>::REG, "FP32 column update forms");
+static_assert(!ColChunk<double, 8, 256>::REG && ColChunk<double, 16, 128>::REG, "FP64 column update forms");
 
 // ------------------------------------------------------------------ row kernel
 // CTA: `rows` consecutive rows (tile), groups of TPF threads each process rows
